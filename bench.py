@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 phase-field step: cell-updates/s of the 3D
+three-variant martensite at 256^3, FP32, Philox noise (the headline workload).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  The path does not shard a single
+simulation: every rank advances its own replica (sim_id = rank) with no data
+collective, so `value` is the whole-job aggregate of N replicas ("weak").
+
+value   -- device time of K steps on resident HBM data, CUDA events on the
+           launching stream, max over ranks.
+e2e     -- the same metric through the C ABI with host buffers: every step
+           uploads the field set from pinned host memory (gs_sim_set_field),
+           steps once (gs_sim_step) and reads the field set back
+           (gs_sim_get_field); host clock around device synchronisation.
+roofline-- the dominant pass, timed live with CUDA events between passes
+           (gs_sim_profile_step), algorithmic bytes / time vs measured HBM.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "general-simulator_b200"))
+
+METRIC = "cell-updates/s at 256³ martensite, % HBM roofline; adjoint:forward; sims/s"
+UNIT = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(n: int, steps: int, extra: dict | None = None) -> dict:
+    cfg = {
+        "workload": f"martensite TDGL + Khachaturyan elasticity, 3D {n}^3, 3 variants, FP32 fields, "
+                    "Philox noise 1e-3, dt 0.005, sigma_zz 0.005",
+        "grid": [n, n, n], "variants": 3, "dtype": "fp32", "timed_steps": steps,
+        "l2": "inputs larger than L2 (field set + spectrum = 2 x 201 MB > 126 MB L2); no flush",
+        "initial": "eta ~ U[-0.01, 0.01], numpy PCG64 seed 1",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_setup(gpus: int):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int) -> None:
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.12)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def committed_traffic() -> dict | None:
+    """DRAM bytes per launch of the dominant pass from the committed ncu
+    summary (profiles/dram_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle on the host cores
+# ---------------------------------------------------------------------------
+def cpu_baseline(n: int, seconds: float) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gs_b200 as gb
+    import oracle_py as orc
+
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    p = gb.mart3d_params(n, noise=1e-3)
+    eta = gb.initial_eta(p, 1)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        eta = orc.mart_run(p, eta, 1, step0=steps)
+        steps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n ** 3 * steps / dt, "unit": UNIT, "cores": orc.get_threads(), "kind": "port",
+            "sample": f"{steps} FP64 oracle step(s) of the {n}^3 3-variant workload, {dt:.1f} s "
+                      f"({orc.get_threads()} OpenMP threads)"}
+
+
+def run_reference(args, ws, rank):
+    """The reference arm: the reference has no CPU implementation of the
+    step (its kernels are device-only), so this times the FP64 CPU port of
+    the same discretisation on all host cores."""
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gs_b200 as gb
+    import oracle_py as orc
+
+    orc.set_threads(cores)
+    p = gb.mart3d_params(args.n, noise=1e-3)
+    eta = gb.initial_eta(p, 1)
+    budget = 150.0
+    t0 = time.perf_counter()
+    for i in range(max(0, min(args.warmup, 1))):
+        eta = orc.mart_run(p, eta, 1, step0=i)
+    done = 0
+    ts = time.perf_counter()
+    for i in range(args.steps):
+        eta = orc.mart_run(p, eta, 1, step0=1 + i)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - ts
+    v = args.n ** 3 * done / dt
+    sample = (f"{done} of {args.steps} requested steps (time budget {budget:.0f} s), FP64 oracle port, "
+              f"{orc.get_threads()} threads")
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
+            "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": workload_config(args.n, done),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": orc.get_threads(), "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, ws, rank, local):
+    import torch
+
+    import gs_b200 as gb
+
+    torch.cuda.set_device(local)
+    dev_uuid = None
+    try:
+        dev_uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    n = args.n
+    p = gb.mart3d_params(n, dtype=gb.GS_DTYPE_F32, noise=1e-3)
+    p.sim_id = rank
+    eta0 = gb.initial_eta(p, 1).astype(np.float32)
+    V, N = p.nvariants, p.ncells
+    sim = gb.Sim(p)
+    sim.set_field("eta", eta0)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        sim.step(args.warmup, sh)
+        launches_per_step = sim.launch_count() / max(args.warmup, 1)
+        torch.cuda.synchronize()
+        barrier(ws)
+        torch.cuda.synchronize()
+        clk = ClockSampler(dev_uuid)
+        clk.start()
+        time.sleep(0.15)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step(args.steps, sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        ms = e0.elapsed_time(e1)
+        barrier(ws)
+    ms_max = max_over_ranks(ms, ws)
+    value = N * args.steps * ws / (ms_max / 1e3)
+    launches = int(round(launches_per_step * args.steps))
+
+    # per-pass device times of one step (live, on the launching stream)
+    with torch.cuda.stream(stream):
+        passes = [sim.profile_step(sh) for _ in range(5)]
+    pass_ms = np.median(np.array(passes), axis=0)
+    # algorithmic HBM bytes of each pass, FP32, V fields of N cells
+    f = 4 * V * N
+    names = ["z_forward_r2c_eta2", "y_forward", "x_fwd_contract_inv", "y_inverse", "z_inverse_c2r_update"]
+    algo = [2 * f, 2 * f, 2 * f, 2 * f, 3 * f]
+    dom = int(np.argmax(pass_ms))
+    peaks = measured_peaks()
+    achieved = algo[dom] / (pass_ms[dom] / 1e3) / 1e9
+    tr = committed_traffic()
+    traffic = None
+    if tr and tr.get("kernel_pass") == names[dom] and tr.get("n") == n:
+        traffic = tr.get("dram_bytes_per_launch")
+    step_bytes = sum(algo)
+    step_gbs = step_bytes * args.steps / (ms / 1e3) / 1e9
+
+    # e2e through the C ABI with host buffers
+    pinned = torch.empty(V * N, dtype=torch.float32).pin_memory()
+    pinned.numpy()[:] = eta0.ravel()
+    out_pinned = torch.empty(V * N, dtype=torch.float32).pin_memory()
+    import ctypes as C
+
+    L = gb.lib()
+    ptr_in = C.c_void_p(pinned.data_ptr())
+    ptr_out = C.c_void_p(out_pinned.data_ptr())
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            gb.check(L.gs_sim_set_field(sim.h, b"eta", ptr_in, V * N, 0), "set_field")
+            sim.step(1, sh)
+            gb.check(L.gs_sim_get_field(sim.h, b"eta", ptr_out, V * N, 0), "get_field")
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            gb.check(L.gs_sim_set_field(sim.h, b"eta", ptr_in, V * N, 0), "set_field")
+            sim.step(1, sh)
+            gb.check(L.gs_sim_get_field(sim.h, b"eta", ptr_out, V * N, 0), "get_field")
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, ws)
+    e2e = {"value": N * args.e2e_steps * ws / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * V * N,
+           "d2h_bytes_per_step": 4 * V * N, "steps": args.e2e_steps,
+           "how": "per step: gs_sim_set_field(eta, pinned host) + gs_sim_step(1) + gs_sim_get_field(eta, pinned "
+                  "host); host clock with device synchronisation"}
+    sim.close()
+
+    if rank != 0:
+        return
+    cpu = None
+    if ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(n, args.cpu_seconds)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(n, args.steps, {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                                                   "step_bytes_algorithmic": step_bytes,
+                                                   "step_gbs_algorithmic": step_gbs}),
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": peaks["source"], "algorithmic_bytes_per_launch": algo[dom],
+                     "launch_ms": float(pass_ms[dom]),
+                     "pass_ms": {nm: float(t) for nm, t in zip(names, pass_ms)}},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # no device work: rank 0 times the CPU implementation, others exit
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    ws, rank, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,82 @@
+"""Build recipe of the B200 phase-field library (sm_100a) and its C++ front end.
+
+Outputs (in-tree, git-ignored, shipped with the working copy):
+  general-simulator_b200/libgsb200.so   CUDA kernels + C ABI (include/gs_capi.h)
+  general-simulator_b200/gsi            script interpreter (the reference's front end)
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+HOST = os.path.join(HERE, "host")
+BUILD = os.path.join(HERE, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+           "-Xptxas", "-warn-spills"]
+CU_SOURCES = ["gs_capi.cu", "gs_k_zy.cu", "gs_k_zy_f32.cu", "gs_k_zy_f64.cu", "gs_k_x.cu", "gs_k_x46.cu",
+              "gs_k_x55.cu", "gs_k_x99.cu", "gs_k_xreg.cu", "gs_k_mart.cu", "gs_k_mart_f32.cu", "gs_k_mart_f64.cu",
+              "gs_plain.cu"]
+LIB = os.path.join(HERE, "libgsb200.so")
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} {cmd[-1]}")
+    if r.stderr.strip():
+        sys.stderr.write(r.stderr)
+
+
+def _stale(out: str, deps: list[str]) -> bool:
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _headers() -> list[str]:
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    return hs + [os.path.join(ROOT, "include", "gs_capi.h")]
+
+
+def build_lib(jobs: int = 8, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    hdrs = _headers()
+    objs = []
+    todo = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if _stale(o, [s] + hdrs):
+            todo.append([NVCC, *ARCH, *NVFLAGS, "-c", s, "-o", o])
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        for f in [ex.submit(_run, c) for c in todo]:
+            f.result()
+    if todo or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcufft", "-Xlinker",
+              "-rpath=/usr/local/cuda/lib64"])
+    return LIB
+
+
+def build_oracle() -> str:
+    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    return os.path.join(ROOT, "oracle", "liboracle.so")
+
+
+def build_all(jobs: int = 8) -> None:
+    build_lib(jobs)
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build_all()
+    print("built", LIB)

@@ -1,0 +1,758 @@
+// gs_capi.cu -- C ABI of the B200 phase-field step (include/gs_capi.h).
+//
+// Owns the device state of one simulation and sequences the HBM sweeps of a
+// step.  The reference's equivalent is Dynamics_mart::Initialize / Calculate
+// / Get (src/dynamics_mart.cu:14-173,348-417,443-456) over Data<Real>
+// buffers, cuFFT plans and cuRAND generators.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gs_capi.h"
+#include "gs_launch.h"
+#include "gs_mart.cuh"
+#include "gs_sim.h"
+
+using namespace gs;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+
+int gs_set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int gs_cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return GS_OK;
+  if (e == cudaErrorMemoryAllocation) return gs_set_error(GS_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+    return gs_set_error(GS_ENODEV, "%s: %s", what, cudaGetErrorString(e));
+  return gs_set_error(GS_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define GS_TRY(expr)             \
+  do {                           \
+    int rc__ = (expr);           \
+    if (rc__ != GS_OK) return rc__; \
+  } while (0)
+#define GS_CU(expr, what) GS_TRY(gs_cuda_check((expr), (what)))
+
+extern "C" int gs_version(void) { return GS_CAPI_VERSION; }
+extern "C" size_t gs_sizeof_params(void) { return sizeof(gs_params); }
+extern "C" size_t gs_sizeof_stats(void) { return sizeof(gs_stats); }
+
+extern "C" int gs_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return GS_EINVAL;
+  snprintf(buf, len, "%s", g_err);
+  return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// defaults
+// ---------------------------------------------------------------------------
+static void set_cubic(gs_params* p, double c11, double c12, double c44) {
+  memset(p->cijkl, 0, sizeof(p->cijkl));
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) p->cijkl[i][i][j][j] = c12;
+  for (int i = 0; i < 3; ++i) p->cijkl[i][i][i][i] = c11;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      if (i != j) {
+        p->cijkl[i][j][i][j] = c44;
+        p->cijkl[i][j][j][i] = c44;
+      }
+}
+
+// default modulus of Dynamics_stress (src/dynamics_stress.cu:56-78)
+static void set_stress_default_modulus(gs_params* p) {
+  memset(p->cijkl, 0, sizeof(p->cijkl));
+  double(*c)[3][3][3] = p->cijkl;
+  c[0][0][0][0] = 5.39; c[1][1][1][1] = 5.39; c[2][2][2][2] = 5.22;
+  c[0][0][1][1] = 3.39; c[1][1][2][2] = 3.56; c[2][2][0][0] = 3.56;
+  c[0][1][0][1] = 0.6;  c[1][2][1][2] = 0.77; c[2][0][2][0] = 0.77;
+  c[1][1][0][0] = 3.39; c[2][2][1][1] = 3.56; c[0][0][2][2] = 3.56;
+  c[1][0][1][0] = 0.60; c[0][1][1][0] = 0.60; c[1][0][0][1] = 0.60;
+  c[2][1][2][1] = 0.77; c[2][1][1][2] = 0.77; c[1][2][2][1] = 0.77;
+  c[0][2][0][2] = 0.77; c[0][2][2][0] = 0.77; c[2][0][0][2] = 0.77;
+}
+
+static void tetragonal(gs_params* p, int nv, double along, double other) {
+  memset(p->eigenstrain, 0, sizeof(p->eigenstrain));
+  for (int v = 0; v < nv; ++v)
+    for (int a = 0; a < 3; ++a) p->eigenstrain[v][a][a] = (a == v % 3) ? along : other;
+}
+
+extern "C" int gs_params_default(gs_params* p, int model, int mode) {
+  if (!p) return gs_set_error(GS_EINVAL, "gs_params_default: null params");
+  memset(p, 0, sizeof(*p));
+  p->model = model;
+  p->mode = mode;
+  p->dtype = GS_DTYPE_F32;
+  p->dx = p->dy = p->dz = 1.0;
+  p->weight_elastic = 1.0;
+  p->xi = 1.0;
+  if (model == GS_MODEL_MART) {
+    if (mode == GS_MODE_REFCOMPAT) {
+      // src/dynamics_mart.cu:20-27,40,80-89
+      p->nvariants = 4;
+      p->nx = p->ny = p->nz = 64;
+      p->dt = 0.01;
+      p->transition_temperature = 450.0;
+      p->temperature = 450.0;
+      p->weight_gradient = 2.5;
+      p->weight_chemical = 1.0;
+      p->weight_elastic = 100000.0;
+      p->weight_dislocation = 1.0;
+      p->noise_amp = 0.0001;
+      p->lpc[2] = 32.05;
+      p->lpc[3] = 37.5;
+      set_cubic(p, 3.5, 1.5, 1.0);
+    } else {
+      // 3D cubic-to-tetragonal, 3 variants, 256^3 (the headline workload)
+      p->nvariants = 3;
+      p->nx = p->ny = p->nz = 256;
+      p->dt = 0.005;
+      p->landau[0] = 0.2;
+      p->landau[1] = 3.0;
+      p->landau[2] = 2.0;
+      p->landau[3] = 1.0;
+      p->kappa = 0.5;
+      p->mobility = 1.0;
+      tetragonal(p, 3, 0.02, -0.01);
+      set_cubic(p, 1.4, 0.84, 0.56);
+      p->applied_stress[2][2] = 0.005;
+      p->noise_amp = 1e-3;
+      p->seed = 1;
+    }
+  } else if (model == GS_MODEL_PRECIPITATE) {
+    p->nvariants = 4;
+    if (mode == GS_MODE_REFCOMPAT) {
+      // src/dynamics_precipitate.cu:20-29,55
+      p->nx = p->ny = p->nz = 64;
+      p->dt = 0.1;
+      const double A[8] = {0, 54.0, -17.0, 7.0, 2.5, 0.2, 0.2, 0.2};
+      memcpy(p->coef, A, sizeof(A));
+      p->kappa_eta = 300.0;
+      p->kappa_c = 300.0;
+      p->mobility_c = 0.4;
+      p->mobility_eta = 0.4;
+      p->xi = 400.0;
+      p->c1 = 0.1;
+      p->c2 = 0.44;
+      p->noise_amp = 1.0;
+      set_cubic(p, 3.5, 1.5, 1.0);
+    } else {
+      // 3D precipitate, c + 4 variants, 256^3
+      p->nx = p->ny = p->nz = 256;
+      p->dt = 0.01;
+      // f = A1/2 (c-c1)^2 + A2/2 (c2-c) S eta^2 - A3/4 S eta^4 + A4/6 S eta^6
+      //     + A5 S_{p<q} eta_p^2 eta_q^2, written in the 7-coefficient form
+      const double A[8] = {0, 2.0, -20.0, 16.0, 14.0, 1.0, 0.0, 0.0};
+      memcpy(p->coef, A, sizeof(A));
+      p->c1 = 0.05;
+      p->c2 = 0.95;
+      p->kappa_c = 1.5;
+      p->kappa_eta = 1.0;
+      p->mobility_c = 1.0;
+      p->mobility_eta = 1.0;
+      p->misfit_c = 0.01;
+      p->c_elastic = 1;
+      p->mass_projection = 1;
+      tetragonal(p, 4, 0.005, -0.0025);
+      set_cubic(p, 1.4, 0.84, 0.56);
+      p->seed = 2;
+    }
+  } else if (model == GS_MODEL_STRESS) {
+    p->nvariants = 4;
+    p->nx = p->ny = p->nz = 64;
+    p->dt = 1.0;
+    if (mode == GS_MODE_REFCOMPAT) {
+      p->xi = 4000.0;  // src/dynamics_stress.cu:34
+      set_stress_default_modulus(p);
+    } else {
+      set_cubic(p, 1.4, 0.84, 0.56);
+    }
+  } else {
+    return gs_set_error(GS_EINVAL, "gs_params_default: unknown model %d", model);
+  }
+  return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// geometry and constants
+// ---------------------------------------------------------------------------
+static int canonicalize(gs_sim* s) {
+  const gs_params& p = s->p;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  if (nx < 1 || ny < 1 || nz < 1) return gs_set_error(GS_EINVAL, "grid %d %d %d", nx, ny, nz);
+  const double d[3] = {p.dx, p.dy, p.dz};
+  int n[3], perm[3];
+  if (nz > 1) {
+    n[0] = nx; n[1] = ny; n[2] = nz; perm[0] = 0; perm[1] = 1; perm[2] = 2;
+  } else if (ny > 1) {
+    n[0] = 1; n[1] = nx; n[2] = ny; perm[0] = 2; perm[1] = 0; perm[2] = 1;
+  } else {
+    n[0] = 1; n[1] = 1; n[2] = nx; perm[0] = 1; perm[1] = 2; perm[2] = 0;
+  }
+  for (int c = 0; c < 3; ++c) {
+    s->perm[c] = perm[c];
+    s->dcan[c] = d[perm[c]];
+  }
+  s->n0 = n[0];
+  s->n1 = n[1];
+  s->n2 = n[2];
+  if (n[2] % 2 != 0) return gs_set_error(GS_ENOTSUP, "last non-unit axis must be even (got %d)", n[2]);
+  s->h = n[2] / 2;
+  s->N = (long long)n[0] * n[1] * n[2];
+  if (!size_supported(s->h) || !size_supported(n[1]) || !size_supported(n[0]))
+    return gs_set_error(GS_ENOTSUP, "grid %dx%dx%d: line lengths must be 1 or one of 2,4,6,8,12,16,24,32,48,64,96,128,256 (z: 2x that)",
+                        nx, ny, nz);
+  if (n[1] != 1 && n[1] % 2 != 0) return gs_set_error(GS_ENOTSUP, "middle axis must be 1 or even");
+  return GS_OK;
+}
+
+// strain sets of the B contraction: 0 = variants x variants, 1 = 6 unit
+// strains x variants, 2 = precipitate fields (eta_p^2 then c)
+static void strain_sets(const gs_params& p, int which, double (*ea)[3][3], int* na, double (*eb)[3][3], int* nb) {
+  const int V = p.nvariants;
+  if (which == 1) {
+    const int bi[6] = {0, 0, 0, 1, 1, 2}, bj[6] = {0, 1, 2, 1, 2, 2};
+    for (int b = 0; b < 6; ++b) {
+      memset(ea[b], 0, sizeof(double) * 9);
+      if (p.mode == GS_MODE_REFCOMPAT || bi[b] == bj[b]) {
+        ea[b][bi[b]][bj[b]] = 1.0;
+      } else {
+        ea[b][bi[b]][bj[b]] = 0.5;
+        ea[b][bj[b]][bi[b]] = 0.5;
+      }
+    }
+    *na = 6;
+    for (int v = 0; v < V; ++v) memcpy(eb[v], p.eigenstrain[v], sizeof(double) * 9);
+    *nb = V;
+    return;
+  }
+  for (int v = 0; v < V; ++v) {
+    memcpy(ea[v], p.eigenstrain[v], sizeof(double) * 9);
+    memcpy(eb[v], p.eigenstrain[v], sizeof(double) * 9);
+  }
+  int F = V;
+  if (which == 2 && p.c_elastic) {
+    memset(ea[V], 0, sizeof(double) * 9);
+    for (int i = 0; i < 3; ++i) ea[V][i][i] = p.misfit_c;
+    memcpy(eb[V], ea[V], sizeof(double) * 9);
+    F = V + 1;
+  }
+  *na = *nb = F;
+}
+
+template <typename T> void build_elastic(const gs_sim* s, int which, double scale, ElasticConst<T>& ec) {
+  const gs_params& p = s->p;
+  double ea[GS_MAXG + 1][3][3], eb[GS_MAXF + 1][3][3];
+  int na, nb;
+  strain_sets(p, which, ea, &na, eb, &nb);
+  memset(&ec, 0, sizeof(ec));
+  ec.na = na;
+  ec.nb = nb;
+  ec.refcompat = p.mode == GS_MODE_REFCOMPAT;
+  const double(*C)[3][3][3] = p.cijkl;
+  const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int q = 0; q < 6; ++q) {
+        const int a = pa[q], b = pb[q];
+        double v = C[i][a][b][j];
+        if (a != b) v += C[i][b][a][j];
+        ec.q[i * 3 + j][q] = (T)v;
+      }
+  auto sig = [&](const double e[3][3], T out[3][3]) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double acc = 0;
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) acc += C[i][j][k][l] * e[k][l];
+        out[i][j] = (T)acc;
+      }
+  };
+  for (int a = 0; a < na; ++a) sig(ea[a], ec.sa[a]);
+  for (int b = 0; b < nb; ++b) sig(eb[b], ec.sb[b]);
+  for (int a = 0; a < na; ++a)
+    for (int b = 0; b < nb; ++b) {
+      double acc = 0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) acc += C[i][j][k][l] * ea[a][i][j] * eb[b][k][l];
+      ec.a0[a][b] = (T)acc;
+    }
+  const int nc[3] = {s->n0, s->n1, s->n2};
+  for (int c = 0; c < 3; ++c) {
+    const double d = s->dcan[c];
+    ec.kscale[c] = (T)(ec.refcompat ? 2.0 * 3.14 * d / nc[c] : 2.0 * M_PI / (nc[c] * d));
+  }
+  ec.scale = (T)scale;
+}
+
+static double contract33(const double a[3][3], const double b[3][3]) {
+  double s = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) s += a[i][j] * b[i][j];
+  return s;
+}
+
+template <typename T> void build_mart(const gs_sim* s, MartConst<T>& mc) {
+  const gs_params& p = s->p;
+  memset(&mc, 0, sizeof(mc));
+  const bool ref = p.mode == GS_MODE_REFCOMPAT;
+  mc.V = p.nvariants;
+  mc.refcompat = ref;
+  mc.has_defect = s->defect != nullptr;
+  mc.has_K = s->K != nullptr;
+  mc.dt = (T)p.dt;
+  const int nc[3] = {s->n0, s->n1, s->n2};
+  for (int c = 0; c < 3; ++c) {
+    const double d = s->dcan[c];
+    if (nc[c] == 1) {
+      mc.lapc[c] = 0;
+      mc.gcoef[c] = 0;
+    } else {
+      mc.lapc[c] = (T)(ref ? p.weight_gradient / (2.0 * d) / 3.0 : p.mobility * p.kappa / (d * d));
+      mc.gcoef[c] = (T)(1.0 / (d * d));
+    }
+  }
+  mc.A2 = (T)p.landau[0];
+  mc.A4 = (T)p.landau[1];
+  mc.A6 = (T)p.landau[2];
+  mc.Ac = (T)p.landau[3];
+  mc.L = (T)p.mobility;
+  mc.kappa = (T)p.kappa;
+  mc.el = (T)(ref ? -p.weight_elastic : -2.0 * p.mobility * p.weight_elastic);
+  for (int v = 0; v < p.nvariants; ++v) {
+    const double sa = contract33(p.applied_stress, p.eigenstrain[v]);
+    mc.lin[v] = (T)(ref ? 0.0 : 2.0 * p.mobility * sa);
+    mc.appl[v] = (T)sa;
+  }
+  mc.kc = (T)(ref ? -25.0 * p.weight_dislocation : 2.0 * p.mobility * p.weight_dislocation);
+  mc.wD = (T)p.weight_dislocation;
+  const float a1 = 0.02f * ((float)p.temperature - (float)p.transition_temperature);
+  mc.a1 = (T)a1;
+  mc.a2 = (T)p.lpc[2];
+  mc.a3 = (T)p.lpc[3];
+  mc.s = (T)std::sqrt(std::fabs((double)a1 / (p.lpc[2] - p.lpc[3])));
+  mc.wC = (T)p.weight_chemical;
+  mc.noise = (T)(ref ? p.dt * p.noise_amp : p.noise_amp);
+  mc.wel_half = (T)(0.5 * p.weight_elastic);
+  mc.k0 = (uint32_t)(p.seed & 0xffffffffu);
+  mc.k1 = (uint32_t)(p.seed >> 32);
+  mc.sim = p.sim_id;
+  mc.step = (uint32_t)s->step;
+}
+
+// twiddle tables w_n^m = exp(-2 pi i m / n), m < n, for n2, h, n1, n0
+template <typename T> static int build_twiddles(gs_sim* s) {
+  const int lens[4] = {s->n2, s->h, s->n1, s->n0};
+  size_t total = 0;
+  for (int i = 0; i < 4; ++i) {
+    s->tw_off[i] = total;
+    total += (size_t)lens[i];
+  }
+  std::vector<cplx<T>> host(total);
+  for (int i = 0; i < 4; ++i)
+    for (int m = 0; m < lens[i]; ++m) {
+      const double a = 2.0 * M_PI * (double)m / (double)lens[i];
+      host[s->tw_off[i] + m] = mk2((T)std::cos(a), (T)-std::sin(a));
+    }
+  GS_CU(cudaMalloc(&s->tw, total * sizeof(cplx<T>)), "cudaMalloc twiddles");
+  GS_CU(cudaMemcpy(s->tw, host.data(), total * sizeof(cplx<T>), cudaMemcpyHostToDevice), "upload twiddles");
+  return GS_OK;
+}
+
+template <typename T> static const cplx<T>* twp(const gs_sim* s, int which) {
+  return reinterpret_cast<const cplx<T>*>(s->tw) + s->tw_off[which];
+}
+
+// ---------------------------------------------------------------------------
+// the martensite step
+// ---------------------------------------------------------------------------
+template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st) {
+  const int V = s->p.nvariants;
+  const long long rows = (long long)s->n0 * s->n1;
+  ZfwdArgs<T> za;
+  memset(&za, 0, sizeof(za));
+  for (int f = 0; f < V; ++f) {
+    za.src[f] = eta + (long long)f * s->N;
+    za.square[f] = 1;
+  }
+  za.dst = reinterpret_cast<cplx<T>*>(s->spec);
+  za.rows_per_field = rows;
+  za.nrows = rows * V;
+  za.tw_h = twp<T>(s, 1);
+  za.tw_n2 = twp<T>(s, 0);
+  GS_CU(launch_zfwd<T>(za, s->h, st), "z forward pass");
+  gs_mark(s, st);
+  YArgs<T> ya;
+  ya.spec = reinterpret_cast<cplx<T>*>(s->spec);
+  ya.n0 = s->n0;
+  ya.n1 = s->n1;
+  ya.h = s->h;
+  ya.tw = twp<T>(s, 2);
+  GS_CU(launch_ypass<T>(ya, s->n1, V, -1, st), "y forward pass");
+  if (s->n1 > 1) gs_mark(s, st);
+  XArgs<T> xa;
+  xa.in = reinterpret_cast<cplx<T>*>(s->spec);
+  xa.out = reinterpret_cast<cplx<T>*>(s->spec);
+  xa.n0 = s->n0;
+  xa.n1 = s->n1;
+  xa.n2 = s->n2;
+  xa.h = s->h;
+  xa.F = V;
+  xa.G = V;
+  for (int c = 0; c < 3; ++c) xa.perm[c] = s->perm[c];
+  xa.tw = twp<T>(s, 3);
+  build_elastic<T>(s, 0, 1.0 / (double)s->N, xa.ec);
+  GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
+  gs_mark(s, st);
+  GS_CU(launch_ypass<T>(ya, s->n1, V, 1, st), "y inverse pass");
+  if (s->n1 > 1) gs_mark(s, st);
+  s->launches += 2 + (s->n1 > 1 ? 2 : 0);
+  return GS_OK;
+}
+
+template <typename T> static void fill_mart_args(gs_sim* s, MartArgs<T>& ma, const T* in, T* out) {
+  memset(&ma, 0, sizeof(ma));
+  ma.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+  ma.eta_in = in;
+  ma.eta_out = out;
+  ma.defect = reinterpret_cast<const T*>(s->defect);
+  ma.K = reinterpret_cast<const T*>(s->K);
+  ma.n0 = s->n0;
+  ma.n1 = s->n1;
+  ma.n2 = s->n2;
+  ma.nrows = (long long)s->n0 * s->n1;
+  ma.tw_h = twp<T>(s, 1);
+  ma.tw_n2 = twp<T>(s, 0);
+  build_mart<T>(s, ma.mc);
+  ma.partials = s->partials;
+}
+
+template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {
+  T* in = reinterpret_cast<T*>(s->eta[s->cur]);
+  T* out = reinterpret_cast<T*>(s->eta[s->cur ^ 1]);
+  GS_TRY(elastic_chain<T>(s, in, st));
+  MartArgs<T> ma;
+  fill_mart_args<T>(s, ma, in, out);
+  GS_CU(launch_mart_update<T>(ma, s->h, false, st, nullptr), "update pass");
+  gs_mark(s, st);
+  s->launches += 1;
+  s->cur ^= 1;
+  s->step += 1;
+  return GS_OK;
+}
+
+template <typename T> static int mart_stats(gs_sim* s, gs_stats* o, cudaStream_t st) {
+  T* in = reinterpret_cast<T*>(s->eta[s->cur]);
+  GS_TRY(elastic_chain<T>(s, in, st));
+  MartArgs<T> ma;
+  fill_mart_args<T>(s, ma, in, nullptr);
+  int nb = 0;
+  GS_CU(launch_mart_update<T>(ma, s->h, true, st, &nb), "statistics pass");
+  GS_CU(launch_reduce(s->partials, nb, ACC_N, s->red, st), "reduce");
+  double acc[ACC_N];
+  GS_CU(cudaMemcpyAsync(acc, s->red, sizeof(acc), cudaMemcpyDeviceToHost, st), "stats D2H");
+  GS_CU(cudaStreamSynchronize(st), "stats sync");
+  const int V = s->p.nvariants;
+  const double N = (double)s->N;
+  const double dV = s->p.dx * s->p.dy * s->p.dz;
+  memset(o, 0, sizeof(*o));
+  o->mass = acc[ACC_MASS];
+  o->eta_mean = acc[ACC_MASS] / (N * V);
+  for (int v = 0; v < V; ++v) {
+    o->eta2[v] = acc[ACC_ETA2 + v] / N;
+    o->vf[v] = acc[ACC_VF + v] / N;
+  }
+  o->e_el = acc[ACC_EEL] * dV;
+  o->e_chem = acc[ACC_ECHEM] * dV;
+  o->e_grad = acc[ACC_EGRAD] * dV;
+  o->e_appl = acc[ACC_EAPPL] * dV;
+  o->e_tot = o->e_el + o->e_chem + o->e_grad + o->e_appl;
+  o->gradient_mean = acc[ACC_FGRAD] / (N * V);
+  o->chemical_mean = acc[ACC_FCHEM] / (N * V);
+  o->elastic_mean = acc[ACC_FEL] / (N * V);
+  o->dislocation_mean = acc[ACC_FDISL] / (N * V);
+  o->step = s->step;
+  return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// lifecycle
+// ---------------------------------------------------------------------------
+static size_t elt(const gs_sim* s) { return s->p.dtype == GS_DTYPE_F64 ? 8 : 4; }
+
+static void free_sim(gs_sim* s) {
+  if (!s) return;
+  void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->tw, s->partials, s->red};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (s->own_stream) cudaStreamDestroy(s->own_stream);
+  for (int i = 0; i < gs_sim::kMaxMarks; ++i)
+    if (s->marks[i]) cudaEventDestroy(s->marks[i]);
+  gs_plain_free(s);
+  delete s;
+}
+
+extern "C" int gs_sim_create(const gs_params* p, gs_sim** out) {
+  if (!p || !out) return gs_set_error(GS_EINVAL, "gs_sim_create: null argument");
+  *out = nullptr;
+  if (p->model != GS_MODEL_MART) return gs_set_error(GS_ENOTSUP, "model %d not available in this build", p->model);
+  if (p->nvariants < 1 || p->nvariants > GS_MAX_V)
+    return gs_set_error(GS_EINVAL, "nvariants %d outside 1..%d", p->nvariants, GS_MAX_V);
+  if (p->dtype != GS_DTYPE_F32 && p->dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", p->dtype);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return gs_set_error(GS_ENODEV, "no CUDA device visible");
+  }
+  gs_sim* s = new gs_sim();
+  s->p = *p;
+  int rc = canonicalize(s);
+  if (rc != GS_OK) {
+    delete s;
+    return rc;
+  }
+  const size_t fb = (size_t)s->N * elt(s);
+  const int V = p->nvariants;
+  auto fail = [&](int code) {
+    free_sim(s);
+    return code;
+  };
+  if ((rc = gs_cuda_check(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking), "stream")) != GS_OK)
+    return fail(rc);
+  for (int i = 0; i < 2; ++i) {
+    if ((rc = gs_cuda_check(cudaMalloc(&s->eta[i], fb * V), "cudaMalloc eta")) != GS_OK) return fail(rc);
+    if ((rc = gs_cuda_check(cudaMemset(s->eta[i], 0, fb * V), "memset eta")) != GS_OK) return fail(rc);
+  }
+  if ((rc = gs_cuda_check(cudaMalloc(&s->spec, fb * V), "cudaMalloc spectrum")) != GS_OK) return fail(rc);
+  rc = p->dtype == GS_DTYPE_F64 ? build_twiddles<double>(s) : build_twiddles<float>(s);
+  if (rc != GS_OK) return fail(rc);
+  s->partials_cap = (size_t)s->n0 * s->n1 + 1;
+  if ((rc = gs_cuda_check(cudaMalloc(&s->partials, s->partials_cap * ACC_N * sizeof(double)), "partials")) != GS_OK)
+    return fail(rc);
+  if ((rc = gs_cuda_check(cudaMalloc(&s->red, 64 * sizeof(double)), "reduce out")) != GS_OK) return fail(rc);
+  *out = s;
+  return GS_OK;
+}
+
+extern "C" int gs_sim_destroy(gs_sim* s) {
+  if (!s) return GS_OK;
+  cudaDeviceSynchronize();
+  free_sim(s);
+  return GS_OK;
+}
+
+template <typename T> static std::vector<T> to_type(const void* host, size_t count, int dtype) {
+  std::vector<T> v(count);
+  if (dtype == GS_DTYPE_F64) {
+    const double* h = static_cast<const double*>(host);
+    for (size_t i = 0; i < count; ++i) v[i] = (T)h[i];
+  } else {
+    const float* h = static_cast<const float*>(host);
+    for (size_t i = 0; i < count; ++i) v[i] = (T)h[i];
+  }
+  return v;
+}
+
+static int upload(gs_sim* s, void* dst, const void* host, size_t count, int dtype) {
+  const int want = s->p.dtype;
+  if (dtype == want) {
+    GS_CU(cudaMemcpy(dst, host, count * elt(s), cudaMemcpyHostToDevice), "upload");
+    return GS_OK;
+  }
+  if (want == GS_DTYPE_F64) {
+    auto v = to_type<double>(host, count, dtype);
+    GS_CU(cudaMemcpy(dst, v.data(), count * 8, cudaMemcpyHostToDevice), "upload");
+  } else {
+    auto v = to_type<float>(host, count, dtype);
+    GS_CU(cudaMemcpy(dst, v.data(), count * 4, cudaMemcpyHostToDevice), "upload");
+  }
+  return GS_OK;
+}
+
+static int download(gs_sim* s, const void* src, void* host, size_t count, int dtype) {
+  const int have = s->p.dtype;
+  if (dtype == have) {
+    GS_CU(cudaMemcpy(host, src, count * elt(s), cudaMemcpyDeviceToHost), "download");
+    return GS_OK;
+  }
+  if (have == GS_DTYPE_F64) {
+    std::vector<double> v(count);
+    GS_CU(cudaMemcpy(v.data(), src, count * 8, cudaMemcpyDeviceToHost), "download");
+    float* h = static_cast<float*>(host);
+    for (size_t i = 0; i < count; ++i) h[i] = (float)v[i];
+  } else {
+    std::vector<float> v(count);
+    GS_CU(cudaMemcpy(v.data(), src, count * 4, cudaMemcpyDeviceToHost), "download");
+    double* h = static_cast<double*>(host);
+    for (size_t i = 0; i < count; ++i) h[i] = (double)v[i];
+  }
+  return GS_OK;
+}
+
+extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, size_t count, int dtype) {
+  if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_set_field: null argument");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  const int V = s->p.nvariants;
+  const size_t N = (size_t)s->N;
+  const std::string nm(name);
+  if (nm == "eta") {
+    if (count != N * V) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, N * V);
+    return upload(s, s->eta[s->cur], host, count, dtype);
+  }
+  if (nm == "defect") {
+    if (count != N) return gs_set_error(GS_EINVAL, "defect: %zu values, expected %zu", count, N);
+    if (!s->defect) GS_CU(cudaMalloc(&s->defect, N * elt(s)), "cudaMalloc defect");
+    return upload(s, s->defect, host, count, dtype);
+  }
+  if (nm == "dislocationstress") {
+    // K_p(x) = sigma(x):eps_p from the 6-component form xx xy xz yy yz zz
+    // (the 3x3 remap of src/dynamics_mart.cu:128-150 and the contraction of
+    // DislocationForceInit, :305-321)
+    if (count != 6 * N) return gs_set_error(GS_EINVAL, "dislocationstress: %zu values, expected %zu", count, 6 * N);
+    std::vector<double> sig(6 * N);
+    if (dtype == GS_DTYPE_F64)
+      memcpy(sig.data(), host, 6 * N * 8);
+    else
+      for (size_t i = 0; i < 6 * N; ++i) sig[i] = static_cast<const float*>(host)[i];
+    std::vector<double> K(N * V);
+    for (int v = 0; v < V; ++v) {
+      const double(*e)[3] = s->p.eigenstrain[v];
+      for (size_t i = 0; i < N; ++i) {
+        const double xx = sig[0 * N + i], xy = sig[1 * N + i], xz = sig[2 * N + i];
+        const double yy = sig[3 * N + i], yz = sig[4 * N + i], zz = sig[5 * N + i];
+        K[v * N + i] = xx * e[0][0] + xy * (e[0][1] + e[1][0]) + xz * (e[0][2] + e[2][0]) + yy * e[1][1] +
+                       yz * (e[1][2] + e[2][1]) + zz * e[2][2];
+      }
+    }
+    if (!s->K) GS_CU(cudaMalloc(&s->K, N * V * elt(s)), "cudaMalloc K");
+    return upload(s, s->K, K.data(), N * V, GS_DTYPE_F64);
+  }
+  return gs_set_error(GS_EINVAL, "unknown field '%s'", name);
+}
+
+extern "C" int gs_sim_get_field(gs_sim* s, const char* name, void* host, size_t count, int dtype) {
+  if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_get_field: null argument");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  GS_CU(cudaStreamSynchronize(s->own_stream), "sync");
+  GS_CU(cudaDeviceSynchronize(), "sync");
+  const int V = s->p.nvariants;
+  const size_t N = (size_t)s->N;
+  const std::string nm(name);
+  if (nm == "eta") {
+    if (count != N * V) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, N * V);
+    return download(s, s->eta[s->cur], host, count, dtype);
+  }
+  if (nm == "defect") {
+    if (!s->defect) return gs_set_error(GS_EINVAL, "defect not set");
+    if (count != N) return gs_set_error(GS_EINVAL, "defect: %zu values, expected %zu", count, N);
+    return download(s, s->defect, host, count, dtype);
+  }
+  return gs_set_error(GS_EINVAL, "unknown field '%s'", name);
+}
+
+extern "C" int gs_sim_set_scalar(gs_sim* s, const char* name, double value) {
+  if (!s || !name) return gs_set_error(GS_EINVAL, "gs_sim_set_scalar: null argument");
+  const std::string nm(name);
+  if (nm == "temperature") {
+    s->p.temperature = value;
+    return GS_OK;
+  }
+  if (nm == "step") {
+    s->step = (int64_t)value;
+    return GS_OK;
+  }
+  return gs_set_error(GS_EINVAL, "unknown scalar '%s'", name);
+}
+
+static cudaStream_t pick_stream(gs_sim* s, void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : s->own_stream;
+}
+
+extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
+  if (!s) return gs_set_error(GS_EINVAL, "gs_sim_step: null sim");
+  if (nsteps < 0) return gs_set_error(GS_EINVAL, "nsteps %d", nsteps);
+  cudaStream_t st = pick_stream(s, stream);
+  s->launches = 0;
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = s->p.dtype == GS_DTYPE_F64 ? mart_step<double>(s, st) : mart_step<float>(s, st);
+    if (rc != GS_OK) return rc;
+  }
+  return GS_OK;
+}
+
+extern "C" int gs_sim_stats(gs_sim* s, gs_stats* out, void* stream) {
+  if (!s || !out) return gs_set_error(GS_EINVAL, "gs_sim_stats: null argument");
+  cudaStream_t st = pick_stream(s, stream);
+  return s->p.dtype == GS_DTYPE_F64 ? mart_stats<double>(s, out, st) : mart_stats<float>(s, out, st);
+}
+
+extern "C" int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes) {
+  if (!s || !name || !dptr) return gs_set_error(GS_EINVAL, "gs_sim_device_field: null argument");
+  const std::string nm(name);
+  const size_t fb = (size_t)s->N * elt(s);
+  if (nm == "eta") {
+    *dptr = s->eta[s->cur];
+    if (bytes) *bytes = fb * s->p.nvariants;
+    return GS_OK;
+  }
+  if (nm == "spectrum") {
+    *dptr = s->spec;
+    if (bytes) *bytes = fb * s->p.nvariants;
+    return GS_OK;
+  }
+  return gs_set_error(GS_EINVAL, "unknown device field '%s'", name);
+}
+
+extern "C" int64_t gs_sim_launch_count(const gs_sim* s) { return s ? s->launches : 0; }
+
+extern "C" int gs_sim_use_graph(gs_sim* s, int on) {
+  if (!s) return gs_set_error(GS_EINVAL, "null sim");
+  s->use_graph = on;
+  return GS_OK;
+}
+
+// instances used by the comparator translation unit
+template void build_elastic<float>(const gs_sim*, int, double, ElasticConst<float>&);
+template void build_elastic<double>(const gs_sim*, int, double, ElasticConst<double>&);
+template void build_mart<float>(const gs_sim*, MartConst<float>&);
+template void build_mart<double>(const gs_sim*, MartConst<double>&);
+
+extern "C" int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int max_pass, int* npass) {
+  if (!s || !pass_ms || !npass) return gs_set_error(GS_EINVAL, "gs_sim_profile_step: null argument");
+  cudaStream_t st = pick_stream(s, stream);
+  for (int i = 0; i < gs_sim::kMaxMarks; ++i)
+    if (!s->marks[i]) GS_CU(cudaEventCreate(&s->marks[i]), "event create");
+  s->nmarks = 0;
+  s->profiling = true;
+  gs_mark(s, st);
+  int rc = gs_sim_step(s, 1, stream);
+  s->profiling = false;
+  if (rc != GS_OK) return rc;
+  GS_CU(cudaEventSynchronize(s->marks[s->nmarks - 1]), "event sync");
+  const int n = s->nmarks - 1 < max_pass ? s->nmarks - 1 : max_pass;
+  for (int i = 0; i < n; ++i) {
+    float ms = 0;
+    GS_CU(cudaEventElapsedTime(&ms, s->marks[i], s->marks[i + 1]), "elapsed");
+    pass_ms[i] = ms;
+  }
+  *npass = n;
+  return GS_OK;
+}

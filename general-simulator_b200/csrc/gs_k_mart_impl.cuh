@@ -1,0 +1,44 @@
+// gs_k_mart_impl.cuh -- launcher template of the fused martensite update
+// (instantiated per dtype in its own translation unit).
+#pragma once
+#include "gs_launch.h"
+#include "gs_mart.cuh"
+
+namespace gs {
+
+template <typename T, int H, int VM, bool ST> cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks) {
+  using L = Line<T, H>;
+  const int per = L::P * a.mc.V;
+  long long lr = 256 / per;
+  if (lr < 1) lr = 1;
+  if (lr > a.nrows) lr = a.nrows;
+  a.lr = (int)lr;
+  const size_t smem = (size_t)lr * a.mc.V * L::PAD * sizeof(cplx<T>);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_mart_update<T, H, VM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long grid = (a.nrows + lr - 1) / lr;
+  if (nblocks) *nblocks = (int)grid;
+  k_mart_update<T, H, VM, ST><<<(unsigned)grid, (unsigned)(per * lr), smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaStream_t s, int* nb) {
+  if (a.mc.V <= 4)
+    return stats ? mu_n<T, H, 4, true>(a, s, nb) : mu_n<T, H, 4, false>(a, s, nb);
+  return stats ? mu_n<T, H, 8, true>(a, s, nb) : mu_n<T, H, 8, false>(a, s, nb);
+}
+
+template <typename T>
+cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks) {
+  switch (H) {
+#define GS_C(N_) \
+  case N_:       \
+    return mu_h<T, N_>(a, stats, s, nblocks);
+    GS_SIZE_CASES(GS_C)
+#undef GS_C
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace gs

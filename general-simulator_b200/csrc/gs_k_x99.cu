@@ -1,0 +1,6 @@
+// gs_k_x99.cu -- x pass instances for up to 9 fields.
+#include "gs_k_x_impl.cuh"
+namespace gs {
+template cudaError_t launch_x_class<float, 9, 9>(XArgs<float>&, cudaStream_t);
+template cudaError_t launch_x_class<double, 9, 9>(XArgs<double>&, cudaStream_t);
+}  // namespace gs

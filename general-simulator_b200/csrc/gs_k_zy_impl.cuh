@@ -1,0 +1,61 @@
+// gs_k_zy_impl.cuh -- launcher templates of the z-forward and y passes
+// (instantiated per dtype in its own translation unit).
+#pragma once
+#include "gs_launch.h"
+#include "gs_passes.cuh"
+
+namespace gs {
+
+template <typename K> static void allow_smem(K kernel, size_t smem) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStream_t s) {
+  using L = Line<T, H>;
+  long long lpc = 256 / L::P;
+  if (lpc < 1) lpc = 1;
+  if (lpc > a.nrows) lpc = a.nrows;
+  a.lpc = (int)lpc;
+  const size_t smem = (size_t)lpc * L::PAD * sizeof(cplx<T>);
+  allow_smem(k_zfwd<T, H>, smem);
+  const long long grid = (a.nrows + lpc - 1) / lpc;
+  k_zfwd<T, H><<<(unsigned)grid, (unsigned)(L::P * lpc), smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s) {
+  switch (H) {
+#define GS_C(N_) \
+  case N_:       \
+    return zfwd_n<T, N_>(a, s);
+    GS_SIZE_CASES(GS_C)
+#undef GS_C
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int N1, int DIR> static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s) {
+  using L = Line<T, N1>;
+  const size_t smem = (size_t)a.tz * L::PAD * sizeof(cplx<T>);
+  allow_smem(k_ypass<T, N1, DIR>, smem);
+  dim3 grid(a.h / a.tz, a.n0, F);
+  k_ypass<T, N1, DIR><<<grid, a.tz * L::P, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s) {
+  if (n1 == 1) return cudaSuccess;
+  a.tz = pick_tz(a.h);
+  switch (n1) {
+#define GS_C(N_) \
+  case N_:       \
+    return dir < 0 ? ypass_n<T, N_, -1>(a, F, s) : ypass_n<T, N_, 1>(a, F, s);
+    GS_SIZE_CASES(GS_C)
+#undef GS_C
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace gs

@@ -1,0 +1,30 @@
+// gs_launch.h -- host launchers of the pass kernels (one translation unit
+// per kernel family, dispatching the runtime line length to the compiled
+// template instance).
+#pragma once
+#include <cuda_runtime.h>
+#include "gs_common.cuh"
+
+namespace gs {
+
+template <typename T> struct ZfwdArgs;
+template <typename T> struct YArgs;
+template <typename T> struct XArgs;
+template <typename T> struct MartArgs;
+
+// line lengths with a compiled plan
+bool size_supported(int n);
+// columns per block of the y and x passes
+int pick_tz(int h);
+
+template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s);
+template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s);
+template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
+// returns the number of blocks through nblocks (statistics partial rows)
+template <typename T> cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks);
+cudaError_t launch_reduce(const double* partials, int nb, int n, double* out, cudaStream_t s);
+
+#define GS_SIZE_CASES(M) \
+  M(1) M(2) M(4) M(6) M(8) M(12) M(16) M(24) M(32) M(48) M(64) M(96) M(128) M(256)
+
+}  // namespace gs

@@ -1,0 +1,260 @@
+// gs_mart.cuh -- last sweep of the martensite step: z-axis C2R of the
+// elastic potential R_p fused with the explicit Euler TDGL update.
+//
+// Replaces, in one pass over the field set, the reference's Grad_Mart_Kernel
+// (src/dynamics_mart.cu:181-188), ChemiFor_Mart_Kernel (:222-250), the
+// elastic product -wE R eta (:291), the dislocation force (:326), the noise
+// (:372), the Euler update (:385) and Block_Mart_Kernel (:333-338), plus the
+// ~20 Data<T> expression sweeps between them (include/datamath.th).
+#pragma once
+#include "gs_passes.cuh"
+
+namespace gs {
+
+// FP64 accumulators of the statistics sweep
+enum {
+  ACC_MASS = 0, ACC_EEL, ACC_ECHEM, ACC_EGRAD, ACC_EAPPL,
+  ACC_FGRAD, ACC_FCHEM, ACC_FEL, ACC_FDISL, ACC_C,
+  ACC_ETA2 = 10,
+  ACC_VF = ACC_ETA2 + 8,
+  ACC_N = ACC_VF + 8
+};
+
+template <typename T> struct MartConst {
+  int V, refcompat, has_defect, has_K;
+  T dt;
+  T lapc[3];   // RHS stencil coefficient per canonical axis
+  T gcoef[3];  // 1/d^2 per canonical axis (gradient energy)
+  T A2, A4, A6, Ac, L, kappa;
+  T el;               // RHS += el * R_p * eta_p
+  T lin[8];           // RHS += lin_p * eta_p
+  T kc;               // RHS += kc * K_p(x) * eta_p
+  T a1, a2, a3, s, wC;  // refcompat chemical force
+  T noise;            // eta += noise * xi
+  T wel_half;         // energy: wel_half * eta^2 * R
+  T appl[8];          // energy: -(appl_p + wD K_p) eta_p^2
+  T wD;
+  uint32_t k0, k1, sim, step;
+};
+
+template <typename T> struct MartArgs {
+  const cplx<T>* spec;  // R spectra [V][n0][n1][h]
+  const T* eta_in;
+  T* eta_out;
+  const T* defect;  // [N] or null
+  const T* K;       // [V][N] or null
+  int n0, n1, n2, lr;
+  long long nrows;  // n0*n1
+  const cplx<T>* tw_h;
+  const cplx<T>* tw_n2;
+  MartConst<T> mc;
+  double* partials;  // [gridDim.x][ACC_N], statistics sweep only
+};
+
+struct Neu {  // Neumaier compensated sum (Neumaier 1974)
+  double s = 0, c = 0;
+  __device__ __forceinline__ void add(double x) {
+    const double t = s + x;
+    if (fabs(s) >= fabs(x))
+      c += (s - t) + x;
+    else
+      c += (x - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ double get() const { return s + c; }
+};
+
+// block sum of acc[0..n) into partials[blockIdx.x*n + i]
+__device__ __forceinline__ void block_reduce_store(Neu* acc, int n, double* out) {
+  __shared__ double red[32];
+  for (int i = 0; i < n; ++i) {
+    double v = acc[i].get();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int nw = (blockDim.x + 31) >> 5;
+      double w = threadIdx.x < nw ? red[threadIdx.x] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if (threadIdx.x == 0) out[(long long)blockIdx.x * n + i] = w;
+    }
+  }
+}
+
+// vector loads of CW consecutive values (CW = 2 or 4, 8/16-byte aligned)
+template <int CW> __device__ __forceinline__ void ldv(const float* p, float (&o)[CW]) {
+  if constexpr (CW == 4) {
+    const float4 x = *reinterpret_cast<const float4*>(p);
+    o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = x.w;
+  } else {
+    const float2 x = *reinterpret_cast<const float2*>(p);
+    o[0] = x.x; o[1] = x.y;
+  }
+}
+template <int CW> __device__ __forceinline__ void ldv(const double* p, double (&o)[CW]) {
+#pragma unroll
+  for (int j = 0; j < CW; j += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(p + j);
+    o[j] = x.x; o[j + 1] = x.y;
+  }
+}
+template <int CW> __device__ __forceinline__ void stv(float* p, const float (&o)[CW]) {
+  if constexpr (CW == 4)
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  else
+    *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+}
+template <int CW> __device__ __forceinline__ void stv(double* p, const double (&o)[CW]) {
+#pragma unroll
+  for (int j = 0; j < CW; j += 2) *reinterpret_cast<double2*>(p + j) = make_double2(o[j], o[j + 1]);
+}
+
+// One row group per block: the inverse z FFT of R_p for every (variant,
+// row) line leaves R in shared memory; then each thread updates a run of CW
+// cells (a quad, or a pair when n2 = 2) for all variants at once, so the
+// Landau coupling, the defect mask and one Philox block per variant serve
+// the whole run.
+template <typename T, int H, int VM, bool STATS>
+__global__ void k_mart_update(MartArgs<T> a) {
+  using L = Line<T, H>;
+  using V = cplx<T>;
+  constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* smb = reinterpret_cast<V*>(smraw);
+  const MartConst<T>& mc = a.mc;
+  const int Vn = mc.V;
+  {
+    const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
+    const int v = line % Vn, rr = line / Vn;
+    const long long row = (long long)blockIdx.x * a.lr + rr;
+    const bool act = rr < a.lr && row < a.nrows;
+    V* sl = smb + line * L::PAD;
+    const V* srow = a.spec + ((long long)v * a.nrows + (act ? row : 0)) * H;
+    V r[L::R1];
+    zinv_row<T, H>(srow, act, t, sl, a.tw_h, a.tw_n2, r);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = r[i];
+    __syncthreads();
+  }
+  Neu acc[STATS ? ACC_N : 1];
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const long long N = a.nrows * n2;
+  const int upr = n2 / CW;
+  const int nunits = a.lr * upr;
+#pragma unroll 1
+  for (int w = threadIdx.x; w < nunits; w += blockDim.x) {
+    const int rr = w / upr, u = w - rr * upr;
+    const long long row = (long long)blockIdx.x * a.lr + rr;
+    if (row >= a.nrows) continue;
+    const int x = (int)(row / n1), y = (int)(row - (long long)x * n1);
+    const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+    const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
+    const int z0 = u * CW;
+    const long long rowb = row * n2, cell = rowb + z0;
+    const long long oxp = ((long long)xp * n1 + y) * n2 + z0, oxm = ((long long)xm * n1 + y) * n2 + z0;
+    const long long oyp = ((long long)x * n1 + yp) * n2 + z0, oym = ((long long)x * n1 + ym) * n2 + z0;
+    const int zl = z0 == 0 ? n2 - 1 : z0 - 1, zr = z0 + CW == n2 ? 0 : z0 + CW;
+    T e[VM][CW];
+#pragma unroll
+    for (int q = 0; q < VM; ++q)
+      if (q < Vn) ldv<CW>(a.eta_in + (long long)q * N + cell, e[q]);
+    T s2[CW], s4[CW], pr[CW];
+#pragma unroll
+    for (int j = 0; j < CW; ++j) {
+      s2[j] = 0; s4[j] = 0; pr[j] = 0;
+#pragma unroll
+      for (int q = 0; q < VM; ++q)
+        if (q < Vn) {
+          const T e2 = e[q][j] * e[q][j];
+          pr[j] += s2[j] * e2;
+          s2[j] += e2;
+          s4[j] += e2 * e2;
+        }
+    }
+    T dfc[CW];
+    if (mc.has_defect) {
+      ldv<CW>(a.defect + cell, dfc);
+#pragma unroll
+      for (int j = 0; j < CW; ++j) dfc[j] = (T)1 - dfc[j];
+    }
+    T ssum[CW];
+    if (mc.refcompat) {
+#pragma unroll
+      for (int j = 0; j < CW; ++j) ssum[j] = mc.s * mc.s * s2[j];
+    }
+#pragma unroll
+    for (int q = 0; q < VM; ++q) {
+      if (q >= Vn) break;
+      const T* eq = a.eta_in + (long long)q * N;
+      T vxp[CW], vxm[CW], vyp[CW], vym[CW];
+      ldv<CW>(eq + oxp, vxp);
+      ldv<CW>(eq + oxm, vxm);
+      ldv<CW>(eq + oyp, vyp);
+      ldv<CW>(eq + oym, vym);
+      const T el_ = eq[rowb + zl], er_ = eq[rowb + zr];
+      const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
+      T Kq[CW];
+      if (mc.has_K) {
+        ldv<CW>(a.K + (long long)q * N + cell, Kq);
+      } else {
+#pragma unroll
+        for (int j = 0; j < CW; ++j) Kq[j] = 0;
+      }
+      T xi[4] = {0, 0, 0, 0};
+      if (!STATS && mc.noise != (T)0) normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
+      const int xo = (int)(cell & 3);
+      T out[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        const T et = e[q][j];
+        const T zlv = j == 0 ? el_ : e[q][j - 1];
+        const T zrv = j == CW - 1 ? er_ : e[q][j + 1];
+        const T d0 = vxp[j] + vxm[j] - 2 * et, d1 = vyp[j] + vym[j] - 2 * et, d2 = zlv + zrv - 2 * et;
+        const T grad = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;
+        T chem;
+        if (mc.refcompat) {
+          const T se = mc.s * et;
+          chem = et >= (T)0 ? -mc.wC * se * (mc.a1 - mc.a2 * se * se + mc.a3 * ssum[j])
+                            : (T)1000 * mc.wC * mc.a2 * et * et;
+        } else {
+          const T e2 = et * et;
+          chem = -mc.L * (mc.A2 * et - mc.A4 * e2 * et + mc.A6 * s2[j] * s2[j] * et + (T)2 * mc.Ac * et * (s2[j] - e2));
+        }
+        const T Rv = Rq[j];
+        const T el = mc.el * Rv * et;
+        const T lin = (mc.lin[q] + mc.kc * Kq[j]) * et;
+        const T rhs = grad + chem + el + lin;
+        T en = et + mc.dt * rhs + mc.noise * xi[(xo + j) & 3];
+        if (mc.has_defect) en *= dfc[j];
+        out[j] = en;
+        if (STATS) {
+          acc[ACC_MASS].add((double)et);
+          acc[ACC_ETA2 + q].add((double)et * (double)et);
+          acc[ACC_VF + q].add(fabs((double)et) > 0.5 ? 1.0 : 0.0);
+          acc[ACC_EEL].add((double)mc.wel_half * (double)et * (double)et * (double)Rv);
+          const double lg = (double)mc.gcoef[0] * d0 + (double)mc.gcoef[1] * d1 + (double)mc.gcoef[2] * d2;
+          acc[ACC_EGRAD].add(-0.5 * (double)mc.kappa * (double)et * lg);
+          acc[ACC_EAPPL].add(-((double)mc.appl[q] + (double)mc.wD * Kq[j]) * (double)et * (double)et);
+          if (q == 0)
+            acc[ACC_ECHEM].add((double)mc.A2 / 2 * s2[j] - (double)mc.A4 / 4 * s4[j] +
+                               (double)mc.A6 / 6 * (double)s2[j] * s2[j] * s2[j] + (double)mc.Ac * pr[j]);
+          acc[ACC_FGRAD].add((double)grad);
+          acc[ACC_FCHEM].add((double)chem);
+          acc[ACC_FEL].add((double)el);
+          acc[ACC_FDISL].add((double)lin);
+        }
+      }
+      if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
+    }
+  }
+  if (STATS) block_reduce_store(acc, ACC_N, a.partials);
+}
+
+// Sum per-block partials [nb][n] into out[n] with Neumaier compensation.
+__global__ void k_reduce_partials(const double* __restrict__ partials, int nb, int n, double* __restrict__ out);
+
+}  // namespace gs

@@ -1,0 +1,48 @@
+// gs_sim.h -- internal state of one simulation handle (gs_sim).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/gs_capi.h"
+
+struct gs_plain_state;  // cuFFT comparator buffers (gs_plain.cu)
+
+struct gs_sim {
+  gs_params p;
+  // canonical grid: unit axes moved to the front, n2 = last axis of extent > 1
+  int n0 = 1, n1 = 1, n2 = 2, h = 1;
+  long long N = 0;
+  int perm[3] = {0, 1, 2};  // canonical axis -> original axis
+  double dcan[3] = {1, 1, 1};
+  cudaStream_t own_stream = nullptr;
+  void* eta[2] = {nullptr, nullptr};  // ping-pong field set [V][N]
+  int cur = 0;
+  void* spec = nullptr;   // packed spectra [F][n0][n1][h]
+  void* spec2 = nullptr;  // second spectral buffer (stress output, CH chain)
+  void* defect = nullptr; // [N]
+  void* K = nullptr;      // dislocation coupling sigma(x):eps_p, [V][N]
+  void* conc = nullptr;   // concentration [N]
+  void* tw = nullptr;     // twiddle tables
+  size_t tw_off[4] = {0, 0, 0, 0};  // n2, h, n1, n0
+  double* partials = nullptr;
+  size_t partials_cap = 0;
+  double* red = nullptr;
+  int64_t step = 0;
+  int64_t launches = 0;
+  int use_graph = 0;
+  gs_plain_state* plain = nullptr;
+  // per-pass event marks of gs_sim_profile_step
+  static constexpr int kMaxMarks = 32;
+  cudaEvent_t marks[kMaxMarks] = {};
+  int nmarks = 0;
+  bool profiling = false;
+};
+
+// record a pass boundary when gs_sim_profile_step is active
+inline void gs_mark(gs_sim* s, cudaStream_t st) {
+  if (s->profiling && s->nmarks < gs_sim::kMaxMarks) cudaEventRecord(s->marks[s->nmarks++], st);
+}
+
+int gs_set_error(int code, const char* fmt, ...);
+int gs_cuda_check(cudaError_t e, const char* what);
+void gs_plain_free(gs_sim* s);

@@ -1,0 +1,339 @@
+"""ctypes binding of the B200-native phase-field step (include/gs_capi.h).
+
+The C ABI is the product boundary; this module only mirrors its POD structs
+and wraps the handles for Python callers (tests, bench.py, the calibration
+harness).  Loading fails loudly when libgsb200.so is missing: there is no
+Python or CPU fallback for the step.
+
+The reference drives the same work through GS_NS::Dynamics
+(src/dynamics.h:9-25); `Sim` mirrors that lifecycle: create = Initialize,
+step = Calculate, stats = Get.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgsb200.so")
+
+GS_OK = 0
+GS_MODEL_MART, GS_MODEL_PRECIPITATE, GS_MODEL_STRESS = 1, 2, 3
+GS_MODE_BASELINE, GS_MODE_REFCOMPAT = 0, 1
+GS_DTYPE_F32, GS_DTYPE_F64 = 0, 1
+GS_MAX_V = 8
+
+
+class GsParams(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("mode", C.c_int), ("dtype", C.c_int), ("nvariants", C.c_int),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
+        ("eigenstrain", C.c_double * 9 * GS_MAX_V),
+        ("cijkl", C.c_double * 81),
+        ("applied_stress", C.c_double * 9),
+        ("weight_elastic", C.c_double),
+        ("landau", C.c_double * 4), ("kappa", C.c_double), ("mobility", C.c_double),
+        ("weight_gradient", C.c_double), ("weight_chemical", C.c_double),
+        ("weight_dislocation", C.c_double), ("lpc", C.c_double * 4),
+        ("transition_temperature", C.c_double), ("temperature", C.c_double),
+        ("noise_amp", C.c_double), ("seed", C.c_uint64), ("sim_id", C.c_uint32), ("pad0", C.c_uint32),
+        ("coef", C.c_double * 8), ("c1", C.c_double), ("c2", C.c_double),
+        ("kappa_c", C.c_double), ("kappa_eta", C.c_double),
+        ("mobility_c", C.c_double), ("mobility_eta", C.c_double),
+        ("xi", C.c_double), ("misfit_c", C.c_double),
+        ("c_elastic", C.c_int), ("mass_projection", C.c_int),
+    ]
+
+    # numpy views of the array members
+    def set_eigenstrain(self, eps: np.ndarray) -> None:
+        eps = np.asarray(eps, dtype=np.float64).reshape(-1, 3, 3)
+        flat = np.zeros((GS_MAX_V, 9))
+        flat[: eps.shape[0]] = eps.reshape(-1, 9)
+        for v in range(GS_MAX_V):
+            for i in range(9):
+                self.eigenstrain[v][i] = flat[v, i]
+
+    def get_eigenstrain(self) -> np.ndarray:
+        return np.array([[self.eigenstrain[v][i] for i in range(9)] for v in range(self.nvariants)]).reshape(-1, 3, 3)
+
+    def set_cijkl(self, c: np.ndarray) -> None:
+        c = np.asarray(c, dtype=np.float64).reshape(81)
+        for i in range(81):
+            self.cijkl[i] = c[i]
+
+    def get_cijkl(self) -> np.ndarray:
+        return np.array([self.cijkl[i] for i in range(81)]).reshape(3, 3, 3, 3)
+
+    def set_applied_stress(self, s: np.ndarray) -> None:
+        s = np.asarray(s, dtype=np.float64).reshape(9)
+        for i in range(9):
+            self.applied_stress[i] = s[i]
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    @property
+    def ncells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def copy(self) -> "GsParams":
+        q = GsParams()
+        C.memmove(C.byref(q), C.byref(self), C.sizeof(GsParams))
+        return q
+
+
+class GsStats(C.Structure):
+    _fields_ = [
+        ("mass", C.c_double), ("eta_mean", C.c_double),
+        ("eta2", C.c_double * GS_MAX_V), ("vf", C.c_double * GS_MAX_V),
+        ("e_el", C.c_double), ("e_chem", C.c_double), ("e_grad", C.c_double),
+        ("e_appl", C.c_double), ("e_tot", C.c_double),
+        ("gradient_mean", C.c_double), ("chemical_mean", C.c_double),
+        ("elastic_mean", C.c_double), ("dislocation_mean", C.c_double),
+        ("c_mean", C.c_double), ("step", C.c_int64),
+    ]
+
+    def as_dict(self, nv: int) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("eta2", "vf")}
+        d["eta2"] = [self.eta2[i] for i in range(nv)]
+        d["vf"] = [self.vf[i] for i in range(nv)]
+        return d
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Load libgsb200.so (built in-tree by build.py); raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libgsb200.so not built at {LIB_PATH}; run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    P, S = C.POINTER(GsParams), C.POINTER(GsStats)
+    vp = C.c_void_p
+    sig = {
+        "gs_version": (C.c_int, []),
+        "gs_sizeof_params": (C.c_size_t, []),
+        "gs_sizeof_stats": (C.c_size_t, []),
+        "gs_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+        "gs_params_default": (C.c_int, [P, C.c_int, C.c_int]),
+        "gs_sim_create": (C.c_int, [P, C.POINTER(vp)]),
+        "gs_sim_destroy": (C.c_int, [vp]),
+        "gs_sim_set_field": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.c_int]),
+        "gs_sim_get_field": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.c_int]),
+        "gs_sim_set_scalar": (C.c_int, [vp, C.c_char_p, C.c_double]),
+        "gs_sim_step": (C.c_int, [vp, C.c_int, vp]),
+        "gs_sim_stats": (C.c_int, [vp, S, vp]),
+        "gs_sim_device_field": (C.c_int, [vp, C.c_char_p, C.POINTER(vp), C.POINTER(C.c_size_t)]),
+        "gs_sim_launch_count": (C.c_int64, [vp]),
+        "gs_sim_profile_step": (C.c_int, [vp, vp, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
+        "gs_sim_use_graph": (C.c_int, [vp, C.c_int]),
+        "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
+        "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().gs_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+class GsError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str) -> None:
+    if rc != GS_OK:
+        raise GsError(f"{what} failed with status {rc}: {last_error()}")
+
+
+def default_params(model: int, mode: int = GS_MODE_BASELINE) -> GsParams:
+    p = GsParams()
+    check(lib().gs_params_default(C.byref(p), model, mode), "gs_params_default")
+    return p
+
+
+def _np_dtype(code: int):
+    return np.float64 if code == GS_DTYPE_F64 else np.float32
+
+
+class Sim:
+    """One simulation handle (gs_sim*).  `plain=True` builds the cuFFT
+    comparator step instead of the hand-written one."""
+
+    def __init__(self, params: GsParams, plain: bool = False):
+        self.params = params.copy()
+        h = C.c_void_p()
+        if plain:
+            check(lib().gs_plain_create(C.byref(self.params), C.byref(h)), "gs_plain_create")
+        else:
+            check(lib().gs_sim_create(C.byref(self.params), C.byref(h)), "gs_sim_create")
+        self.h = h
+        self.plain = plain
+
+    def close(self) -> None:
+        if self.h:
+            lib().gs_sim_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_field(self, name: str, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr)
+        code = GS_DTYPE_F64 if a.dtype == np.float64 else GS_DTYPE_F32
+        a = np.ascontiguousarray(a, dtype=_np_dtype(code))
+        check(lib().gs_sim_set_field(self.h, name.encode(), a.ctypes.data, a.size, code), f"set_field({name})")
+
+    def get_field(self, name: str, count: int, dtype=np.float64) -> np.ndarray:
+        out = np.empty(count, dtype=dtype)
+        code = GS_DTYPE_F64 if dtype == np.float64 else GS_DTYPE_F32
+        check(lib().gs_sim_get_field(self.h, name.encode(), out.ctypes.data, count, code), f"get_field({name})")
+        return out
+
+    def eta(self, dtype=np.float64) -> np.ndarray:
+        p = self.params
+        return self.get_field("eta", p.nvariants * p.ncells, dtype).reshape(p.nvariants, p.nx, p.ny, p.nz)
+
+    def concentration(self, dtype=np.float64) -> np.ndarray:
+        p = self.params
+        return self.get_field("concentration", p.ncells, dtype).reshape(p.nx, p.ny, p.nz)
+
+    def set_scalar(self, name: str, value: float) -> None:
+        check(lib().gs_sim_set_scalar(self.h, name.encode(), float(value)), f"set_scalar({name})")
+
+    def step(self, n: int = 1, stream: int = 0) -> None:
+        if self.plain:
+            check(lib().gs_plain_step(self.h, n, C.c_void_p(stream)), "gs_plain_step")
+        else:
+            check(lib().gs_sim_step(self.h, n, C.c_void_p(stream)), "gs_sim_step")
+
+    def stats(self, stream: int = 0) -> dict:
+        s = GsStats()
+        check(lib().gs_sim_stats(self.h, C.byref(s), C.c_void_p(stream)), "gs_sim_stats")
+        return s.as_dict(self.params.nvariants)
+
+    def device_field(self, name: str):
+        ptr = C.c_void_p()
+        nb = C.c_size_t()
+        check(lib().gs_sim_device_field(self.h, name.encode(), C.byref(ptr), C.byref(nb)), "device_field")
+        return ptr.value, nb.value
+
+    def profile_step(self, stream: int = 0) -> list:
+        buf = (C.c_double * 32)()
+        n = C.c_int()
+        check(lib().gs_sim_profile_step(self.h, C.c_void_p(stream), buf, 32, C.byref(n)), "profile_step")
+        return [buf[i] for i in range(n.value)]
+
+    def launch_count(self) -> int:
+        return int(lib().gs_sim_launch_count(self.h))
+
+    def use_graph(self, on: bool) -> None:
+        check(lib().gs_sim_use_graph(self.h, 1 if on else 0), "use_graph")
+
+
+# ---------------------------------------------------------------------------
+# workload builders: the configurations the step is measured and tested on
+# ---------------------------------------------------------------------------
+
+def cubic_cijkl(c11: float, c12: float, c44: float) -> np.ndarray:
+    C4 = np.zeros((3, 3, 3, 3))
+    for i in range(3):
+        for j in range(3):
+            C4[i, i, j, j] = c12
+        C4[i, i, i, i] = c11
+    for i in range(3):
+        for j in range(3):
+            if i != j:
+                C4[i, j, i, j] = c44
+                C4[i, j, j, i] = c44
+    return C4
+
+
+def tetragonal_eigenstrains(nv: int, along: float, other: float) -> np.ndarray:
+    """Variant p: `along` on axis p mod 3, `other` on the two other axes."""
+    eps = np.zeros((nv, 3, 3))
+    for p in range(nv):
+        for a in range(3):
+            eps[p, a, a] = along if a == p % 3 else other
+    return eps
+
+
+def mart2d_params(n: int = 128, dtype: int = GS_DTYPE_F64) -> GsParams:
+    """2D square-to-rectangle martensite, 2 variants, FP64, 1000 explicit steps."""
+    p = default_params(GS_MODEL_MART, GS_MODE_BASELINE)
+    p.dtype = dtype
+    p.nvariants = 2
+    p.nx, p.ny, p.nz = n, n, 1
+    p.dx = p.dy = p.dz = 1.0
+    p.dt = 0.01
+    p.landau[0], p.landau[1], p.landau[2], p.landau[3] = 0.2, 3.0, 2.0, 1.0
+    p.kappa = 1.0
+    p.mobility = 1.0
+    eps = np.zeros((2, 3, 3))
+    eps[0, 0, 0], eps[0, 1, 1] = 0.02, -0.02
+    eps[1, 0, 0], eps[1, 1, 1] = -0.02, 0.02
+    p.set_eigenstrain(eps)
+    p.set_cijkl(cubic_cijkl(1.4, 0.84, 0.28))
+    p.set_applied_stress(np.zeros(9))
+    p.noise_amp = 0.0
+    p.seed = 0
+    return p
+
+
+def mart3d_params(n: int = 256, dtype: int = GS_DTYPE_F32, noise: float = 1e-3) -> GsParams:
+    """3D cubic-to-tetragonal martensite, 3 variants, sigma_zz = 0.005."""
+    p = default_params(GS_MODEL_MART, GS_MODE_BASELINE)
+    p.dtype = dtype
+    p.nvariants = 3
+    p.nx = p.ny = p.nz = n
+    p.dx = p.dy = p.dz = 1.0
+    p.dt = 0.005
+    p.landau[0], p.landau[1], p.landau[2], p.landau[3] = 0.2, 3.0, 2.0, 1.0
+    p.kappa = 0.5
+    p.mobility = 1.0
+    p.set_eigenstrain(tetragonal_eigenstrains(3, 0.02, -0.01))
+    p.set_cijkl(cubic_cijkl(1.4, 0.84, 0.56))
+    s = np.zeros((3, 3))
+    s[2, 2] = 0.005
+    p.set_applied_stress(s)
+    p.noise_amp = noise
+    p.seed = 1
+    return p
+
+
+def precip3d_params(n: int = 256, dtype: int = GS_DTYPE_F32) -> GsParams:
+    """3D precipitate: CH concentration + 4 AC variants, semi-implicit."""
+    p = default_params(GS_MODEL_PRECIPITATE, GS_MODE_BASELINE)
+    p.dtype = dtype
+    p.nvariants = 4
+    p.nx = p.ny = p.nz = n
+    return p
+
+
+def initial_eta(p: GsParams, seed: int, amp: float = 0.01) -> np.ndarray:
+    """eta ~ U[-amp, amp] from numpy's PCG64 with the given seed."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-amp, amp, size=(p.nvariants, p.nx, p.ny, p.nz))
+
+
+def initial_c(p: GsParams, seed: int, c0: float = 0.12, amp: float = 0.01) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return c0 + rng.uniform(-amp, amp, size=(p.nx, p.ny, p.nz))

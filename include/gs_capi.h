@@ -1,0 +1,190 @@
+/*
+ * gs_capi.h -- C ABI of the B200-native phase-field step of General-Simulator.
+ *
+ * The reference drives its physics through the C++ plugin class
+ * GS_NS::Dynamics (src/dynamics.h:9-25): Initialize / Calculate / RunFunc /
+ * Fix / Get, with parameters read from the string map Vars and fields from
+ * the Data<Real> map Datas.  The plugins that carry the hot path are
+ * Dynamics_mart (src/dynamics_mart.cu), Dynamics_precipitate
+ * (src/dynamics_precipitate.cu) and Dynamics_stress (src/dynamics_stress.cu).
+ *
+ * This header replaces what those plugins do on the device with plain C entry
+ * points: POD structs, host pointers and sizes, an int status, no exceptions
+ * and no C++ or torch types.  The C++ front end (the gsi script interpreter,
+ * host/ in this package) keeps the reference's Dynamics interface and calls
+ * these functions from Initialize / Calculate / Get.
+ *
+ * Field layout everywhere: [V][nx][ny][nz], z fastest (include/datamain.th:
+ * 72-76 in the reference).  Status codes 0 / -1 / -2 / -3 / -4 / -5 keep the
+ * meaning of the reference's Code_* constants (src/pub.h:17-22); the codes
+ * below -5 are new.
+ */
+#ifndef GS_CAPI_H
+#define GS_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_CAPI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define GS_OK 0             /* Code_NORMAL */
+#define GS_ERR (-1)         /* Code_ERR */
+#define GS_EINVAL (-10)     /* bad argument, size or field name */
+#define GS_ENOMEM (-11)     /* device allocation failed */
+#define GS_ECUDA (-12)      /* a CUDA call or launch failed */
+#define GS_ETIMEOUT (-13)   /* a bounded device wait gave up */
+#define GS_ENOTSUP (-14)    /* configuration not supported by the kernels */
+#define GS_ENODEV (-15)     /* no CUDA device visible */
+
+/* ---- enums ------------------------------------------------------------- */
+#define GS_MODEL_MART 1        /* Dynamics_mart: TDGL of V variants + FFT elasticity */
+#define GS_MODEL_PRECIPITATE 2 /* Dynamics_precipitate: CH(c) + AC(eta_p), semi-implicit */
+#define GS_MODEL_STRESS 3      /* Dynamics_stress: stress field of an eta configuration */
+
+/* GS_MODE_BASELINE: the discretisation written for this project (2-4-6
+ * Landau, kappa/dx^2 seven-point Laplacian, B(0)=0, k = 2*pi*m/(n*d)).
+ * GS_MODE_REFCOMPAT: the reference's own formulas (HEAD side): Laplacian
+ * divided by (2d)*3, the square-root Landau form of ChemiFor_Mart_Kernel,
+ * k = 2*3.14*d*m/n, B(0) = C:eps:eps, elastic force without the factor 2. */
+#define GS_MODE_BASELINE 0
+#define GS_MODE_REFCOMPAT 1
+
+#define GS_DTYPE_F32 0
+#define GS_DTYPE_F64 1
+
+#define GS_MAX_V 8
+
+/* ---- parameters -------------------------------------------------------- */
+typedef struct gs_params {
+  int model;     /* GS_MODEL_* */
+  int mode;      /* GS_MODE_* */
+  int dtype;     /* GS_DTYPE_*: storage and arithmetic type of the fields */
+  int nvariants; /* V, 1..GS_MAX_V */
+  int nx, ny, nz;
+  double dx, dy, dz;
+  double dt;
+
+  /* elasticity (all models): eigenstrain of each variant, C_ijkl, the
+   * applied (uniform) stress and a multiplier of the elastic driving force */
+  double eigenstrain[GS_MAX_V][3][3];
+  double cijkl[3][3][3][3];
+  double applied_stress[3][3];
+  double weight_elastic;
+
+  /* martensite, baseline: f = A2/2 S eta^2 - A4/4 S eta^4 + A6/6 (S eta^2)^3
+   * + Ac S_{p<q} eta_p^2 eta_q^2; d eta/dt = -L (df/deta - kappa lap eta +
+   * dE_el/deta - 2 sigma_a:eps_p eta_p) + noise */
+  double landau[4]; /* A2 A4 A6 Ac */
+  double kappa;
+  double mobility;
+
+  /* martensite, refcompat (src/dynamics_mart.cu:20-27,40,207-250) */
+  double weight_gradient, weight_chemical, weight_dislocation;
+  double lpc[4]; /* lpc[2], lpc[3]: a2, a3; a1 = 0.02 (T - T_tr) */
+  double transition_temperature;
+  double temperature;
+
+  /* noise: baseline adds noise_amp * xi to eta every step; refcompat adds
+   * dt * noise_amp * xi (weightnoise).  xi ~ N(0,1) from Philox4x32-10 with
+   * key (seed lo, seed hi) and counter (cell, step, sim_id, block). */
+  double noise_amp;
+  uint64_t seed;
+  uint32_t sim_id;
+  uint32_t pad0;
+
+  /* precipitate (src/dynamics_precipitate.cu:20-29,118-248): the local
+   * free-energy derivatives use coef[1..7] exactly as the reference's
+   * LocalCon/LocalEtaFreeEnergy kernels; baseline configs map onto them. */
+  double coef[8];
+  double c1, c2;          /* Concentration1, Concentration2 */
+  double kappa_c;         /* beta: gradient coefficient of c */
+  double kappa_eta;       /* arfi: gradient coefficient of eta */
+  double mobility_c;      /* meta */
+  double mobility_eta;    /* lpp */
+  double xi;              /* elastic scale Xi (precipitate and stress) */
+  double misfit_c;        /* dilatational eigenstrain per unit c (baseline) */
+  int c_elastic;          /* 1: c couples to elasticity through misfit_c */
+  int mass_projection;    /* 1: hold sum(c) at its FP64 initial value */
+} gs_params;
+
+/* FP64 statistics of the current state (compensated sums on the device). */
+typedef struct gs_stats {
+  double mass;            /* sum of c (precipitate) or of all eta (mart) */
+  double eta_mean;        /* mean of eta over V*N (reference "eta" key) */
+  double eta2[GS_MAX_V];  /* mean of eta_p^2 */
+  double vf[GS_MAX_V];    /* fraction of cells with |eta_p| > 0.5 */
+  double e_el;            /* elastic energy, dV/2 S_x S_p S_p R_p */
+  double e_chem;          /* local (Landau / chemical) energy */
+  double e_grad;          /* gradient energy */
+  double e_appl;          /* applied / dislocation stress energy */
+  double e_tot;
+  /* reference "info" keys (means of the force fields, src/dynamics_mart.cu:443-456) */
+  double gradient_mean, chemical_mean, elastic_mean, dislocation_mean;
+  double c_mean;
+  int64_t step;
+} gs_stats;
+
+typedef struct gs_sim gs_sim;
+
+/* ---- library ----------------------------------------------------------- */
+int gs_version(void);
+/* sizeof(gs_params) / sizeof(gs_stats) as compiled, for FFI layout checks. */
+size_t gs_sizeof_params(void);
+size_t gs_sizeof_stats(void);
+/* Copy the calling thread's last error message into buf. */
+int gs_last_error(char* buf, size_t len);
+/* Fill p with the defaults of model/mode (the reference's defaults for
+ * GS_MODE_REFCOMPAT, src/dynamics_mart.cu:20-27,80-89 and
+ * src/dynamics_precipitate.cu:21-29,55; the BASELINE configs otherwise). */
+int gs_params_default(gs_params* p, int model, int mode);
+
+/* ---- one simulation (replaces Dynamics_*::Initialize/Calculate/Get) ---- */
+/* Dynamics_*::Initialize: allocate device state for the grid; builds the
+ * per-direction B(n) constants (replaces GTensorB::InitB, src/gtensorb.cu:55-108). */
+int gs_sim_create(const gs_params* p, gs_sim** out);
+int gs_sim_destroy(gs_sim* s);
+/* Upload a host field.  Names: "eta" [V][nx][ny][nz]; "concentration"
+ * [nx][ny][nz]; "defect" [nx][ny][nz]; "dislocationstress" [6][nx][ny][nz]
+ * (xx xy xz yy yz zz, src/dynamics_mart.cu:128-150).  dtype is the type of
+ * the host buffer; count is its number of elements. */
+int gs_sim_set_field(gs_sim* s, const char* name, const void* host, size_t count, int dtype);
+/* Download a field: "eta", "concentration", "stress" [6][N], "defect",
+ * "elastic_potential" (R_p of the last step, [F][N]). */
+int gs_sim_get_field(gs_sim* s, const char* name, void* host, size_t count, int dtype);
+/* Per-step scalars read by Calculate: "temperature" (refcompat a1). */
+int gs_sim_set_scalar(gs_sim* s, const char* name, double value);
+/* Dynamics_*::Calculate, nsteps times, on stream (a cudaStream_t, NULL =
+ * the library's own stream).  Replaces src/dynamics_mart.cu:348-417,
+ * src/dynamics_precipitate.cu:278-289 and src/dynamics_stress.cu:179-194. */
+int gs_sim_step(gs_sim* s, int nsteps, void* stream);
+/* Dynamics_*::Get statistics of the current state, FP64. */
+int gs_sim_stats(gs_sim* s, gs_stats* out, void* stream);
+/* Device pointer of a resident field, for callers that keep data on the GPU. */
+int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes);
+/* Run one step with a CUDA event between consecutive passes on the step's
+ * stream; pass_ms[i] receives the device time of pass i (in launch order:
+ * z forward, y forward, x contraction, y inverse, update for the
+ * martensite step; y passes are absent when the middle axis is 1). */
+int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int max_pass, int* npass);
+/* Number of kernel launches issued by the last gs_sim_step call. */
+int64_t gs_sim_launch_count(const gs_sim* s);
+/* Make gs_sim_step replay a captured CUDA graph of one step (1) or launch
+ * the passes directly (0, default). */
+int gs_sim_use_graph(gs_sim* s, int on);
+
+/* ---- comparator: the same step with cuFFT C2C and unfused sweeps ------ */
+/* The plain GPU step in the reference's structure (cufftPlanMany C2C batch
+ * V, B streamed from a [V][V][N] array, one sweep per term); used only as a
+ * timed comparison, never on the product path. */
+int gs_plain_create(const gs_params* p, gs_sim** out);
+int gs_plain_step(gs_sim* s, int nsteps, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GS_CAPI_H */

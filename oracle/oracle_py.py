@@ -1,0 +1,137 @@
+"""ctypes wrapper of the FP64 CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline legs, as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "general-simulator_b200"))
+import gs_b200 as gb  # noqa: E402  (struct layouts shared with the C ABI)
+
+LIB = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            import subprocess
+            subprocess.run(["make", "-s", "-C", HERE], check=True)
+        L = C.CDLL(LIB)
+        P, S = C.POINTER(gb.GsParams), C.POINTER(gb.GsStats)
+        dp = C.POINTER(C.c_double)
+        L.or_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.or_normals4.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, dp]
+        L.or_fft3.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.or_bmat_at.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.or_mart_run.argtypes = [P, dp, dp, dp, C.c_int, C.c_int64]
+        L.or_mart_stats.argtypes = [P, dp, dp, dp, S]
+        L.or_mart_potential.argtypes = [P, dp, dp]
+        L.or_precip_run.argtypes = [P, dp, dp, C.c_int, C.c_int64]
+        L.or_precip_stats.argtypes = [P, dp, dp, S]
+        L.or_stress.argtypes = [P, dp, dp, dp]
+        L.or_set_threads.argtypes = [C.c_int]
+        L.or_get_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().or_philox4x32_10(c, k, o)
+    return [o[i] for i in range(4)]
+
+
+def normals4(seed, cell, step, sim, block):
+    z = np.zeros(4)
+    lib().or_normals4(seed, cell, step, sim, block, _dp(z))
+    return z
+
+
+def fft3(a: np.ndarray, sign: int) -> np.ndarray:
+    b = np.ascontiguousarray(a, dtype=np.complex128).copy()
+    n0, n1, n2 = b.shape
+    lib().or_fft3(b.ctypes.data_as(C.POINTER(C.c_double)), n0, n1, n2, sign)
+    return b
+
+
+def bmat(p: gb.GsParams, which: int, m) -> np.ndarray:
+    B = np.zeros(100)
+    na, nb = C.c_int(), C.c_int()
+    lib().or_bmat_at(C.byref(p), which, int(m[0]), int(m[1]), int(m[2]), _dp(B), C.byref(na), C.byref(nb))
+    return B[: na.value * nb.value].reshape(na.value, nb.value)
+
+
+def mart_run(p, eta, nsteps, step0=0, defect=None, dstress=None) -> np.ndarray:
+    e = _f64(eta).copy()
+    d = None if defect is None else _f64(defect)
+    s = None if dstress is None else _f64(dstress)
+    lib().or_mart_run(C.byref(p), _dp(e), _dp(d), _dp(s), nsteps, step0)
+    return e
+
+
+def mart_stats(p, eta, defect=None, dstress=None) -> dict:
+    st = gb.GsStats()
+    e = _f64(eta)
+    d = None if defect is None else _f64(defect)
+    s = None if dstress is None else _f64(dstress)
+    lib().or_mart_stats(C.byref(p), _dp(e), _dp(d), _dp(s), C.byref(st))
+    return st.as_dict(p.nvariants)
+
+
+def mart_potential(p, eta) -> np.ndarray:
+    e = _f64(eta)
+    R = np.zeros_like(e)
+    lib().or_mart_potential(C.byref(p), _dp(e), _dp(R))
+    return R
+
+
+def precip_run(p, c, eta, nsteps, step0=0):
+    cc = _f64(c).copy()
+    e = _f64(eta).copy()
+    lib().or_precip_run(C.byref(p), _dp(cc), _dp(e), nsteps, step0)
+    return cc, e
+
+
+def precip_stats(p, c, eta) -> dict:
+    st = gb.GsStats()
+    lib().or_precip_stats(C.byref(p), _dp(_f64(c)), _dp(_f64(eta)), C.byref(st))
+    return st.as_dict(p.nvariants)
+
+
+def stress(p, eta):
+    e = _f64(eta)
+    n = p.nx * p.ny * p.nz
+    s = np.zeros((6, n))
+    d = np.zeros(n)
+    lib().or_stress(C.byref(p), _dp(e), _dp(s), _dp(d))
+    return s.reshape(6, p.nx, p.ny, p.nz), d.reshape(p.nx, p.ny, p.nz)
+
+
+def set_threads(n: int) -> None:
+    lib().or_set_threads(n)
+
+
+def get_threads() -> int:
+    return lib().or_get_threads()

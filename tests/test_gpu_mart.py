@@ -1,0 +1,211 @@
+"""Parity of the CUDA martensite step (through the C ABI) with the FP64 oracle.
+
+Tolerances: FP64 fields agree to 1e-11 relative L2 (the two sides use
+different FFT algorithms); FP32 fields to 1e-6 relative L2 per step and 1e-5
+after tens of steps (BASELINE: 1e-6 per step, 1e-4 after 1000 steps).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+F64, F32 = 1, 0
+
+
+def gpu_run(gb, p, eta0, steps, defect=None, dstress=None, temperature=None, plain=False):
+    s = gb.Sim(p, plain=plain)
+    try:
+        s.set_field("eta", eta0)
+        if defect is not None:
+            s.set_field("defect", defect)
+        if dstress is not None:
+            s.set_field("dislocationstress", dstress)
+        if temperature is not None:
+            s.set_scalar("temperature", temperature)
+        s.step(steps)
+        return s.eta(np.float64)
+    finally:
+        s.close()
+
+
+def base3d(gb, shape, dtype, noise=0.0, V=3):
+    p = gb.mart3d_params(16, dtype=dtype, noise=noise)
+    p.nx, p.ny, p.nz = shape
+    if V != 3:
+        p.nvariants = V
+        p.set_eigenstrain(gb.tetragonal_eigenstrains(V, 0.02, -0.01))
+    return p
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (8, 16, 32), (12, 24, 48), (4, 8, 96), (32, 8, 4),
+                                   (16, 1, 16), (1, 1, 64), (6, 12, 24), (256, 2, 4), (2, 4, 512 // 2)])
+def test_fp64_matches_oracle(gb, orc, shape):
+    p = base3d(gb, shape, F64)
+    eta0 = gb.initial_eta(p, 11, 0.6)
+    ref = orc.mart_run(p, eta0, 3)
+    got = gpu_run(gb, p, eta0, 3)
+    assert rel_l2(got, ref) < 1e-11
+
+
+def test_fp64_2d_config1(gb, orc):
+    p = gb.mart2d_params(128, dtype=F64)
+    eta0 = gb.initial_eta(p, 0, 0.01)
+    ref = orc.mart_run(p, eta0, 50)
+    got = gpu_run(gb, p, eta0, 50)
+    assert rel_l2(got, ref) < 1e-11
+
+
+def test_fp64_large_amplitude_elastic_dominated(gb, orc):
+    p = base3d(gb, (16, 16, 16), F64)
+    p.weight_elastic = 1e3  # make the FFT-elasticity term large
+    eta0 = gb.initial_eta(p, 5, 1.0)
+    ref = orc.mart_run(p, eta0, 2)
+    got = gpu_run(gb, p, eta0, 2)
+    start = rel_l2(eta0, ref)
+    assert start > 1e-3  # the step moved the field
+    assert rel_l2(got, ref) < 1e-11
+
+
+@pytest.mark.parametrize("V", [1, 2, 4, 6])
+def test_fp64_variant_counts(gb, orc, V):
+    p = base3d(gb, (8, 8, 16), F64, V=V)
+    eta0 = gb.initial_eta(p, 3 + V, 0.5)
+    assert rel_l2(gpu_run(gb, p, eta0, 2), orc.mart_run(p, eta0, 2)) < 1e-11
+
+
+def test_fp32_one_step(gb, orc):
+    p = base3d(gb, (32, 32, 32), F32)
+    eta0 = gb.initial_eta(p, 1, 0.01)
+    ref = orc.mart_run(p, eta0, 1)
+    got = gpu_run(gb, p, eta0.astype(np.float32), 1)
+    assert rel_l2(got, ref) < 1e-6
+
+
+def test_fp32_many_steps(gb, orc):
+    p = base3d(gb, (32, 32, 32), F32)
+    eta0 = gb.initial_eta(p, 2, 0.5)
+    ref = orc.mart_run(p, eta0.astype(np.float32).astype(np.float64), 40)
+    got = gpu_run(gb, p, eta0.astype(np.float32), 40)
+    assert rel_l2(got, ref) < 1e-5
+
+
+def test_noise_fp64_same_bits(gb, orc):
+    p = base3d(gb, (8, 16, 16), F64, noise=1e-3)
+    p.seed = 0x123456789ABC
+    p.sim_id = 7
+    eta0 = gb.initial_eta(p, 4, 0.3)
+    ref = orc.mart_run(p, eta0, 3, step0=0)
+    got = gpu_run(gb, p, eta0, 3)
+    # noise moves each cell by ~1e-3; agreement far below that shows identical Philox bits
+    assert rel_l2(got, ref) < 1e-11
+
+
+def test_noise_fp32(gb, orc):
+    p = base3d(gb, (16, 16, 16), F32, noise=1e-3)
+    eta0 = gb.initial_eta(p, 9, 0.01).astype(np.float32)
+    ref = orc.mart_run(p, eta0.astype(np.float64), 2)
+    got = gpu_run(gb, p, eta0, 2)
+    assert rel_l2(got, ref) < 1e-6
+
+
+def test_defect_and_dislocation_field(gb, orc):
+    p = base3d(gb, (8, 8, 16), F64)
+    p.weight_dislocation = 3.0
+    rng = np.random.default_rng(3)
+    eta0 = gb.initial_eta(p, 8, 0.5)
+    defect = (rng.random((8, 8, 16)) < 0.1).astype(np.float64)
+    ds = rng.uniform(-0.01, 0.01, (6, 8, 8, 16))
+    ref = orc.mart_run(p, eta0, 2, defect=defect, dstress=ds)
+    got = gpu_run(gb, p, eta0, 2, defect=defect, dstress=ds)
+    assert rel_l2(got, ref) < 1e-11
+    assert np.all(got[:, defect > 0] == 0)
+
+
+def refcompat_params(gb, shape, dtype):
+    p = gb.default_params(gb.GS_MODEL_MART, gb.GS_MODE_REFCOMPAT)
+    p.dtype = dtype
+    p.nx, p.ny, p.nz = shape
+    p.dx = p.dy = p.dz = 0.2
+    p.nvariants = 4
+    t = 0.0063
+    eps = np.array([[[0, t, t], [t, 0, t], [t, t, 0]],
+                    [[0, t, -t], [t, 0, -t], [-t, -t, 0]],
+                    [[0, -t, t], [-t, 0, -t], [t, -t, 0]],
+                    [[0, -t, -t], [-t, 0, t], [-t, t, 0]]])
+    p.set_eigenstrain(eps)  # the variant tensor of scripts/in.mart
+    p.noise_amp = 0.0
+    p.temperature = 300.0
+    return p
+
+
+@pytest.mark.parametrize("dtype,tol", [(F64, 1e-11), (F32, 2e-6)])
+def test_refcompat_matches_oracle(gb, orc, dtype, tol):
+    p = refcompat_params(gb, (16, 16, 16), dtype)
+    p.weight_dislocation = 0.1
+    rng = np.random.default_rng(21)
+    eta0 = gb.initial_eta(p, 12, 0.3)
+    ds = rng.uniform(-0.05, 0.05, (6, 16, 16, 16))
+    defect = (rng.random((16, 16, 16)) < 0.05).astype(np.float64)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    ref = orc.mart_run(p, eta0, 3, defect=defect, dstress=ds)
+    got = gpu_run(gb, p, eta0, 3, defect=defect, dstress=ds)
+    assert rel_l2(got, ref) < tol
+
+
+def test_stats_match_oracle(gb, orc):
+    p = base3d(gb, (16, 16, 32), F64)
+    p.weight_dislocation = 2.0
+    rng = np.random.default_rng(5)
+    eta0 = gb.initial_eta(p, 13, 0.8)
+    ds = rng.uniform(-0.01, 0.01, (6, 16, 16, 32))
+    s = gb.Sim(p)
+    s.set_field("eta", eta0)
+    s.set_field("dislocationstress", ds)
+    st = s.stats()
+    s.close()
+    ref = orc.mart_stats(p, eta0, dstress=ds)
+    for k in ["mass", "eta_mean", "e_el", "e_chem", "e_grad", "e_appl", "e_tot", "gradient_mean",
+              "chemical_mean", "elastic_mean", "dislocation_mean"]:
+        assert abs(st[k] - ref[k]) <= 1e-10 * max(1.0, abs(ref[k])), k
+    assert np.allclose(st["eta2"], ref["eta2"], rtol=1e-12)
+    assert st["vf"] == ref["vf"]
+
+
+def test_stats_fp32_within_1e3(gb, orc):
+    p = base3d(gb, (32, 32, 32), F32)
+    eta0 = gb.initial_eta(p, 14, 0.8).astype(np.float32)
+    s = gb.Sim(p)
+    s.set_field("eta", eta0)
+    st = s.stats()
+    s.close()
+    ref = orc.mart_stats(p, eta0.astype(np.float64))
+    for k in ["mass", "e_el", "e_chem", "e_grad", "e_tot"]:
+        assert abs(st[k] - ref[k]) <= 1e-3 * abs(ref[k]) + 1e-9, k
+    assert np.allclose(st["vf"], ref["vf"], atol=1e-3)
+
+
+@pytest.mark.parametrize("dtype,tol", [(F64, 1e-11), (F32, 1e-6)])
+def test_plain_comparator_matches_oracle(gb, orc, dtype, tol):
+    p = base3d(gb, (16, 16, 16), dtype, noise=1e-3)
+    eta0 = gb.initial_eta(p, 15, 0.4)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    ref = orc.mart_run(p, eta0, 2)
+    got = gpu_run(gb, p, eta0, 2, plain=True)
+    assert rel_l2(got, ref) < tol
+
+
+def test_step_counter_continues_noise_stream(gb, orc):
+    p = base3d(gb, (8, 8, 8), F64, noise=1e-2)
+    eta0 = gb.initial_eta(p, 16, 0.2)
+    ref = orc.mart_run(p, eta0, 4)
+    s = gb.Sim(p)
+    s.set_field("eta", eta0)
+    s.step(1)
+    s.step(3)
+    got = s.eta()
+    s.close()
+    assert rel_l2(got, ref) < 1e-11

@@ -1,0 +1,126 @@
+"""The FP64 oracle against independent references: numpy.fft, Philox4x32-10
+known answers, closed-form B(n), analytic Landau and linear-mode dynamics."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (1, 16, 12), (4, 6, 10), (1, 1, 16), (3, 5, 7), (12, 24, 6)])
+def test_fft3_matches_numpy(orc, shape):
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    f = orc.fft3(a, -1)
+    assert rel_l2(f, np.fft.fftn(a)) < 1e-13
+    b = orc.fft3(f, +1) / a.size
+    assert rel_l2(b, a) < 1e-13
+
+
+def test_philox_known_answers(orc):
+    # Random123 philox4x32-10 known-answer vectors (Salmon et al., SC'11)
+    assert orc.philox([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    f = 0xFFFFFFFF
+    assert orc.philox([f, f, f, f], [f, f]) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert orc.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0]) == [
+        0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_normals_statistics(orc):
+    z = np.array([orc.normals4(7, i, 3, 0, 0) for i in range(20000)]).ravel()
+    assert abs(z.mean()) < 0.02
+    assert abs(z.std() - 1.0) < 0.02
+
+
+def test_bmat_isotropic_closed_form(gb, orc):
+    # isotropic C with a dilatational eigenstrain e*I: B(n) = 2 mu (1+nu)/(1-nu) (3e)^2 ... in
+    # Khachaturyan's form B = C:e:e - n.s.Omega.s.n; for lam, mu: B = 18 K mu e^2 / (lam + 2 mu) * ...
+    lam, mu, e = 1.2, 0.7, 0.01
+    C4 = np.zeros((3, 3, 3, 3))
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                for l in range(3):
+                    C4[i, j, k, l] = lam * (i == j) * (k == l) + mu * ((i == k) * (j == l) + (i == l) * (j == k))
+    p = gb.default_params(gb.GS_MODEL_MART, gb.GS_MODE_BASELINE)
+    p.nvariants = 1
+    p.nx = p.ny = p.nz = 16
+    p.set_cijkl(C4)
+    p.set_eigenstrain(np.eye(3)[None] * e)
+    Kb = lam + 2 * mu / 3
+    # sigma0 = 3 K e I; B(n) = C:e:e - (3Ke)^2 / (lam + 2 mu), independent of n
+    expect = 9 * Kb * e * e - (3 * Kb * e) ** 2 / (lam + 2 * mu)
+    for m in [(1, 0, 0), (0, 3, 2), (5, -4, 1), (-8, 7, -3)]:
+        B = orc.bmat(p, 0, m)
+        assert abs(B[0, 0] - expect) < 1e-14 * max(1, abs(expect)) + 1e-16
+    assert orc.bmat(p, 0, (0, 0, 0))[0, 0] == 0.0  # baseline B(0) = 0
+
+
+def test_bmat_symmetric_even(gb, orc):
+    p = gb.mart3d_params(16)
+    for m in [(1, 2, 3), (-5, 4, 0), (7, -1, -6)]:
+        B = orc.bmat(p, 0, m)
+        assert np.allclose(B, B.T, atol=1e-18)
+        assert np.allclose(B, orc.bmat(p, 0, tuple(-x for x in m)), atol=1e-18)
+
+
+def _uniform_eta(p, vals):
+    return np.broadcast_to(np.asarray(vals, dtype=np.float64)[:, None, None, None],
+                           (p.nvariants, p.nx, p.ny, p.nz)).copy()
+
+
+def test_mart_uniform_landau_ode(gb, orc):
+    # uniform fields: no gradient, B(0)=0 -> pure Landau ODE with the applied stress term
+    p = gb.mart3d_params(8, noise=0.0)
+    vals = np.array([0.3, -0.1, 0.05])
+    eta = _uniform_eta(p, vals)
+    out = orc.mart_run(p, eta, 5)
+    A2, A4, A6, Ac = (p.landau[i] for i in range(4))
+    sa = np.array([0.0, 0.0, 0.005])
+    v = vals.copy()
+    for _ in range(5):
+        s2 = (v * v).sum()
+        fp = A2 * v - A4 * v ** 3 + A6 * s2 * s2 * v + 2 * Ac * v * (s2 - v * v)
+        eps = p.get_eigenstrain()
+        lin = 2 * np.array([np.sum(np.diag(sa) * eps[q]) for q in range(3)])
+        v = v + p.dt * (-p.mobility) * (fp - lin * v)
+    assert np.allclose(out[:, 0, 0, 0], v, rtol=1e-13, atol=1e-16)
+    assert np.allclose(out, out[:, :1, :1, :1], atol=1e-15)
+
+
+def test_mart_single_mode_linear_growth(gb, orc):
+    # small single Fourier mode: eta(t+dt) = (1 - dt L (A2 + kappa K(k))) eta for the 7-point symbol
+    p = gb.mart3d_params(16, noise=0.0)
+    p.set_applied_stress(np.zeros(9))
+    n = 16
+    x = np.arange(n)
+    amp = 1e-7
+    mode = amp * np.cos(2 * np.pi * 3 * x / n)[:, None, None] * np.ones((n, n, n))
+    eta = np.zeros((3, n, n, n))
+    eta[1] = mode
+    out = orc.mart_run(p, eta, 1)
+    K = 4 * math.sin(math.pi * 3 / n) ** 2
+    expect = (1 - p.dt * p.mobility * (p.landau[0] + p.kappa * K)) * mode
+    assert rel_l2(out[1], expect) < 1e-6  # nonlinear terms are O(amp^2)
+
+
+def test_precip_mass_conserved(gb, orc):
+    p = gb.precip3d_params(16, dtype=gb.GS_DTYPE_F64)
+    c = gb.initial_c(p, 2)
+    eta = gb.initial_eta(p, 3, 0.1)
+    m0 = c.sum()
+    c1, e1 = orc.precip_run(p, c, eta, 3)
+    assert abs(c1.sum() - m0) / m0 < 1e-12
+    assert np.isfinite(e1).all()
+
+
+def test_stress_uniform_eta_is_zero_baseline(gb, orc):
+    p = gb.default_params(gb.GS_MODEL_STRESS, gb.GS_MODE_BASELINE)
+    p.nx = p.ny = p.nz = 8
+    p.nvariants = 2
+    p.set_eigenstrain(gb.tetragonal_eigenstrains(2, 0.01, -0.005))
+    eta = _uniform_eta(p, [0.5, 0.2])
+    s, d = orc.stress(p, eta)
+    assert np.abs(s).max() < 1e-15  # B(0) = 0: a uniform field is stress free
+    assert d.max() == 0.0
