@@ -256,25 +256,44 @@ static void strain_sets(const gs_params& p, int which, double (*ea)[3][3], int* 
   *na = *nb = F;
 }
 
+// B(n) is invariant under a relabelling of the axes applied to n, C and the
+// strains together, so the constants are expressed in the canonical axis
+// order (canonical axis c = original axis perm[c]) and the kernels use the
+// canonical wave vector directly.
 template <typename T> void build_elastic(const gs_sim* s, int which, double scale, ElasticConst<T>& ec) {
   const gs_params& p = s->p;
-  double ea[GS_MAXG + 1][3][3], eb[GS_MAXF + 1][3][3];
+  double ea0[GS_MAXG + 1][3][3], eb0[GS_MAXF + 1][3][3];
   int na, nb;
-  strain_sets(p, which, ea, &na, eb, &nb);
+  strain_sets(p, which, ea0, &na, eb0, &nb);
+  const int* pm = s->perm;
+  double ea[GS_MAXG + 1][3][3], eb[GS_MAXF + 1][3][3], C[3][3][3][3];
+  for (int a = 0; a < na; ++a)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) ea[a][i][j] = ea0[a][pm[i]][pm[j]];
+  for (int b = 0; b < nb; ++b)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) eb[b][i][j] = eb0[b][pm[i]][pm[j]];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) C[i][j][k][l] = p.cijkl[pm[i]][pm[j]][pm[k]][pm[l]];
   memset(&ec, 0, sizeof(ec));
   ec.na = na;
   ec.nb = nb;
   ec.refcompat = p.mode == GS_MODE_REFCOMPAT;
-  const double(*C)[3][3][3] = p.cijkl;
+  // Omega^-1_ij = C_iklj n_k n_l on the six entries ij = 00 01 02 11 12 22,
+  // symmetrised over ij (exact for a modulus with the major and minor
+  // symmetries) and over kl (n_k n_l is symmetric)
   const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j)
-      for (int q = 0; q < 6; ++q) {
-        const int a = pa[q], b = pb[q];
-        double v = C[i][a][b][j];
-        if (a != b) v += C[i][b][a][j];
-        ec.q[i * 3 + j][q] = (T)v;
-      }
+  for (int e = 0; e < 6; ++e) {
+    const int i = pa[e], j = pb[e];
+    for (int q = 0; q < 6; ++q) {
+      const int a = pa[q], b = pb[q];
+      double v = 0.5 * (C[i][a][b][j] + C[j][a][b][i]);
+      if (a != b) v += 0.5 * (C[i][b][a][j] + C[j][b][a][i]);
+      ec.qs[e][q] = (T)v;
+    }
+  }
   auto sig = [&](const double e[3][3], T out[3][3]) {
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) {
@@ -417,7 +436,6 @@ template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st
   xa.h = s->h;
   xa.F = V;
   xa.G = V;
-  for (int c = 0; c < 3; ++c) xa.perm[c] = s->perm[c];
   xa.tw = twp<T>(s, 3);
   build_elastic<T>(s, 0, 1.0 / (double)s->N, xa.ec);
   GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
@@ -443,6 +461,9 @@ template <typename T> static void fill_mart_args(gs_sim* s, MartArgs<T>& ma, con
   ma.tw_n2 = twp<T>(s, 0);
   build_mart<T>(s, ma.mc);
   ma.partials = s->partials;
+  ma.fd_n1 = FastDiv((uint32_t)s->n1);
+  ma.fd_upr = FastDiv((uint32_t)(s->n2 % 4 == 0 ? s->n2 / 4 : s->n2 / 2));
+  ma.fd_v = FastDiv((uint32_t)s->p.nvariants);
 }
 
 template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {

@@ -44,12 +44,26 @@ template <typename V> __host__ __device__ __forceinline__ V muli(V a) { return m
 template <typename T> struct ElasticConst {
   int na, nb;           // rows (outputs) and columns (inputs) of B
   int refcompat;        // B(0) = C:ea:eb and |k| <= 5e-7 test (reference rule)
-  T q[9][6];            // Omega^-1_ij = sum_{a<=b} q[ij][ab] n_a n_b
+  T qs[6][6];           // Omega^-1_e = sum_{a<=b} qs[e][ab] n_a n_b, e = 00 01 02 11 12 22
   T sa[GS_MAXG][3][3];  // sigma of the output set, C:ea
   T sb[GS_MAXF][3][3];  // sigma of the input set, C:eb
   T a0[GS_MAXG][GS_MAXF];  // C:ea:eb
   T kscale[3];          // k_axis = kscale * folded index
   T scale;              // multiplier of the contraction (1/N and field scales)
+};
+
+// Division by a runtime constant d with one multiply-high and a shift
+// (Granlund & Montgomery, PLDI'94, round-up variant); valid for n < 2^31.
+struct FastDiv {
+  uint32_t d = 1, m = 1, s = 0;
+  FastDiv() = default;
+  explicit FastDiv(uint32_t dv) : d(dv) {
+    uint32_t l = 0;
+    while ((1ull << l) < dv) ++l;
+    m = (uint32_t)(((1ull << 32) * ((1ull << l) - dv)) / dv + 1);
+    s = l;
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t n) const { return (__umulhi(n, m) + n) >> s; }
 };
 
 struct Geo {

@@ -6,16 +6,10 @@ namespace gs {
 
 template <typename T, int FM, int GM> cudaError_t launch_x_class(XArgs<T>& a, cudaStream_t s);
 
-cudaError_t launch_xreg_f32(XArgs<float>& a, cudaStream_t s, bool* done);
-
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s) {
-  if constexpr (sizeof(T) == 4) {
-    bool done = false;
-    cudaError_t e = launch_xreg_f32(a, s, &done);
-    if (done) return e;
-  }
-  if (a.F <= 4 && a.G <= 6) return launch_x_class<T, 4, 6>(a, s);
-  if (sizeof(T) == 4 && a.F <= 5 && a.G <= 5) return launch_x_class<T, 5, 5>(a, s);
+  if (a.F <= 3 && a.G <= 3) return launch_x_class<T, 3, 3>(a, s);
+  if (a.F <= 5 && a.G <= 5) return launch_x_class<T, 5, 5>(a, s);
+  if (a.F <= 8 && a.G <= 6) return launch_x_class<T, 8, 6>(a, s);
   return launch_x_class<T, 9, 9>(a, s);
 }
 

@@ -1,4 +1,4 @@
-// gs_k_x55.cu -- x pass instances for 5 fields (concentration + 4 variants).
+// gs_k_x55.cu -- x pass instances for up to 5 input and 5 output fields.
 #include "gs_k_x_impl.cuh"
 namespace gs {
 template cudaError_t launch_x_class<float, 5, 5>(XArgs<float>&, cudaStream_t);

@@ -1,4 +1,4 @@
-// gs_k_x99.cu -- x pass instances for up to 9 fields.
+// gs_k_x99.cu -- x pass instances for up to 9 input and 9 output fields.
 #include "gs_k_x_impl.cuh"
 namespace gs {
 template cudaError_t launch_x_class<float, 9, 9>(XArgs<float>&, cudaStream_t);

@@ -9,18 +9,33 @@ namespace gs {
 
 template <typename T, int N0, int FM, int GM> static cudaError_t xc_n(XArgs<T>& a, cudaStream_t s) {
   using L = Line<T, N0>;
-  const int nreg = a.F > a.G ? a.F : a.G;
+  const int groups = a.F > a.G ? a.F : a.G;
+  // 8-column tiles for the FP32 hot sizes: a 3-field block then needs 384
+  // threads x 80 registers, so two blocks share an SM and one block's
+  // contraction overlaps the other's loads and stores
   int tz = pick_tz(a.h);
-  size_t smem = (size_t)nreg * tz * L::PAD * sizeof(cplx<T>);
-  while (tz > 1 && smem > 200 * 1024) {
-    tz >>= 1;
-    smem = (size_t)nreg * tz * L::PAD * sizeof(cplx<T>);
-  }
+  if (sizeof(T) == 4 && N0 >= 64 && tz > 8) tz = 8;
+  auto smem_of = [&](int tzv) {
+    return (size_t)groups * tzv * L::PAD * sizeof(cplx<T>) + (size_t)GM * N0 * sizeof(cplx<T>);
+  };
+  constexpr int maxthr = XBounds<FM, GM>::v;
+  while (tz > 1 && (smem_of(tz) > 200 * 1024 || tz * L::P * groups > maxthr)) tz >>= 1;
+  if (tz * L::P * groups > maxthr) return cudaErrorInvalidConfiguration;
   a.tz = tz;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_xcontract<T, N0, FM, GM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  a.groups = groups;
+  const size_t smem = smem_of(tz);
   dim3 grid(a.h / tz, a.n1);
-  k_xcontract<T, N0, FM, GM><<<grid, tz * L::P, smem, s>>>(a);
+  if constexpr (sizeof(T) == 4 && N0 >= 64) {
+    if (tz == 8) {
+      if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_xpass<T, N0, FM, GM, 8><<<grid, tz * L::P * groups, smem, s>>>(a);
+      return cudaGetLastError();
+    }
+  }
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_xpass<T, N0, FM, GM, 0><<<grid, tz * L::P * groups, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -49,6 +49,7 @@ template <typename T> struct MartArgs {
   const cplx<T>* tw_n2;
   MartConst<T> mc;
   double* partials;  // [gridDim.x][ACC_N], statistics sweep only
+  FastDiv fd_n1, fd_upr, fd_v;  // y extent, update runs per row, variants
 };
 
 struct Neu {  // Neumaier compensated sum (Neumaier 1974)
@@ -144,112 +145,104 @@ __global__ void k_mart_update(MartArgs<T> a) {
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const long long N = a.nrows * n2;
   const int upr = n2 / CW;
-  const int nunits = a.lr * upr;
+  const int nunits = a.lr * Vn * upr;
+  // unit w -> (row rr, variant q, run u); runs of one (row, variant) are
+  // consecutive so neighbouring threads touch neighbouring cells
 #pragma unroll 1
   for (int w = threadIdx.x; w < nunits; w += blockDim.x) {
-    const int rr = w / upr, u = w - rr * upr;
+    const int rq = (int)a.fd_upr.div((uint32_t)w), u = w - rq * upr;
+    const int rr = (int)a.fd_v.div((uint32_t)rq), q = rq - rr * Vn;
     const long long row = (long long)blockIdx.x * a.lr + rr;
     if (row >= a.nrows) continue;
-    const int x = (int)(row / n1), y = (int)(row - (long long)x * n1);
+    const int x = (int)a.fd_n1.div((uint32_t)row), y = (int)(row - (long long)x * n1);
     const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
     const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
     const int z0 = u * CW;
     const long long rowb = row * n2, cell = rowb + z0;
-    const long long oxp = ((long long)xp * n1 + y) * n2 + z0, oxm = ((long long)xm * n1 + y) * n2 + z0;
-    const long long oyp = ((long long)x * n1 + yp) * n2 + z0, oym = ((long long)x * n1 + ym) * n2 + z0;
-    const int zl = z0 == 0 ? n2 - 1 : z0 - 1, zr = z0 + CW == n2 ? 0 : z0 + CW;
     T e[VM][CW];
 #pragma unroll
-    for (int q = 0; q < VM; ++q)
-      if (q < Vn) ldv<CW>(a.eta_in + (long long)q * N + cell, e[q]);
-    T s2[CW], s4[CW], pr[CW];
+    for (int p = 0; p < VM; ++p)
+      if (p < Vn) ldv<CW>(a.eta_in + (long long)p * N + cell, e[p]);
+    const T* eq = a.eta_in + (long long)q * N;
+    T vxp[CW], vxm[CW], vyp[CW], vym[CW], et_[CW];
+    ldv<CW>(eq + ((long long)xp * n1 + y) * n2 + z0, vxp);
+    ldv<CW>(eq + ((long long)xm * n1 + y) * n2 + z0, vxm);
+    ldv<CW>(eq + ((long long)x * n1 + yp) * n2 + z0, vyp);
+    ldv<CW>(eq + ((long long)x * n1 + ym) * n2 + z0, vym);
+    ldv<CW>(eq + cell, et_);
+    const T el_ = eq[rowb + (z0 == 0 ? n2 - 1 : z0 - 1)];
+    const T er_ = eq[rowb + (z0 + CW == n2 ? 0 : z0 + CW)];
+    const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
+    T Kq[CW], dfc[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
-      s2[j] = 0; s4[j] = 0; pr[j] = 0;
-#pragma unroll
-      for (int q = 0; q < VM; ++q)
-        if (q < Vn) {
-          const T e2 = e[q][j] * e[q][j];
-          pr[j] += s2[j] * e2;
-          s2[j] += e2;
-          s4[j] += e2 * e2;
-        }
+      Kq[j] = 0;
+      dfc[j] = 1;
     }
-    T dfc[CW];
+    if (mc.has_K) ldv<CW>(a.K + (long long)q * N + cell, Kq);
     if (mc.has_defect) {
       ldv<CW>(a.defect + cell, dfc);
 #pragma unroll
       for (int j = 0; j < CW; ++j) dfc[j] = (T)1 - dfc[j];
     }
-    T ssum[CW];
-    if (mc.refcompat) {
+    T xi[4] = {0, 0, 0, 0};
+    if (!STATS && mc.noise != (T)0) normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
+    const int xo = (int)(cell & 3);
+    T lq = 0;
 #pragma unroll
-      for (int j = 0; j < CW; ++j) ssum[j] = mc.s * mc.s * s2[j];
-    }
+    for (int p = 0; p < VM; ++p)
+      if (p == q) lq = mc.lin[p];
+    T out[CW];
 #pragma unroll
-    for (int q = 0; q < VM; ++q) {
-      if (q >= Vn) break;
-      const T* eq = a.eta_in + (long long)q * N;
-      T vxp[CW], vxm[CW], vyp[CW], vym[CW];
-      ldv<CW>(eq + oxp, vxp);
-      ldv<CW>(eq + oxm, vxm);
-      ldv<CW>(eq + oyp, vyp);
-      ldv<CW>(eq + oym, vym);
-      const T el_ = eq[rowb + zl], er_ = eq[rowb + zr];
-      const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
-      T Kq[CW];
-      if (mc.has_K) {
-        ldv<CW>(a.K + (long long)q * N + cell, Kq);
+    for (int j = 0; j < CW; ++j) {
+      T s2 = 0, s4 = 0, pr = 0;
+#pragma unroll
+      for (int p = 0; p < VM; ++p)
+        if (p < Vn) {
+          const T e2 = e[p][j] * e[p][j];
+          pr += s2 * e2;
+          s2 += e2;
+          s4 += e2 * e2;
+        }
+      const T et = et_[j];
+      const T zlv = j == 0 ? el_ : et_[j - 1];
+      const T zrv = j == CW - 1 ? er_ : et_[j + 1];
+      const T d0 = vxp[j] + vxm[j] - 2 * et, d1 = vyp[j] + vym[j] - 2 * et, d2 = zlv + zrv - 2 * et;
+      const T grad = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;
+      T chem;
+      if (mc.refcompat) {
+        const T se = mc.s * et;
+        chem = et >= (T)0 ? -mc.wC * se * (mc.a1 - mc.a2 * se * se + mc.a3 * mc.s * mc.s * s2)
+                          : (T)1000 * mc.wC * mc.a2 * et * et;
       } else {
-#pragma unroll
-        for (int j = 0; j < CW; ++j) Kq[j] = 0;
+        const T e2 = et * et;
+        chem = -mc.L * (mc.A2 * et - mc.A4 * e2 * et + mc.A6 * s2 * s2 * et + (T)2 * mc.Ac * et * (s2 - e2));
       }
-      T xi[4] = {0, 0, 0, 0};
-      if (!STATS && mc.noise != (T)0) normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
-      const int xo = (int)(cell & 3);
-      T out[CW];
-#pragma unroll
-      for (int j = 0; j < CW; ++j) {
-        const T et = e[q][j];
-        const T zlv = j == 0 ? el_ : e[q][j - 1];
-        const T zrv = j == CW - 1 ? er_ : e[q][j + 1];
-        const T d0 = vxp[j] + vxm[j] - 2 * et, d1 = vyp[j] + vym[j] - 2 * et, d2 = zlv + zrv - 2 * et;
-        const T grad = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;
-        T chem;
-        if (mc.refcompat) {
-          const T se = mc.s * et;
-          chem = et >= (T)0 ? -mc.wC * se * (mc.a1 - mc.a2 * se * se + mc.a3 * ssum[j])
-                            : (T)1000 * mc.wC * mc.a2 * et * et;
-        } else {
-          const T e2 = et * et;
-          chem = -mc.L * (mc.A2 * et - mc.A4 * e2 * et + mc.A6 * s2[j] * s2[j] * et + (T)2 * mc.Ac * et * (s2[j] - e2));
-        }
-        const T Rv = Rq[j];
-        const T el = mc.el * Rv * et;
-        const T lin = (mc.lin[q] + mc.kc * Kq[j]) * et;
-        const T rhs = grad + chem + el + lin;
-        T en = et + mc.dt * rhs + mc.noise * xi[(xo + j) & 3];
-        if (mc.has_defect) en *= dfc[j];
-        out[j] = en;
-        if (STATS) {
-          acc[ACC_MASS].add((double)et);
-          acc[ACC_ETA2 + q].add((double)et * (double)et);
-          acc[ACC_VF + q].add(fabs((double)et) > 0.5 ? 1.0 : 0.0);
-          acc[ACC_EEL].add((double)mc.wel_half * (double)et * (double)et * (double)Rv);
-          const double lg = (double)mc.gcoef[0] * d0 + (double)mc.gcoef[1] * d1 + (double)mc.gcoef[2] * d2;
-          acc[ACC_EGRAD].add(-0.5 * (double)mc.kappa * (double)et * lg);
-          acc[ACC_EAPPL].add(-((double)mc.appl[q] + (double)mc.wD * Kq[j]) * (double)et * (double)et);
-          if (q == 0)
-            acc[ACC_ECHEM].add((double)mc.A2 / 2 * s2[j] - (double)mc.A4 / 4 * s4[j] +
-                               (double)mc.A6 / 6 * (double)s2[j] * s2[j] * s2[j] + (double)mc.Ac * pr[j]);
-          acc[ACC_FGRAD].add((double)grad);
-          acc[ACC_FCHEM].add((double)chem);
-          acc[ACC_FEL].add((double)el);
-          acc[ACC_FDISL].add((double)lin);
-        }
+      const T Rv = Rq[j];
+      const T el = mc.el * Rv * et;
+      const T lin = (lq + mc.kc * Kq[j]) * et;
+      const T rhs = grad + chem + el + lin;
+      T en = et + mc.dt * rhs + mc.noise * xi[(xo + j) & 3];
+      if (mc.has_defect) en *= dfc[j];
+      out[j] = en;
+      if (STATS) {
+        acc[ACC_MASS].add((double)et);
+        acc[ACC_ETA2 + q].add((double)et * (double)et);
+        acc[ACC_VF + q].add(fabs((double)et) > 0.5 ? 1.0 : 0.0);
+        acc[ACC_EEL].add((double)mc.wel_half * (double)et * (double)et * (double)Rv);
+        const double lg = (double)mc.gcoef[0] * d0 + (double)mc.gcoef[1] * d1 + (double)mc.gcoef[2] * d2;
+        acc[ACC_EGRAD].add(-0.5 * (double)mc.kappa * (double)et * lg);
+        acc[ACC_EAPPL].add(-((double)mc.appl[q] + (double)mc.wD * Kq[j]) * (double)et * (double)et);
+        if (q == 0)
+          acc[ACC_ECHEM].add((double)mc.A2 / 2 * s2 - (double)mc.A4 / 4 * s4 +
+                             (double)mc.A6 / 6 * (double)s2 * s2 * s2 + (double)mc.Ac * pr);
+        acc[ACC_FGRAD].add((double)grad);
+        acc[ACC_FCHEM].add((double)chem);
+        acc[ACC_FEL].add((double)el);
+        acc[ACC_FDISL].add((double)lin);
       }
-      if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
     }
+    if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
   }
   if (STATS) block_reduce_store(acc, ACC_N, a.partials);
 }

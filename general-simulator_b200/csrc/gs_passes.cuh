@@ -37,8 +37,15 @@ __device__ __forceinline__ double gs_rsqrt(double x) { return 1.0 / sqrt(x); }
 __device__ __forceinline__ float gs_rcp(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double gs_rcp(double x) { return 1.0 / x; }
 
-// out[g] += w * sum_f B_gf(k) in[f], with B_gf = C:ea_g:eb_f - (n sigma_g)
-// Omega (sigma_f n) evaluated inside the sum.  k is in the original axes.
+// out[g] += w * sum_f B_gf(k) in[f] for the Khachaturyan
+//   B_gf(n) = C:ea_g:eb_f - (sigma_g n) . Omega(n) . (sigma_f n),
+//   Omega(n)^-1_ij = C_iklj n_k n_l,
+// evaluated as  out_g = sum_f a0_gf in_f - v_g . Omega (sum_f w_f in_f)
+// with w_f = sigma_f n, v_g = sigma_g n (sigma = C:eps is symmetric), so
+// no B entry is ever formed.  Omega^-1 is symmetric for a modulus with the
+// major and minor symmetries; its six entries and the cofactor inverse
+// follow src/gtensorb.cu:121-157 (|det| < 1e-8 -> Omega = 0 in the
+// reference's rule).  k and the constants are in the canonical axis order.
 template <typename T, int FM, int GM>
 __device__ __forceinline__ void contract_k(const ElasticConst<T>& ec, const T k[3], const cplx<T> (&in)[FM],
                                            cplx<T> (&out)[GM], T w) {
@@ -59,55 +66,46 @@ __device__ __forceinline__ void contract_k(const ElasticConst<T>& ec, const T k[
     n[2] = k[2] * im;
   }
   const T nn[6] = {n[0] * n[0], n[0] * n[1], n[0] * n[2], n[1] * n[1], n[1] * n[2], n[2] * n[2]};
-  T m[9];
+  T m[6];  // m00 m01 m02 m11 m12 m22
 #pragma unroll
-  for (int ij = 0; ij < 9; ++ij) {
+  for (int e = 0; e < 6; ++e) {
     T sacc = 0;
 #pragma unroll
-    for (int q = 0; q < 6; ++q) sacc += ec.q[ij][q] * nn[q];
-    m[ij] = sacc;
+    for (int q = 0; q < 6; ++q) sacc += ec.qs[e][q] * nn[q];
+    m[e] = sacc;
   }
-  const T det = -m[2] * m[4] * m[6] + m[1] * m[5] * m[6] + m[2] * m[3] * m[7] - m[0] * m[5] * m[7] -
-                m[1] * m[3] * m[8] + m[0] * m[4] * m[8];
-  T om[9];
+  const T c00 = m[3] * m[5] - m[4] * m[4], c01 = m[2] * m[4] - m[1] * m[5], c02 = m[1] * m[4] - m[2] * m[3];
+  const T c11 = m[0] * m[5] - m[2] * m[2], c12 = m[1] * m[2] - m[0] * m[4], c22 = m[0] * m[3] - m[1] * m[1];
+  const T det = m[0] * c00 + m[1] * c01 + m[2] * c02;
   const bool ok = ec.refcompat ? (det >= (T)1e-8 || det <= (T)-1e-8) : (det != (T)0);
-  if (ok) {
-    const T id = gs_rcp(det);
-    om[0] = (-m[5] * m[7] + m[4] * m[8]) * id;
-    om[1] = (m[2] * m[7] - m[1] * m[8]) * id;
-    om[2] = (-m[2] * m[4] + m[1] * m[5]) * id;
-    om[3] = (m[5] * m[6] - m[3] * m[8]) * id;
-    om[4] = (-m[2] * m[6] + m[0] * m[8]) * id;
-    om[5] = (m[2] * m[3] - m[0] * m[5]) * id;
-    om[6] = (-m[4] * m[6] + m[3] * m[7]) * id;
-    om[7] = (m[1] * m[6] - m[0] * m[7]) * id;
-    om[8] = (-m[1] * m[3] + m[0] * m[4]) * id;
-  } else {
-#pragma unroll
-    for (int i = 0; i < 9; ++i) om[i] = 0;
-  }
-  T wb[FM][3];
+  const T id = ok ? gs_rcp(det) : (T)0;
+  const T o00 = c00 * id, o01 = c01 * id, o02 = c02 * id, o11 = c11 * id, o12 = c12 * id, o22 = c22 * id;
+  // u = sum_f (sigma_f n) in_f
+  cplx<T> u0 = mk2((T)0, (T)0), u1 = u0, u2 = u0;
 #pragma unroll
   for (int f = 0; f < FM; ++f) {
-#pragma unroll
-    for (int i = 0; i < 3; ++i) wb[f][i] = ec.sb[f][i][0] * n[0] + ec.sb[f][i][1] * n[1] + ec.sb[f][i][2] * n[2];
+    if (f < ec.nb) {
+      const T w0 = ec.sb[f][0][0] * n[0] + ec.sb[f][0][1] * n[1] + ec.sb[f][0][2] * n[2];
+      const T w1 = ec.sb[f][1][0] * n[0] + ec.sb[f][1][1] * n[1] + ec.sb[f][1][2] * n[2];
+      const T w2 = ec.sb[f][2][0] * n[0] + ec.sb[f][2][1] * n[1] + ec.sb[f][2][2] * n[2];
+      u0 = u0 + in[f] * w0;
+      u1 = u1 + in[f] * w1;
+      u2 = u2 + in[f] * w2;
+    }
   }
+  const cplx<T> p0 = u0 * o00 + u1 * o01 + u2 * o02;
+  const cplx<T> p1 = u0 * o01 + u1 * o11 + u2 * o12;
+  const cplx<T> p2 = u0 * o02 + u1 * o12 + u2 * o22;
 #pragma unroll
   for (int g = 0; g < GM; ++g) {
     if (g < ec.na) {
-      T va[3], ova[3];
+      const T v0 = ec.sa[g][0][0] * n[0] + ec.sa[g][0][1] * n[1] + ec.sa[g][0][2] * n[2];
+      const T v1 = ec.sa[g][1][0] * n[0] + ec.sa[g][1][1] * n[1] + ec.sa[g][1][2] * n[2];
+      const T v2 = ec.sa[g][2][0] * n[0] + ec.sa[g][2][1] * n[1] + ec.sa[g][2][2] * n[2];
+      cplx<T> acc = mk2((T)0, (T)0) - (p0 * v0 + p1 * v1 + p2 * v2);
 #pragma unroll
-      for (int j = 0; j < 3; ++j) va[j] = n[0] * ec.sa[g][0][j] + n[1] * ec.sa[g][1][j] + n[2] * ec.sa[g][2][j];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) ova[c] = va[0] * om[0 * 3 + c] + va[1] * om[1 * 3 + c] + va[2] * om[2 * 3 + c];
-      cplx<T> acc = mk2((T)0, (T)0);
-#pragma unroll
-      for (int f = 0; f < FM; ++f) {
-        if (f < ec.nb) {
-          const T b = ec.a0[g][f] - (ova[0] * wb[f][0] + ova[1] * wb[f][1] + ova[2] * wb[f][2]);
-          acc = acc + in[f] * b;
-        }
-      }
+      for (int f = 0; f < FM; ++f)
+        if (f < ec.nb) acc = acc + in[f] * ec.a0[g][f];
       out[g] = out[g] + acc * w;
     }
   }
@@ -123,8 +121,8 @@ __device__ __forceinline__ int fold_idx(int i, int n, int refcompat) {
 // spectrum stays Hermitian (equal to the real part of the reference's C2C
 // inverse, which sees both signs through the conjugate partner).
 template <typename T, int FM, int GM>
-__device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int (&perm)[3], const int (&nn)[3],
-                                            int ix, int iy, int iz, const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+__device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int (&nn)[3], int ix, int iy, int iz,
+                                            const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
   const int id[3] = {ix, iy, iz};
   int m[3];
   bool nyq = false;
@@ -137,17 +135,15 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
   }
 #pragma unroll
   for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
-  T k[3];
+  const T w = nyq ? (T)0.5 * ec.scale : ec.scale;
+  const int trips = nyq ? 2 : 1;
+#pragma unroll 1
+  for (int trip = 0; trip < trips; ++trip) {
+    T k[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) k[perm[c]] = ec.kscale[c] * (T)m[c];
-  if (!nyq) {
-    contract_k<T, FM, GM>(ec, k, in, out, ec.scale);
-    return;
+    for (int c = 0; c < 3; ++c) k[c] = ec.kscale[c] * (T)((trip && isnyq[c]) ? -m[c] : m[c]);
+    contract_k<T, FM, GM>(ec, k, in, out, w);
   }
-  contract_k<T, FM, GM>(ec, k, in, out, (T)0.5 * ec.scale);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) k[perm[c]] = ec.kscale[c] * (T)(isnyq[c] ? -m[c] : m[c]);
-  contract_k<T, FM, GM>(ec, k, in, out, (T)0.5 * ec.scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -312,219 +308,134 @@ __global__ void k_ypass(YArgs<T> a) {
 
 // ---------------------------------------------------------------------------
 // x pass: forward x FFT of F fields -> B(n) contraction -> inverse x FFT of
-// G fields.  One block per (kz tile, ky slot).
+// G fields.  One block per (kz tile, ky slot); one thread group per field,
+// so the F line FFTs of a tile run side by side.  The spectra meet in
+// shared memory for the contraction, which every thread of the block shares.
 // ---------------------------------------------------------------------------
 template <typename T> struct XArgs {
   const cplx<T>* in;  // [F][n0][n1][h]
-  cplx<T>* out;       // [G][n0][n1][h] (may alias in when G <= F)
-  int n0, n1, n2, h, tz, F, G;
-  int perm[3];
+  cplx<T>* out;       // [G][n0][n1][h] (may alias in)
+  int n0, n1, n2, h, tz, F, G, groups;
   const cplx<T>* tw;  // w_n0^m
   ElasticConst<T> ec;
 };
 
-template <typename T, int N0, int FM, int GM>
-__global__ void k_xcontract(XArgs<T> a) {
+// threads per block of the x pass for a field-count class (FM, GM)
+template <int FM, int GM> struct XBounds {
+  static constexpr int G = FM > GM ? FM : GM;
+  static constexpr int v = G <= 3 ? 768 : (G <= 5 ? 640 : 1024);
+};
+
+template <typename T, int N0, int FM, int GM, int TZC>
+__global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   using L = Line<T, N0>;
   using V = cplx<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* smb = reinterpret_cast<V*>(smraw);
-  const int TZ = a.tz;
-  const int c = threadIdx.x % TZ, t = threadIdx.x / TZ;
+  const int TZ = TZC ? TZC : a.tz;  // compile-time tile width when TZC > 0
+  const int gsz = TZ * L::P;
+  const int grp = threadIdx.x / gsz, l = threadIdx.x - grp * gsz;
+  const int c = l % TZ, t = l / TZ;
   const int kz0 = blockIdx.x * TZ, ky = blockIdx.y;
-  const int h = a.h, n1 = a.n1;
+  const int h = a.h, n1 = a.n1, HH = n1 / 2;
   const long long fstride = (long long)a.n0 * n1 * h;
-  const long long colbase = (long long)ky * h + kz0;
+  const int rstride = n1 * h;
   const int region = L::PAD * TZ;
-  // forward FFT of each input field into its own shared region
-  for (int f = 0; f < a.F; ++f) {
-    V* rg = smb + f * region;
-    auto sm = [rg, TZ, c](int pos) -> V& { return rg[pos * TZ + c]; };
-    const V* col = a.in + f * fstride + colbase + c;
-    V v[L::R1];
+  V* rg = smb + grp * region + c;
+  auto sm = [rg, TZ](int pos) -> V& { return rg[pos * TZ]; };
+  V* part = smb + a.groups * region;  // GM x N0 results of the packed column
+  V v[L::R1];
+  // forward FFT, group grp takes field grp
+  const bool fw = grp < a.F;
+  {
+    const V* src = a.in + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
 #pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = col[(long long)L::in_pos(t, r) * n1 * h];
-    L::template run<-1>(v, t, sm, a.tw);
-    __syncthreads();
+    for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
+  }
+  L::template run<-1>(v, t, sm, a.tw);
+  __syncthreads();
+  if (fw) {
 #pragma unroll
     for (int i = 0; i < L::R1; ++i) sm(L::out_pos(t, i)) = v[i];
   }
   __syncthreads();
-  // contraction over Hermitian pairs (kx, n0 - kx)
+  // contraction over all (kx, column) points of the tile
+  const bool special_blk = kz0 == 0 && (n1 == 1 || ky == 0 || ky == HH);
   {
-    constexpr int npair = N0 / 2 + 1;
-    const int HH = n1 / 2;
     const int nn[3] = {a.n0, a.n1, a.n2};
-    for (int idx = threadIdx.x; idx < npair * TZ; idx += blockDim.x) {
-      const int cc = idx % TZ, p = idx / TZ;
-      const int kxa = p % N0, kxb = (N0 - p) % N0;
+#pragma unroll 1
+    for (int idx = threadIdx.x; idx < N0 * TZ; idx += blockDim.x) {
+      const int cc = idx % TZ, kx = idx / TZ;
       const int kz = kz0 + cc;
-      bool special = false;
       int kyA = ky, kzA = kz, kyB = 0, kzB = 0;
       if (kz == 0) {
         if (n1 == 1) {
-          special = true;
           kyA = 0; kzA = 0; kyB = 0; kzB = h;
         } else if (ky == 0) {
-          special = true;
           kyA = 0; kzA = 0; kyB = HH; kzB = 0;
         } else if (ky == HH) {
-          special = true;
           kyA = 0; kzA = h; kyB = HH; kzB = h;
         } else if (ky > HH) {
           kyA = ky - HH; kzA = h;
         }
       }
-      V wa[FM], wb[FM];
+      const V* pin = smb + kx * TZ + cc;
+      if (!(special_blk && cc == 0)) {
+        V in[FM], out[GM];
 #pragma unroll
-      for (int f = 0; f < FM; ++f) {
-        wa[f] = f < a.F ? smb[f * region + kxa * TZ + cc] : mk2((T)0, (T)0);
-        wb[f] = f < a.F ? smb[f * region + kxb * TZ + cc] : mk2((T)0, (T)0);
-      }
-      if (!special) {
-        V oa[GM];
-        contract_at<T, FM, GM>(a.ec, a.perm, nn, kxa, kyA, kzA, wa, oa);
+        for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pin[f * region] : mk2((T)0, (T)0);
+        contract_at<T, FM, GM>(a.ec, nn, kx, kyA, kzA, in, out);
+        V* pout = smb + kx * TZ + cc;
 #pragma unroll
         for (int g = 0; g < GM; ++g)
-          if (g < a.G) smb[g * region + kxa * TZ + cc] = oa[g];
-        if (kxb != kxa) {
-          contract_at<T, FM, GM>(a.ec, a.perm, nn, kxb, kyA, kzA, wb, oa);
-#pragma unroll
-          for (int g = 0; g < GM; ++g)
-            if (g < a.G) smb[g * region + kxb * TZ + cc] = oa[g];
-        }
+          if (g < a.G) pout[g * region] = out[g];
       } else {
         // two real sequences packed in one column: A = (W(k) + conj W(-k))/2,
-        // B = -i (W(k) - conj W(-k))/2, contracted with their own k
-        V Af[FM], Bf[FM];
+        // B = -i (W(k) - conj W(-k))/2, each contracted with its own k
+        const int kxb = (N0 - kx) % N0;
+        V res[2][GM];
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+          V in[FM];
 #pragma unroll
-        for (int f = 0; f < FM; ++f) {
-          Af[f] = mk2((T)0.5 * (wa[f].x + wb[f].x), (T)0.5 * (wa[f].y - wb[f].y));
-          const V d = mk2(wa[f].x - wb[f].x, wa[f].y + wb[f].y);
-          Bf[f] = mk2((T)0.5 * d.y, (T)-0.5 * d.x);
-        }
-        V ra[GM], rb[GM];
-        contract_at<T, FM, GM>(a.ec, a.perm, nn, kxa, kyA, kzA, Af, ra);
-        contract_at<T, FM, GM>(a.ec, a.perm, nn, kxa, kyB, kzB, Bf, rb);
-#pragma unroll
-        for (int g = 0; g < GM; ++g) {
-          if (g < a.G) {
-            smb[g * region + kxa * TZ + cc] = mk2(ra[g].x - rb[g].y, ra[g].y + rb[g].x);
-            if (kxb != kxa) smb[g * region + kxb * TZ + cc] = mk2(ra[g].x + rb[g].y, -ra[g].y + rb[g].x);
+          for (int f = 0; f < FM; ++f) {
+            const V wa = f < a.F ? smb[f * region + kx * TZ] : mk2((T)0, (T)0);
+            const V wb = f < a.F ? smb[f * region + kxb * TZ] : mk2((T)0, (T)0);
+            if (half == 0) {
+              in[f] = mk2((T)0.5 * (wa.x + wb.x), (T)0.5 * (wa.y - wb.y));
+            } else {
+              in[f] = mk2((T)0.5 * (wa.y + wb.y), (T)-0.5 * (wa.x - wb.x));
+            }
           }
+          V out[GM];
+          contract_at<T, FM, GM>(a.ec, nn, kx, half ? kyB : kyA, half ? kzB : kzA, in, out);
+#pragma unroll
+          for (int g = 0; g < GM; ++g) res[half][g] = out[g];
         }
+#pragma unroll
+        for (int g = 0; g < GM; ++g)
+          if (g < a.G) part[g * N0 + kx] = mk2(res[0][g].x - res[1][g].y, res[0][g].y + res[1][g].x);
       }
     }
   }
   __syncthreads();
-  // inverse FFT of each output field
-  for (int g = 0; g < a.G; ++g) {
-    V* rg = smb + g * region;
-    auto sm = [rg, TZ, c](int pos) -> V& { return rg[pos * TZ + c]; };
-    V v[L::R1];
-#pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = sm(L::in_pos(t, r));
-    __syncthreads();
-    L::template run<1>(v, t, sm, a.tw);
-    V* col = a.out + g * fstride + colbase + c;
-#pragma unroll
-    for (int i = 0; i < L::R1; ++i) col[(long long)L::out_pos(t, i) * n1 * h] = v[i];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// x pass with every field held in registers.  For a square plan (R1 == R2,
-// or one stage) the forward FFT leaves X[out_pos(t,i)] with out_pos == in_pos,
-// so the contraction runs on registers and its result is directly the input
-// of the inverse FFT: shared memory carries only the FFT exchange (and, in the
-// blocks holding the two packed columns, the Hermitian partners).
-// ---------------------------------------------------------------------------
-template <typename T, int N0, int F>
-__global__ void __launch_bounds__(256) k_xreg(XArgs<T> a) {
-  using L = Line<T, N0>;
-  using V = cplx<T>;
-  static_assert(L::R2 == 1 || L::R1 == L::R2, "square plan");
-  extern __shared__ __align__(16) unsigned char smraw[];
-  V* smb = reinterpret_cast<V*>(smraw);
-  const int TZ = a.tz;
-  const int c = threadIdx.x % TZ, t = threadIdx.x / TZ;
-  const int kz0 = blockIdx.x * TZ, ky = blockIdx.y;
-  const int h = a.h, n1 = a.n1, HH = n1 / 2;
-  const long long fstride = (long long)a.n0 * n1 * h;
-  const long long colbase = (long long)ky * h + kz0 + c;
-  const long long rstride = (long long)n1 * h;
-  auto sm = [smb, TZ, c](int pos) -> V& { return smb[pos * TZ + c]; };
-  V v[F][L::R1];
-#pragma unroll
-  for (int f = 0; f < F; ++f)
-#pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[f][r] = a.in[f * fstride + colbase + L::in_pos(t, r) * rstride];
-#pragma unroll
-  for (int f = 0; f < F; ++f) {
-    if (f > 0) __syncthreads();
-    L::template run<-1>(v[f], t, sm, a.tw);
-  }
-  // packed columns (kz slot 0 with ky slot 0 or n1/2, or n1 == 1) need W(-kx)
-  const bool special_blk = kz0 == 0 && (n1 == 1 || ky == 0 || ky == HH);
-  V* part = smb + L::PAD * TZ;  // F x N0 partner buffer after the exchange area
   if (special_blk) {
-    __syncthreads();
-    if (c == 0) {
-#pragma unroll
-      for (int f = 0; f < F; ++f)
-#pragma unroll
-        for (int i = 0; i < L::R1; ++i) part[f * N0 + L::out_pos(t, i)] = v[f][i];
+    for (int idx = threadIdx.x; idx < a.G * N0; idx += blockDim.x) {
+      const int g = idx / N0, kx = idx - g * N0;
+      smb[g * region + kx * TZ] = part[g * N0 + kx];
     }
     __syncthreads();
   }
-  const int nn[3] = {a.n0, a.n1, a.n2};
-  const int kz = kz0 + c;
-  int kyA = ky, kzA = kz, kyB = 0, kzB = 0;
-  const bool special = special_blk && c == 0;
-  if (kz == 0) {
-    if (n1 == 1) {
-      kyA = 0; kzA = 0; kyB = 0; kzB = h;
-    } else if (ky == 0) {
-      kyA = 0; kzA = 0; kyB = HH; kzB = 0;
-    } else if (ky == HH) {
-      kyA = 0; kzA = h; kyB = HH; kzB = h;
-    } else if (ky > HH) {
-      kyA = ky - HH; kzA = h;
-    }
-  }
+  // inverse FFT, group grp takes output field grp
+  const bool iv = grp < a.G;
 #pragma unroll
-  for (int i = 0; i < L::R1; ++i) {
-    const int kx = L::out_pos(t, i);
-    V in[F], out[F];
+  for (int r = 0; r < L::R1; ++r) v[r] = iv ? sm(L::in_pos(t, r)) : mk2((T)0, (T)0);
+  __syncthreads();
+  L::template run<1>(v, t, sm, a.tw);
+  if (iv) {
+    V* dst = a.out + grp * fstride + (long long)ky * h + kz0 + c;
 #pragma unroll
-    for (int f = 0; f < F; ++f) in[f] = v[f][i];
-    if (!special) {
-      contract_at<T, F, F>(a.ec, a.perm, nn, kx, kyA, kzA, in, out);
-#pragma unroll
-      for (int f = 0; f < F; ++f) v[f][i] = out[f];
-    } else {
-      const int kxb = (N0 - kx) % N0;
-      V Af[F], Bf[F], ra[F], rb[F];
-#pragma unroll
-      for (int f = 0; f < F; ++f) {
-        const V wb = part[f * N0 + kxb];
-        Af[f] = mk2((T)0.5 * (in[f].x + wb.x), (T)0.5 * (in[f].y - wb.y));
-        const V d = mk2(in[f].x - wb.x, in[f].y + wb.y);
-        Bf[f] = mk2((T)0.5 * d.y, (T)-0.5 * d.x);
-      }
-      contract_at<T, F, F>(a.ec, a.perm, nn, kx, kyA, kzA, Af, ra);
-      contract_at<T, F, F>(a.ec, a.perm, nn, kx, kyB, kzB, Bf, rb);
-#pragma unroll
-      for (int f = 0; f < F; ++f) v[f][i] = mk2(ra[f].x - rb[f].y, ra[f].y + rb[f].x);
-    }
-  }
-#pragma unroll
-  for (int f = 0; f < F; ++f) {
-    __syncthreads();
-    L::template run<1>(v[f], t, sm, a.tw);
-    V* col = a.out + f * fstride + colbase;
-#pragma unroll
-    for (int i = 0; i < L::R1; ++i) col[L::out_pos(t, i) * rstride] = v[f][i];
+    for (int i = 0; i < L::R1; ++i) dst[(long long)L::out_pos(t, i) * rstride] = v[i];
   }
 }
 

@@ -52,13 +52,16 @@ __host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t 
 }
 
 // Box & Muller (1958) on two 24-bit uniforms: (r cos, r sin).
+// FP32: the angle 2 pi u2 is shifted to [-pi, pi), where the hardware
+// sine / cosine approximations have an absolute error below 2^-21.4; with
+// sin(t) = -sin(t - pi) and cos(t) = -cos(t - pi).
 __device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b, float) {
   const float u1 = ((float)(a >> 8) + 0.5f) * (1.0f / 16777216.0f);
   const float u2 = ((float)(b >> 8) + 0.5f) * (1.0f / 16777216.0f);
   const float r = sqrtf(-2.0f * logf(u1));
   float s, c;
-  sincospif(2.0f * u2, &s, &c);
-  return make_float2(r * c, r * s);
+  __sincosf(6.283185307179586f * u2 - 3.141592653589793f, &s, &c);
+  return make_float2(-r * c, -r * s);
 }
 __device__ __forceinline__ double2 box_muller(uint32_t a, uint32_t b, double) {
   const double u1 = ((double)(a >> 8) + 0.5) * (1.0 / 16777216.0);

@@ -41,13 +41,13 @@ template <typename T> __global__ void k_plain_bfill(T* B, ElasticConst<T> ec, PG
   const int z = (int)(idx % g.n2), y = (int)((idx / g.n2) % g.n1), x = (int)(idx / ((long long)g.n1 * g.n2));
   const int id[3] = {x, y, z}, nn[3] = {g.n0, g.n1, g.n2};
   T k[3];
-  for (int c = 0; c < 3; ++c) k[g.perm[c]] = ec.kscale[c] * (T)fold_idx(id[c], nn[c], ec.refcompat);
+  for (int c = 0; c < 3; ++c) k[c] = ec.kscale[c] * (T)fold_idx(id[c], nn[c], ec.refcompat);
   // column b of B: contract a unit input vector e_b
   for (int b = 0; b < g.V; ++b) {
-    cplx<T> in[GS_MAXF], out[GS_MAXG];
+    cplx<T> in[GS_MAXF], out[GS_MAXF];
     for (int f = 0; f < GS_MAXF; ++f) in[f] = mk2(f == b ? (T)1 : (T)0, (T)0);
-    for (int a = 0; a < GS_MAXG; ++a) out[a] = mk2((T)0, (T)0);
-    contract_k<T, GS_MAXF, GS_MAXG>(ec, k, in, out, ec.scale);
+    for (int a = 0; a < GS_MAXF; ++a) out[a] = mk2((T)0, (T)0);
+    contract_k<T, GS_MAXF, GS_MAXF>(ec, k, in, out, ec.scale);
     for (int a = 0; a < g.V; ++a) B[((long long)a * g.V + b) * g.N + idx] = out[a].x;
   }
 }

@@ -1,0 +1,195 @@
+"""Generate golden fixtures by running the reference's own gsi
+(oracle/_ref/gsi, built by oracle/build_ref.sh from the reference sources)
+on small seeded inputs.  The physics cases need a CUDA device (the
+reference's kernels are device-only); the front-end cases run anywhere.
+
+  python tests/golden/make_ref_fixtures.py --out DIR [--physics] [--frontend]
+
+Writes DIR/ref_<case>.npz (inputs, dumps, the info lines) and
+DIR/frontend_<script>.txt.  The committed copies under tests/golden/ are
+the outputs of this script; the tests never run the reference.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+GSI = os.path.join(ROOT, "oracle", "_ref", "gsi")
+
+MART_TENSOR = """3 4 3 3
+0.00 0.0063 0.0063  0.0063 0.0 0.0063    0.0063 0.0063 0.0
+0.00 0.0063 -0.0063  0.0063 0.0 -0.0063 -0.0063 -0.0063 0.0
+0.00 -0.0063 0.0063  -0.0063 0.0 -0.0063  0.0063 -0.0063 0.0
+0.00 -0.0063 -0.0063  -0.0063 0.0 0.0063  -0.0063 0.0063 0.0"""
+
+PRECIP_TENSOR = """3 4 3 3
+-0.01126 -0.00709 -0.00709 -0.00709 -0.01126 -0.00709 -0.00709 -0.00709 -0.01126
+-0.01126 0.00709 0.00709 0.00709 -0.01126 -0.00709 0.00709 -0.00709 -0.01126
+-0.01126 0.00709 -0.00709 0.00709 -0.01126 0.00709 -0.00709 0.00709 -0.01126
+-0.01126 -0.00709 0.00709 -0.00709 -0.01126 0.00709 0.00709 0.00709 -0.01126"""
+
+# the expression block of the stress script (values evaluated by the script engine)
+STRESS_TENSOR = """3 4 3 3
+{
+-1.835*0.01, -8.1868274*0.001, -5.7889605*0.001,-8.1868256*0.001, -8.897*0.001, -3.3422573*0.001,-5.7889605*0.001, -3.3422580*0.001, -6.54*0.001
+-4.17*0.001,  0.0,  0.0, 0.0, -2.3*0.01, 6.6845156*0.001, 0.0,  6.6845166*0.001, -6.5*0.001
+-4.17*0.001,  0.0,  0.0, 0.0, -4.17*0.001, 0.0,0.0,  0.0, -2.544*0.01
+-1.835*0.01,  8.1868265*0.001,  5.788961*0.001,8.1868256*0.001, -8.897*0.001, -3.3422573*0.001,5.7889605*0.001, -3.3422580*0.001, -6.5*0.001
+}"""
+
+SHAPE = (16, 12, 8)
+
+
+def write_text_field(path: str, arr: np.ndarray) -> None:
+    """The reference's text field format: 'ndim d1 .. dn' then one value per line."""
+    a = np.asarray(arr, dtype=np.float32)
+    with open(path, "w") as f:
+        f.write(" ".join(str(x) for x in [a.ndim, *a.shape]) + " \n")
+        f.write("\n".join(repr(float(x)) for x in a.ravel()) + "\n")
+
+
+def read_binary_field(path: str) -> np.ndarray:
+    """The reference's binary field format: int32 ndim, int32 dims, float32 values."""
+    with open(path, "rb") as f:
+        nd = struct.unpack("i", f.read(4))[0]
+        dims = struct.unpack("i" * nd, f.read(4 * nd))
+        vals = np.frombuffer(f.read(), dtype=np.float32)
+    return vals.reshape(dims)
+
+
+def run_gsi(workdir: str, script: str, name: str) -> str:
+    path = os.path.join(workdir, name)
+    with open(path, "w") as f:
+        f.write(script)
+    r = subprocess.run([GSI, name], cwd=workdir, capture_output=True, text=True, timeout=600)
+    return r.stdout
+
+
+def case_mart(out: str) -> None:
+    rng = np.random.default_rng(7)
+    nx, ny, nz = SHAPE
+    eta = rng.uniform(0.0, 0.1, (4, nx, ny, nz)).astype(np.float32)
+    ds = rng.uniform(-0.05, 0.05, (6, nx, ny, nz)).astype(np.float32)
+    defect = (rng.random((nx, ny, nz)) < 0.05).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        write_text_field(os.path.join(d, "data.eta"), eta)
+        write_text_field(os.path.join(d, "data.stress"), ds)
+        write_text_field(os.path.join(d, "data.defect"), defect)
+        script = f"""sys mart
+set binary off
+set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
+set deltatime 0.01
+set transitiontemperature 450
+set weightdislocation .1
+set weightnoise 0
+read eta data.eta
+read dislocationstress data.stress
+read defect data.defect
+readhere varianttensor
+{MART_TENSOR}
+info 5 temperature eta gradient chemical elastic dislocation
+set binary on
+dump dumpdir 5 eta
+set fix temperature 460 300
+run 5
+"""
+        log = run_gsi(d, script, "in.mart16")
+        dumps = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"eta.{i}.data")) for i in range(1, 6)])
+    np.savez_compressed(os.path.join(out, "ref_mart.npz"), eta0=eta, dislocationstress=ds, defect=defect,
+                        eta_steps=dumps, log=np.array(log))
+
+
+def case_precipitate(out: str) -> None:
+    rng = np.random.default_rng(8)
+    nx, ny, nz = SHAPE
+    eta = rng.uniform(0.0, 0.5, (4, nx, ny, nz)).astype(np.float32)
+    con = (0.2 + rng.uniform(-0.02, 0.02, (nx, ny, nz))).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        write_text_field(os.path.join(d, "data.eta"), eta)
+        write_text_field(os.path.join(d, "data.con"), con)
+        script = f"""sys precipitate
+set binary off
+set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
+set deltatime 0.1
+set coefficient 54.00 -17.0 7.0 2.5 0.2 0.2 0.2
+set arfi 300.0
+set beta 300.0
+set meta 0.4
+set lpp  0.4
+set xi   400
+set concentration 0.1 0.44
+set weightnoise 0
+read eta data.eta
+read concentration data.con
+readhere varianttensor
+{PRECIP_TENSOR}
+info 5 eta_average
+set binary on
+dump dumpdir 5 eta concentration
+run 5
+"""
+        log = run_gsi(d, script, "in.precipitate16")
+        e = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"eta.{i}.data")) for i in range(1, 6)])
+        c = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"concentration.{i}.data")) for i in range(1, 6)])
+    np.savez_compressed(os.path.join(out, "ref_precipitate.npz"), eta0=eta, con0=con, eta_steps=e, con_steps=c,
+                        log=np.array(log))
+
+
+def case_stress(out: str) -> None:
+    rng = np.random.default_rng(9)
+    nx, ny, nz = SHAPE
+    eta = rng.uniform(0.0, 1.0, (4, nx, ny, nz)).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        write_text_field(os.path.join(d, "data.eta"), eta)
+        script = f"""sys stress
+set binary off
+set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
+read eta data.eta
+readhere varianttensor
+{STRESS_TENSOR}
+writehere varianttensor
+set binary on
+dump dumpdir 1 stress defect
+run 1
+"""
+        log = run_gsi(d, script, "in.stress16")
+        stress = read_binary_field(os.path.join(d, "dumpdir", "stress.1.data"))
+        defect = read_binary_field(os.path.join(d, "dumpdir", "defect.1.data"))
+    np.savez_compressed(os.path.join(out, "ref_stress.npz"), eta0=eta, stress=stress, defect=defect, log=np.array(log))
+
+
+def case_frontend(out: str) -> None:
+    for name in ["in.if.loop.while", "in.pow"]:
+        src = os.path.join(os.environ.get("REF", "/root/reference"), "scripts", name)
+        with tempfile.TemporaryDirectory() as d:
+            shutil.copy(src, os.path.join(d, name))
+            r = subprocess.run([GSI, name], cwd=d, capture_output=True, text=True, timeout=60)
+        with open(os.path.join(out, f"frontend_{name.replace('.', '_')}.txt"), "w") as f:
+            f.write(r.stdout)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--physics", action="store_true")
+    ap.add_argument("--frontend", action="store_true")
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    if a.frontend:
+        case_frontend(a.out)
+    if a.physics:
+        case_mart(a.out)
+        case_precipitate(a.out)
+        case_stress(a.out)
+
+
+if __name__ == "__main__":
+    main()
