@@ -16,6 +16,7 @@
 #include "../../include/gs_capi.h"
 #include "gs_launch.h"
 #include "gs_mart.cuh"
+#include "gs_precip.cuh"
 #include "gs_sim.h"
 
 using namespace gs;
@@ -403,18 +404,21 @@ template <typename T> static const cplx<T>* twp(const gs_sim* s, int which) {
 // ---------------------------------------------------------------------------
 // the martensite step
 // ---------------------------------------------------------------------------
-template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st) {
-  const int V = s->p.nvariants;
+// z forward (with the eta^2 prologue where square[f]) -> y forward -> x pass
+// (B contraction, F inputs -> G outputs, into out_spec) -> y inverse.
+template <typename T>
+static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, int F, int which, double scale,
+                           void* out_spec, int G, cudaStream_t st) {
   const long long rows = (long long)s->n0 * s->n1;
   ZfwdArgs<T> za;
   memset(&za, 0, sizeof(za));
-  for (int f = 0; f < V; ++f) {
-    za.src[f] = eta + (long long)f * s->N;
-    za.square[f] = 1;
+  for (int f = 0; f < F; ++f) {
+    za.src[f] = src[f];
+    za.square[f] = square[f];
   }
   za.dst = reinterpret_cast<cplx<T>*>(s->spec);
   za.rows_per_field = rows;
-  za.nrows = rows * V;
+  za.nrows = rows * F;
   za.tw_h = twp<T>(s, 1);
   za.tw_n2 = twp<T>(s, 0);
   GS_CU(launch_zfwd<T>(za, s->h, st), "z forward pass");
@@ -425,25 +429,39 @@ template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st
   ya.n1 = s->n1;
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
-  GS_CU(launch_ypass<T>(ya, s->n1, V, -1, st), "y forward pass");
+  GS_CU(launch_ypass<T>(ya, s->n1, F, -1, st), "y forward pass");
   if (s->n1 > 1) gs_mark(s, st);
   XArgs<T> xa;
+  memset(&xa, 0, sizeof(xa));
   xa.in = reinterpret_cast<cplx<T>*>(s->spec);
-  xa.out = reinterpret_cast<cplx<T>*>(s->spec);
+  xa.out = reinterpret_cast<cplx<T>*>(out_spec);
   xa.n0 = s->n0;
   xa.n1 = s->n1;
   xa.n2 = s->n2;
   xa.h = s->h;
-  xa.F = V;
-  xa.G = V;
+  xa.F = F;
+  xa.G = G;
   xa.tw = twp<T>(s, 3);
-  build_elastic<T>(s, 0, 1.0 / (double)s->N, xa.ec);
+  build_elastic<T>(s, which, scale, xa.ec);
   GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
   gs_mark(s, st);
-  GS_CU(launch_ypass<T>(ya, s->n1, V, 1, st), "y inverse pass");
+  YArgs<T> yb = ya;
+  yb.spec = reinterpret_cast<cplx<T>*>(out_spec);
+  GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st), "y inverse pass");
   if (s->n1 > 1) gs_mark(s, st);
   s->launches += 2 + (s->n1 > 1 ? 2 : 0);
   return GS_OK;
+}
+
+template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st) {
+  const int V = s->p.nvariants;
+  const T* src[GS_MAXF];
+  int sq[GS_MAXF];
+  for (int f = 0; f < V; ++f) {
+    src[f] = eta + (long long)f * s->N;
+    sq[f] = 1;
+  }
+  return elastic_chain_g<T>(s, src, sq, V, 0, 1.0 / (double)s->N, s->spec, V, st);
 }
 
 template <typename T> static void fill_mart_args(gs_sim* s, MartArgs<T>& ma, const T* in, T* out) {
@@ -515,13 +533,252 @@ template <typename T> static int mart_stats(gs_sim* s, gs_stats* o, cudaStream_t
 }
 
 // ---------------------------------------------------------------------------
+// the precipitate step (src/dynamics_precipitate.cu:278-289)
+// ---------------------------------------------------------------------------
+static int precip_nfields(const gs_sim* s) { return s->p.nvariants + (s->p.c_elastic ? 1 : 0); }
+
+template <typename T> static void fill_ktab(gs_sim* s) {
+  // K(k) per canonical axis: refcompat |k|^2 of the 3.14 vector (_gSquare,
+  // src/gtensorb.cu:9-23), baseline the seven-point symbol 4/d^2 sin^2(pi m/n)
+  const gs_params& p = s->p;
+  const int nc[3] = {s->n0, s->n1, s->n2};
+  std::vector<T> host;
+  for (int c = 0; c < 3; ++c) {
+    s->ktab_off[c] = host.size();
+    const double d = s->dcan[c];
+    for (int i = 0; i < nc[c]; ++i) {
+      double v = 0;
+      if (nc[c] > 1) {
+        if (p.mode == GS_MODE_REFCOMPAT) {
+          const int m = i < nc[c] / 2 ? i : i - nc[c];
+          const double k = 2.0 * 3.14 * d / nc[c] * m;
+          v = k * k;
+        } else {
+          const double sn = std::sin(M_PI * (double)i / nc[c]);
+          v = 4.0 / (d * d) * sn * sn;
+        }
+      }
+      host.push_back((T)v);
+    }
+  }
+  cudaMemcpy(s->ktab, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+template <typename T> static int precip_potential(gs_sim* s, cudaStream_t st) {
+  const int V = s->p.nvariants, F1 = precip_nfields(s);
+  const T* eta = reinterpret_cast<const T*>(s->eta[0]);
+  const T* src[GS_MAXF + 1];
+  int sq[GS_MAXF + 1];
+  for (int f = 0; f < V; ++f) {
+    src[f] = eta + (long long)f * s->N;
+    sq[f] = 1;
+  }
+  if (F1 > V) {
+    src[V] = reinterpret_cast<const T*>(s->conc);
+    sq[V] = 0;
+  }
+  GS_TRY(elastic_chain_g<T>(s, src, sq, F1, 2, 1.0 / (double)s->N, s->spec, F1, st));
+  ZinvArgs<T> zi;
+  memset(&zi, 0, sizeof(zi));
+  zi.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+  for (int f = 0; f < F1; ++f) zi.dst[f] = reinterpret_cast<T*>(s->rbuf) + (long long)f * s->N;
+  zi.rows_per_field = (long long)s->n0 * s->n1;
+  zi.nrows = zi.rows_per_field * F1;
+  zi.tw_h = twp<T>(s, 1);
+  zi.tw_n2 = twp<T>(s, 0);
+  zi.offset_field = -1;
+  GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (elastic potential)");
+  gs_mark(s, st);
+  s->launches += 1;
+  return GS_OK;
+}
+
+template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
+  const gs_params& p = s->p;
+  const int V = p.nvariants;
+  const long long N = s->N;
+  const bool ref = p.mode == GS_MODE_REFCOMPAT;
+  GS_TRY(precip_potential<T>(s, st));
+  T* eta = reinterpret_cast<T*>(s->eta[0]);
+  T* c = reinterpret_cast<T*>(s->conc);
+  T* mu = reinterpret_cast<T*>(s->mubuf);
+  T* g = mu + N;
+  PrecipLocalArgs<T> la;
+  memset(&la, 0, sizeof(la));
+  la.c = c;
+  la.eta = eta;
+  la.R = reinterpret_cast<const T*>(s->rbuf);
+  la.mu = mu;
+  la.g = g;
+  la.N = N;
+  la.V = V;
+  la.c_elastic = p.c_elastic && !ref;
+  for (int i = 0; i < 8; ++i) la.A[i] = (T)p.coef[i];
+  la.c1 = (T)p.c1;
+  la.c2 = (T)p.c2;
+  la.Es = (T)(p.xi * p.weight_elastic);
+  la.an = (T)(p.noise_amp * (ref ? 1e-4 : 1.0));
+  la.k0 = (uint32_t)(p.seed & 0xffffffffu);
+  la.k1 = (uint32_t)(p.seed >> 32);
+  la.sim = p.sim_id;
+  la.step = (uint32_t)s->step;
+  GS_CU(launch_precip_local<T>(la, st), "precipitate local terms");
+  gs_mark(s, st);
+  // chain 2: [c, mu, eta_0, g_0, eta_1, g_1, ...] -> k-space update -> [c', eta']
+  const int F2 = 2 * V + 2, G2 = V + 1;
+  const long long rows = (long long)s->n0 * s->n1;
+  ZfwdArgs<T> za;
+  memset(&za, 0, sizeof(za));
+  za.src[0] = c;
+  za.src[1] = mu;
+  for (int v = 0; v < V; ++v) {
+    za.src[2 + 2 * v] = eta + (long long)v * N;
+    za.src[3 + 2 * v] = g + (long long)v * N;
+  }
+  za.dst = reinterpret_cast<cplx<T>*>(s->spec2);
+  za.rows_per_field = rows;
+  za.nrows = rows * F2;
+  za.tw_h = twp<T>(s, 1);
+  za.tw_n2 = twp<T>(s, 0);
+  GS_CU(launch_zfwd<T>(za, s->h, st), "z forward (update fields)");
+  gs_mark(s, st);
+  YArgs<T> ya;
+  ya.spec = reinterpret_cast<cplx<T>*>(s->spec2);
+  ya.n0 = s->n0;
+  ya.n1 = s->n1;
+  ya.h = s->h;
+  ya.tw = twp<T>(s, 2);
+  GS_CU(launch_ypass<T>(ya, s->n1, F2, -1, st), "y forward (update fields)");
+  if (s->n1 > 1) gs_mark(s, st);
+  XArgs<T> xa;
+  memset(&xa, 0, sizeof(xa));
+  xa.in = reinterpret_cast<cplx<T>*>(s->spec2);
+  xa.out = reinterpret_cast<cplx<T>*>(s->spec2);
+  xa.n0 = s->n0;
+  xa.n1 = s->n1;
+  xa.n2 = s->n2;
+  xa.h = s->h;
+  xa.F = F2;
+  xa.G = G2;
+  xa.tw = twp<T>(s, 3);
+  xa.pu.V = V;
+  xa.pu.mass_proj = p.mass_projection;
+  xa.pu.dtM = (T)(p.dt * p.mobility_c);
+  xa.pu.dtL = (T)(p.dt * p.mobility_eta);
+  xa.pu.kc = (T)p.kappa_c;
+  xa.pu.ke = (T)p.kappa_eta;
+  xa.pu.scale = (T)(1.0 / (double)N);
+  for (int c3 = 0; c3 < 3; ++c3) xa.pu.ktab[c3] = reinterpret_cast<const T*>(s->ktab) + s->ktab_off[c3];
+  GS_CU(launch_xprecip<T>(xa, st), "x pass (k-space update)");
+  gs_mark(s, st);
+  GS_CU(launch_ypass<T>(ya, s->n1, G2, 1, st), "y inverse (update fields)");
+  if (s->n1 > 1) gs_mark(s, st);
+  ZinvArgs<T> zi;
+  memset(&zi, 0, sizeof(zi));
+  zi.spec = reinterpret_cast<const cplx<T>*>(s->spec2);
+  zi.dst[0] = c;
+  for (int v = 0; v < V; ++v) zi.dst[1 + v] = eta + (long long)v * N;
+  zi.rows_per_field = rows;
+  zi.nrows = rows * G2;
+  zi.tw_h = twp<T>(s, 1);
+  zi.tw_n2 = twp<T>(s, 0);
+  zi.offset_field = p.mass_projection ? 0 : -1;
+  zi.offset = s->mass0 / (double)N;
+  GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (c, eta)");
+  gs_mark(s, st);
+  s->launches += 3 + (s->n1 > 1 ? 2 : 0);
+  s->step += 1;
+  return GS_OK;
+}
+
+template <typename T> static int precip_stats(gs_sim* s, gs_stats* o, cudaStream_t st) {
+  const gs_params& p = s->p;
+  const int V = p.nvariants;
+  GS_TRY(precip_potential<T>(s, st));
+  PrecipStatsArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.c = reinterpret_cast<const T*>(s->conc);
+  a.eta = reinterpret_cast<const T*>(s->eta[0]);
+  a.R = reinterpret_cast<const T*>(s->rbuf);
+  a.N = s->N;
+  a.n0 = s->n0;
+  a.n1 = s->n1;
+  a.n2 = s->n2;
+  a.V = V;
+  a.c_elastic = p.c_elastic;
+  for (int i = 0; i < 8; ++i) a.A[i] = (T)p.coef[i];
+  a.c1 = (T)p.c1;
+  a.c2 = (T)p.c2;
+  a.Es = (T)(p.xi * p.weight_elastic);
+  a.kc = (T)p.kappa_c;
+  a.ke = (T)p.kappa_eta;
+  const int nc[3] = {s->n0, s->n1, s->n2};
+  for (int c = 0; c < 3; ++c) a.gcoef[c] = nc[c] > 1 ? (T)(1.0 / (s->dcan[c] * s->dcan[c])) : (T)0;
+  a.partials = s->partials;
+  int nb = 0;
+  GS_CU(launch_precip_stats<T>(a, st, &nb), "precipitate statistics");
+  GS_CU(launch_reduce(s->partials, nb, ACC_N, s->red, st), "reduce");
+  double acc[ACC_N];
+  GS_CU(cudaMemcpyAsync(acc, s->red, sizeof(acc), cudaMemcpyDeviceToHost, st), "stats D2H");
+  GS_CU(cudaStreamSynchronize(st), "stats sync");
+  const double N = (double)s->N, dV = p.dx * p.dy * p.dz;
+  memset(o, 0, sizeof(*o));
+  o->mass = acc[ACC_MASS];
+  o->c_mean = acc[ACC_MASS] / N;
+  o->eta_mean = acc[ACC_C] / (N * V);
+  for (int v = 0; v < V; ++v) {
+    o->eta2[v] = acc[ACC_ETA2 + v] / N;
+    o->vf[v] = acc[ACC_VF + v] / N;
+  }
+  o->e_el = acc[ACC_EEL] * dV;
+  o->e_chem = acc[ACC_ECHEM] * dV;
+  o->e_grad = acc[ACC_EGRAD] * dV;
+  o->e_tot = o->e_el + o->e_chem + o->e_grad;
+  o->step = s->step;
+  return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the stress field (src/dynamics_stress.cu:147-194)
+// ---------------------------------------------------------------------------
+template <typename T> static int stress_step(gs_sim* s, cudaStream_t st) {
+  const int V = s->p.nvariants;
+  const T* eta = reinterpret_cast<const T*>(s->eta[0]);
+  const T* src[GS_MAXF];
+  int sq[GS_MAXF];
+  for (int f = 0; f < V; ++f) {
+    src[f] = eta + (long long)f * s->N;
+    sq[f] = 1;
+  }
+  // sigma_b = -Xi IFFT(sum_v B_bv FFT(eta_v^2) / N)
+  GS_TRY(elastic_chain_g<T>(s, src, sq, V, 1, -s->p.xi / (double)s->N, s->spec2, 6, st));
+  ZinvArgs<T> zi;
+  memset(&zi, 0, sizeof(zi));
+  zi.spec = reinterpret_cast<const cplx<T>*>(s->spec2);
+  for (int b = 0; b < 6; ++b) zi.dst[b] = reinterpret_cast<T*>(s->stressbuf) + (long long)b * s->N;
+  zi.rows_per_field = (long long)s->n0 * s->n1;
+  zi.nrows = zi.rows_per_field * 6;
+  zi.tw_h = twp<T>(s, 1);
+  zi.tw_n2 = twp<T>(s, 0);
+  zi.offset_field = -1;
+  GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (stress)");
+  gs_mark(s, st);
+  GS_CU(launch_defect<T>(eta, reinterpret_cast<T*>(s->defect), s->N, V, st), "defect mask");
+  gs_mark(s, st);
+  s->launches += 2;
+  s->step += 1;
+  return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
 // lifecycle
 // ---------------------------------------------------------------------------
 static size_t elt(const gs_sim* s) { return s->p.dtype == GS_DTYPE_F64 ? 8 : 4; }
 
 static void free_sim(gs_sim* s) {
   if (!s) return;
-  void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->tw, s->partials, s->red};
+  void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->rbuf, s->mubuf,
+                  s->stressbuf, s->ktab, s->tw, s->partials, s->red};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -531,10 +788,22 @@ static void free_sim(gs_sim* s) {
   delete s;
 }
 
+template <typename T> __global__ void k_fill(T* p, long long n, T v) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+static int dalloc(void** p, size_t bytes, const char* what) {
+  GS_CU(cudaMalloc(p, bytes), what);
+  GS_CU(cudaMemset(*p, 0, bytes), what);
+  return GS_OK;
+}
+
 extern "C" int gs_sim_create(const gs_params* p, gs_sim** out) {
   if (!p || !out) return gs_set_error(GS_EINVAL, "gs_sim_create: null argument");
   *out = nullptr;
-  if (p->model != GS_MODEL_MART) return gs_set_error(GS_ENOTSUP, "model %d not available in this build", p->model);
+  if (p->model != GS_MODEL_MART && p->model != GS_MODEL_PRECIPITATE && p->model != GS_MODEL_STRESS)
+    return gs_set_error(GS_EINVAL, "unknown model %d", p->model);
   if (p->nvariants < 1 || p->nvariants > GS_MAX_V)
     return gs_set_error(GS_EINVAL, "nvariants %d outside 1..%d", p->nvariants, GS_MAX_V);
   if (p->dtype != GS_DTYPE_F32 && p->dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", p->dtype);
@@ -558,14 +827,39 @@ extern "C" int gs_sim_create(const gs_params* p, gs_sim** out) {
   };
   if ((rc = gs_cuda_check(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking), "stream")) != GS_OK)
     return fail(rc);
-  for (int i = 0; i < 2; ++i) {
-    if ((rc = gs_cuda_check(cudaMalloc(&s->eta[i], fb * V), "cudaMalloc eta")) != GS_OK) return fail(rc);
-    if ((rc = gs_cuda_check(cudaMemset(s->eta[i], 0, fb * V), "memset eta")) != GS_OK) return fail(rc);
+  if ((rc = dalloc(&s->eta[0], fb * V, "eta")) != GS_OK) return fail(rc);
+  if (p->model == GS_MODEL_MART) {
+    if ((rc = dalloc(&s->eta[1], fb * V, "eta pair")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->spec, fb * V, "spectrum")) != GS_OK) return fail(rc);
+  } else if (p->model == GS_MODEL_PRECIPITATE) {
+    const int F1 = precip_nfields(s);
+    if ((rc = dalloc(&s->conc, fb, "concentration")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->spec, fb * F1, "spectrum")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->rbuf, fb * F1, "elastic potentials")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->mubuf, fb * (V + 1), "local terms")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->spec2, fb * (2 * V + 2), "update spectra")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->ktab, elt(s) * (size_t)(s->n0 + s->n1 + s->n2), "K table")) != GS_OK) return fail(rc);
+    if (p->dtype == GS_DTYPE_F64)
+      fill_ktab<double>(s);
+    else
+      fill_ktab<float>(s);
+    // the reference's default concentration c1 + (c2 - c1)/3 (src/dynamics_precipitate.cu:42-47)
+    const double c0 = p->c1 + (p->c2 - p->c1) / 3.0;
+    if (p->dtype == GS_DTYPE_F64)
+      k_fill<double><<<256, 256>>>(reinterpret_cast<double*>(s->conc), s->N, c0);
+    else
+      k_fill<float><<<256, 256>>>(reinterpret_cast<float*>(s->conc), s->N, (float)c0);
+    if ((rc = gs_cuda_check(cudaDeviceSynchronize(), "init concentration")) != GS_OK) return fail(rc);
+    s->mass0 = (p->dtype == GS_DTYPE_F64 ? c0 : (double)(float)c0) * (double)s->N;
+  } else {
+    if ((rc = dalloc(&s->spec, fb * V, "spectrum")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->spec2, fb * 6, "stress spectra")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->stressbuf, fb * 6, "stress")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&s->defect, fb, "defect")) != GS_OK) return fail(rc);
   }
-  if ((rc = gs_cuda_check(cudaMalloc(&s->spec, fb * V), "cudaMalloc spectrum")) != GS_OK) return fail(rc);
   rc = p->dtype == GS_DTYPE_F64 ? build_twiddles<double>(s) : build_twiddles<float>(s);
   if (rc != GS_OK) return fail(rc);
-  s->partials_cap = (size_t)s->n0 * s->n1 + 1;
+  s->partials_cap = (size_t)s->n0 * s->n1 + 148 * 16 + 1;
   if ((rc = gs_cuda_check(cudaMalloc(&s->partials, s->partials_cap * ACC_N * sizeof(double)), "partials")) != GS_OK)
     return fail(rc);
   if ((rc = gs_cuda_check(cudaMalloc(&s->red, 64 * sizeof(double)), "reduce out")) != GS_OK) return fail(rc);
@@ -638,7 +932,24 @@ extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, s
     if (count != N * V) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, N * V);
     return upload(s, s->eta[s->cur], host, count, dtype);
   }
+  if (nm == "concentration") {
+    if (s->p.model != GS_MODEL_PRECIPITATE) return gs_set_error(GS_EINVAL, "concentration: not a precipitate model");
+    if (count != N) return gs_set_error(GS_EINVAL, "concentration: %zu values, expected %zu", count, N);
+    GS_TRY(upload(s, s->conc, host, count, dtype));
+    // FP64 mass of the values as stored on the device (the projection target)
+    double m = 0, cmp = 0;
+    for (size_t i = 0; i < N; ++i) {
+      double x = dtype == GS_DTYPE_F64 ? static_cast<const double*>(host)[i] : static_cast<const float*>(host)[i];
+      if (s->p.dtype == GS_DTYPE_F32) x = (double)(float)x;
+      const double t = m + x;
+      cmp += std::fabs(m) >= std::fabs(x) ? (m - t) + x : (x - t) + m;
+      m = t;
+    }
+    s->mass0 = m + cmp;
+    return GS_OK;
+  }
   if (nm == "defect") {
+    if (s->p.model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "defect is an input of the martensite model only");
     if (count != N) return gs_set_error(GS_EINVAL, "defect: %zu values, expected %zu", count, N);
     if (!s->defect) GS_CU(cudaMalloc(&s->defect, N * elt(s)), "cudaMalloc defect");
     return upload(s, s->defect, host, count, dtype);
@@ -686,6 +997,16 @@ extern "C" int gs_sim_get_field(gs_sim* s, const char* name, void* host, size_t 
     if (count != N) return gs_set_error(GS_EINVAL, "defect: %zu values, expected %zu", count, N);
     return download(s, s->defect, host, count, dtype);
   }
+  if (nm == "concentration") {
+    if (!s->conc) return gs_set_error(GS_EINVAL, "concentration: not a precipitate model");
+    if (count != N) return gs_set_error(GS_EINVAL, "concentration: %zu values, expected %zu", count, N);
+    return download(s, s->conc, host, count, dtype);
+  }
+  if (nm == "stress") {
+    if (!s->stressbuf) return gs_set_error(GS_EINVAL, "stress: not a stress model");
+    if (count != 6 * N) return gs_set_error(GS_EINVAL, "stress: %zu values, expected %zu", count, 6 * N);
+    return download(s, s->stressbuf, host, count, dtype);
+  }
   return gs_set_error(GS_EINVAL, "unknown field '%s'", name);
 }
 
@@ -712,8 +1033,15 @@ extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
   if (nsteps < 0) return gs_set_error(GS_EINVAL, "nsteps %d", nsteps);
   cudaStream_t st = pick_stream(s, stream);
   s->launches = 0;
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
   for (int i = 0; i < nsteps; ++i) {
-    int rc = s->p.dtype == GS_DTYPE_F64 ? mart_step<double>(s, st) : mart_step<float>(s, st);
+    int rc;
+    if (s->p.model == GS_MODEL_MART)
+      rc = f64 ? mart_step<double>(s, st) : mart_step<float>(s, st);
+    else if (s->p.model == GS_MODEL_PRECIPITATE)
+      rc = f64 ? precip_step<double>(s, st) : precip_step<float>(s, st);
+    else
+      rc = f64 ? stress_step<double>(s, st) : stress_step<float>(s, st);
     if (rc != GS_OK) return rc;
   }
   return GS_OK;
@@ -722,7 +1050,13 @@ extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
 extern "C" int gs_sim_stats(gs_sim* s, gs_stats* out, void* stream) {
   if (!s || !out) return gs_set_error(GS_EINVAL, "gs_sim_stats: null argument");
   cudaStream_t st = pick_stream(s, stream);
-  return s->p.dtype == GS_DTYPE_F64 ? mart_stats<double>(s, out, st) : mart_stats<float>(s, out, st);
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  if (s->p.model == GS_MODEL_MART) return f64 ? mart_stats<double>(s, out, st) : mart_stats<float>(s, out, st);
+  if (s->p.model == GS_MODEL_PRECIPITATE)
+    return f64 ? precip_stats<double>(s, out, st) : precip_stats<float>(s, out, st);
+  memset(out, 0, sizeof(*out));
+  out->step = s->step;
+  return GS_OK;
 }
 
 extern "C" int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes) {

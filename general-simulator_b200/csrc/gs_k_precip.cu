@@ -1,0 +1,66 @@
+// gs_k_precip.cu -- launchers of the z-inverse-to-real pass and of the
+// precipitate / stress real-space sweeps.
+#include "gs_launch.h"
+#include "gs_precip.cuh"
+
+namespace gs {
+
+template <typename T, int H> static cudaError_t zinv_n(ZinvArgs<T>& a, cudaStream_t s) {
+  using L = Line<T, H>;
+  long long lpc = 256 / L::P;
+  if (lpc < 1) lpc = 1;
+  if (lpc > a.nrows) lpc = a.nrows;
+  a.lpc = (int)lpc;
+  const size_t smem = (size_t)lpc * L::PAD * sizeof(cplx<T>);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv<T, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long grid = (a.nrows + lpc - 1) / lpc;
+  k_zinv<T, H><<<(unsigned)grid, (unsigned)(L::P * lpc), smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_zinv(ZinvArgs<T>& a, int H, cudaStream_t s) {
+  switch (H) {
+#define GS_C(N_) \
+  case N_:       \
+    return zinv_n<T, N_>(a, s);
+    GS_SIZE_CASES(GS_C)
+#undef GS_C
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+static unsigned grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+template <typename T> cudaError_t launch_precip_local(PrecipLocalArgs<T>& a, cudaStream_t s) {
+  k_precip_local<T><<<grid_for((a.N + 3) / 4, 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_defect(const T* eta, T* defect, long long N, int V, cudaStream_t s) {
+  k_defect<T><<<grid_for(N, 256), 256, 0, s>>>(eta, defect, N, V, (T)0.9);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_precip_stats(PrecipStatsArgs<T>& a, cudaStream_t s, int* nblocks) {
+  const unsigned g = grid_for(a.N, 256);
+  *nblocks = (int)g;
+  k_precip_stats<T><<<g, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+#define GS_INST(T)                                                                         \
+  template cudaError_t launch_zinv<T>(ZinvArgs<T>&, int, cudaStream_t);                    \
+  template cudaError_t launch_precip_local<T>(PrecipLocalArgs<T>&, cudaStream_t);          \
+  template cudaError_t launch_defect<T>(const T*, T*, long long, int, cudaStream_t);       \
+  template cudaError_t launch_precip_stats<T>(PrecipStatsArgs<T>&, cudaStream_t, int*);
+GS_INST(float)
+GS_INST(double)
+#undef GS_INST
+
+}  // namespace gs

@@ -1,19 +1,26 @@
-// gs_k_x.cu -- x pass (B(n) contraction): picks the field-count class.
+// gs_k_x.cu -- x pass: picks the field-count class of the per-point op.
 #include "gs_launch.h"
 #include "gs_passes.cuh"
 
 namespace gs {
 
-template <typename T, int FM, int GM> cudaError_t launch_x_class(XArgs<T>& a, cudaStream_t s);
+template <typename T, int FM, int GM, class Op> cudaError_t launch_x_class(XArgs<T>& a, cudaStream_t s);
 
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s) {
-  if (a.F <= 3 && a.G <= 3) return launch_x_class<T, 3, 3>(a, s);
-  if (a.F <= 5 && a.G <= 5) return launch_x_class<T, 5, 5>(a, s);
-  if (a.F <= 8 && a.G <= 6) return launch_x_class<T, 8, 6>(a, s);
-  return launch_x_class<T, 9, 9>(a, s);
+  if (a.F <= 3 && a.G <= 3) return launch_x_class<T, 3, 3, ContractOp>(a, s);
+  if (a.F <= 5 && a.G <= 5) return launch_x_class<T, 5, 5, ContractOp>(a, s);
+  if (a.F <= 8 && a.G <= 6) return launch_x_class<T, 8, 6, ContractOp>(a, s);
+  return launch_x_class<T, 9, 9, ContractOp>(a, s);
+}
+
+template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s) {
+  if (a.F <= 10 && a.G <= 5) return launch_x_class<T, 10, 5, PrecipOp>(a, s);
+  return launch_x_class<T, 18, 9, PrecipOp>(a, s);
 }
 
 template cudaError_t launch_xcontract<float>(XArgs<float>&, cudaStream_t);
 template cudaError_t launch_xcontract<double>(XArgs<double>&, cudaStream_t);
+template cudaError_t launch_xprecip<float>(XArgs<float>&, cudaStream_t);
+template cudaError_t launch_xprecip<double>(XArgs<double>&, cudaStream_t);
 
 }  // namespace gs

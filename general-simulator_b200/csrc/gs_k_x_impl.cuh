@@ -7,7 +7,7 @@
 
 namespace gs {
 
-template <typename T, int N0, int FM, int GM> static cudaError_t xc_n(XArgs<T>& a, cudaStream_t s) {
+template <typename T, int N0, int FM, int GM, class Op> static cudaError_t xc_n(XArgs<T>& a, cudaStream_t s) {
   using L = Line<T, N0>;
   const int groups = a.F > a.G ? a.F : a.G;
   // 8-column tiles for the FP32 hot sizes: a 3-field block then needs 384
@@ -28,22 +28,22 @@ template <typename T, int N0, int FM, int GM> static cudaError_t xc_n(XArgs<T>& 
   if constexpr (sizeof(T) == 4 && N0 >= 64) {
     if (tz == 8) {
       if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_xpass<T, N0, FM, GM, 8><<<grid, tz * L::P * groups, smem, s>>>(a);
+        cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 8, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_xpass<T, N0, FM, GM, 8, Op><<<grid, tz * L::P * groups, smem, s>>>(a);
       return cudaGetLastError();
     }
   }
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_xpass<T, N0, FM, GM, 0><<<grid, tz * L::P * groups, smem, s>>>(a);
+    cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 0, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_xpass<T, N0, FM, GM, 0, Op><<<grid, tz * L::P * groups, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <typename T, int FM, int GM> cudaError_t launch_x_class(XArgs<T>& a, cudaStream_t s) {
+template <typename T, int FM, int GM, class Op> cudaError_t launch_x_class(XArgs<T>& a, cudaStream_t s) {
   switch (a.n0) {
 #define GS_C(N_) \
   case N_:       \
-    return xc_n<T, N_, FM, GM>(a, s);
+    return xc_n<T, N_, FM, GM, Op>(a, s);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:

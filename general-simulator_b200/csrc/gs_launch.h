@@ -11,6 +11,9 @@ template <typename T> struct ZfwdArgs;
 template <typename T> struct YArgs;
 template <typename T> struct XArgs;
 template <typename T> struct MartArgs;
+template <typename T> struct ZinvArgs;
+template <typename T> struct PrecipLocalArgs;
+template <typename T> struct PrecipStatsArgs;
 
 // line lengths with a compiled plan
 bool size_supported(int n);
@@ -20,6 +23,11 @@ int pick_tz(int h);
 template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s);
 template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s);
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
+template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s);
+template <typename T> cudaError_t launch_zinv(ZinvArgs<T>& a, int H, cudaStream_t s);
+template <typename T> cudaError_t launch_precip_local(PrecipLocalArgs<T>& a, cudaStream_t s);
+template <typename T> cudaError_t launch_defect(const T* eta, T* defect, long long N, int V, cudaStream_t s);
+template <typename T> cudaError_t launch_precip_stats(PrecipStatsArgs<T>& a, cudaStream_t s, int* nblocks);
 // returns the number of blocks through nblocks (statistics partial rows)
 template <typename T> cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks);
 cudaError_t launch_reduce(const double* partials, int nb, int n, double* out, cudaStream_t s);

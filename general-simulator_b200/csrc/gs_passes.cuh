@@ -150,8 +150,8 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
 // z forward: real rows -> packed half spectrum, with a fused prologue.
 // ---------------------------------------------------------------------------
 template <typename T> struct ZfwdArgs {
-  const T* src[GS_MAXF];   // row source of each field (n0*n1 rows of n2)
-  int square[GS_MAXF];     // 1: transform src^2 (eta^2), 0: src
+  const T* src[2 * GS_MAXF];   // row source of each field (n0*n1 rows of n2)
+  int square[2 * GS_MAXF];     // 1: transform src^2 (eta^2), 0: src
   cplx<T>* dst;            // [F][n0][n1][h]
   long long rows_per_field;
   long long nrows;         // F * rows_per_field
@@ -312,21 +312,60 @@ __global__ void k_ypass(YArgs<T> a) {
 // so the F line FFTs of a tile run side by side.  The spectra meet in
 // shared memory for the contraction, which every thread of the block shares.
 // ---------------------------------------------------------------------------
+// Semi-implicit CH/AC update of the precipitate in k space
+// (src/dynamics_precipitate.cu:197-206,234-248): inputs [c, mu, eta_0, g_0,
+// eta_1, g_1, ...], outputs [c', eta'_0..V-1], with K(k) = sum of per-axis tables
+// (|k|^2 of the 3.14 vector in refcompat, the seven-point symbol otherwise).
+template <typename T> struct PrecipUpd {
+  int V, mass_proj;
+  T dtM, dtL, kc, ke;      // dt*M, dt*L, kappa_c, kappa_eta
+  T scale;                 // 1/N of the unnormalised transforms
+  const T* ktab[3];        // K contribution per canonical axis and index
+};
+
 template <typename T> struct XArgs {
   const cplx<T>* in;  // [F][n0][n1][h]
   cplx<T>* out;       // [G][n0][n1][h] (may alias in)
   int n0, n1, n2, h, tz, F, G, groups;
   const cplx<T>* tw;  // w_n0^m
   ElasticConst<T> ec;
+  PrecipUpd<T> pu;
+};
+
+// per-point operations of the x pass
+struct ContractOp {
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    contract_at<T, FM, GM>(a.ec, nn, ix, iy, iz, in, out);
+  }
+};
+struct PrecipOp {
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    const PrecipUpd<T>& u = a.pu;
+    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+    const T ic = u.scale / ((T)1 + u.dtM * u.kc * K * K);
+    const T ie = u.scale / ((T)1 + u.dtL * u.ke * K);
+#pragma unroll
+    for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
+    out[0] = (in[0] - in[1] * (u.dtM * K)) * ic;
+    if (u.mass_proj && ix == 0 && iy == 0 && iz == 0) out[0] = mk2((T)0, (T)0);
+    // inputs interleaved per variant: in[2 + 2p] = eta_p, in[3 + 2p] = g_p
+#pragma unroll
+    for (int p = 0; p < GM - 1; ++p)
+      if (p < u.V && 3 + 2 * p < FM) out[1 + p] = (in[2 + 2 * p] - in[3 + 2 * p] * u.dtL) * ie;
+  }
 };
 
 // threads per block of the x pass for a field-count class (FM, GM)
 template <int FM, int GM> struct XBounds {
   static constexpr int G = FM > GM ? FM : GM;
-  static constexpr int v = G <= 3 ? 768 : (G <= 5 ? 640 : 1024);
+  static constexpr int v = G <= 3 ? 768 : (G <= 10 ? 640 : 576);
 };
 
-template <typename T, int N0, int FM, int GM, int TZC>
+template <typename T, int N0, int FM, int GM, int TZC, class Op>
 __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   using L = Line<T, N0>;
   using V = cplx<T>;
@@ -384,7 +423,7 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
         V in[FM], out[GM];
 #pragma unroll
         for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pin[f * region] : mk2((T)0, (T)0);
-        contract_at<T, FM, GM>(a.ec, nn, kx, kyA, kzA, in, out);
+        Op::template apply<T, FM, GM>(a, nn, kx, kyA, kzA, in, out);
         V* pout = smb + kx * TZ + cc;
 #pragma unroll
         for (int g = 0; g < GM; ++g)
@@ -408,7 +447,7 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
             }
           }
           V out[GM];
-          contract_at<T, FM, GM>(a.ec, nn, kx, half ? kyB : kyA, half ? kzB : kzA, in, out);
+          Op::template apply<T, FM, GM>(a, nn, kx, half ? kyB : kyA, half ? kzB : kzA, in, out);
 #pragma unroll
           for (int g = 0; g < GM; ++g) res[half][g] = out[g];
         }
@@ -481,6 +520,47 @@ __device__ __forceinline__ void zinv_row(const cplx<T>* __restrict__ srow, bool 
   __syncthreads();
   auto sm = [sl](int pos) -> V& { return sl[pos]; };
   L::template run<1>(v, t, sm, tw_h);
+}
+
+// ---------------------------------------------------------------------------
+// z inverse to real rows: spectra [F][rows][h] -> dst[f] rows of n2 reals.
+// One field may get an FP64 offset added before rounding (the mass
+// projection of the concentration).
+// ---------------------------------------------------------------------------
+template <typename T> struct ZinvArgs {
+  const cplx<T>* spec;
+  T* dst[GS_MAXG + 1];
+  long long rows_per_field, nrows;  // nrows = F * rows_per_field
+  int lpc;
+  const cplx<T>* tw_h;
+  const cplx<T>* tw_n2;
+  int offset_field;  // -1: none
+  double offset;
+};
+
+template <typename T, int H>
+__global__ void k_zinv(ZinvArgs<T> a) {
+  using L = Line<T, H>;
+  using V = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* smb = reinterpret_cast<V*>(smraw);
+  const int t = threadIdx.x % L::P, line = threadIdx.x / L::P;
+  const long long row = (long long)blockIdx.x * a.lpc + line;
+  const bool act = row < a.nrows;
+  V* sl = smb + line * L::PAD;
+  V r[L::R1];
+  zinv_row<T, H>(a.spec + (act ? row : 0) * H, act, t, sl, a.tw_h, a.tw_n2, r);
+  if (!act) return;
+  const int f = (int)(row / a.rows_per_field);
+  const long long rin = row - (long long)f * a.rows_per_field;
+  V* dst = reinterpret_cast<V*>(a.dst[f]) + rin * H;
+  const bool off = f == a.offset_field;
+#pragma unroll
+  for (int i = 0; i < L::R1; ++i) {
+    V x = r[i];
+    if (off) x = mk2((T)((double)x.x + a.offset), (T)((double)x.y + a.offset));
+    dst[L::out_pos(t, i)] = x;
+  }
 }
 
 }  // namespace gs

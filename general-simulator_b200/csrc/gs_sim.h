@@ -22,6 +22,12 @@ struct gs_sim {
   void* defect = nullptr; // [N]
   void* K = nullptr;      // dislocation coupling sigma(x):eps_p, [V][N]
   void* conc = nullptr;   // concentration [N]
+  void* rbuf = nullptr;   // elastic potentials R_a [F][N] (precipitate)
+  void* mubuf = nullptr;  // mu_c and g_p [1 + V][N] (precipitate)
+  void* stressbuf = nullptr;  // stress components [6][N] (stress model)
+  void* ktab = nullptr;   // K(k) per canonical axis (precipitate)
+  size_t ktab_off[3] = {0, 0, 0};
+  double mass0 = 0;       // FP64 sum of the initial concentration
   void* tw = nullptr;     // twiddle tables
   size_t tw_off[4] = {0, 0, 0, 0};  // n2, h, n1, n0
   double* partials = nullptr;

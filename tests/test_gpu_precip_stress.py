@@ -1,0 +1,152 @@
+"""Parity of the CUDA precipitate and stress models (through the C ABI) with
+the FP64 oracle and with the reference's own outputs (tests/golden)."""
+import numpy as np
+import pytest
+
+import refcases as rc
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+F64, F32 = 1, 0
+
+
+def run_precip(gb, p, c0, e0, steps):
+    s = gb.Sim(p)
+    try:
+        s.set_field("concentration", c0)
+        s.set_field("eta", e0)
+        s.step(steps)
+        return s.concentration(), s.eta()
+    finally:
+        s.close()
+
+
+def precip_base(gb, shape, dtype, V=4):
+    p = gb.precip3d_params(16, dtype=dtype)
+    p.nx, p.ny, p.nz = shape
+    if V != 4:
+        p.nvariants = V
+        p.set_eigenstrain(gb.tetragonal_eigenstrains(V, 0.005, -0.0025))
+    return p
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (8, 12, 32), (16, 1, 24), (1, 32, 16)])
+def test_precip_baseline_fp64(gb, orc, shape):
+    p = precip_base(gb, shape, F64)
+    c0 = gb.initial_c(p, 2)
+    e0 = gb.initial_eta(p, 3, 0.4)
+    cr, er = orc.precip_run(p, c0, e0, 3)
+    cg, eg = run_precip(gb, p, c0, e0, 3)
+    assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
+    assert rel_l2(er, e0) > 1e-3
+
+
+def test_precip_baseline_noise_fp64(gb, orc):
+    p = precip_base(gb, (8, 8, 16), F64)
+    p.noise_amp = 1e-2
+    p.seed = 77
+    c0 = gb.initial_c(p, 4)
+    e0 = gb.initial_eta(p, 5, 0.4)
+    cr, er = orc.precip_run(p, c0, e0, 2)
+    cg, eg = run_precip(gb, p, c0, e0, 2)
+    assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
+
+
+@pytest.mark.parametrize("V", [1, 2, 3])
+def test_precip_variant_counts(gb, orc, V):
+    p = precip_base(gb, (8, 8, 8), F64, V=V)
+    c0 = gb.initial_c(p, 6)
+    e0 = gb.initial_eta(p, 7, 0.4)
+    cr, er = orc.precip_run(p, c0, e0, 2)
+    cg, eg = run_precip(gb, p, c0, e0, 2)
+    assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
+
+
+def test_precip_refcompat_fp64(gb, orc):
+    p = rc.precip_params(gb)
+    p.dtype = F64
+    d = rc.load("precipitate")
+    c0, e0 = d["con0"].astype(np.float64), d["eta0"].astype(np.float64)
+    cr, er = orc.precip_run(p, c0, e0, 3)
+    cg, eg = run_precip(gb, p, c0, e0, 3)
+    assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
+
+
+def test_precip_fp32_matches_reference_fixture(gb):
+    p = rc.precip_params(gb)
+    d = rc.load("precipitate")
+    s = gb.Sim(p)
+    s.set_field("concentration", d["con0"])
+    s.set_field("eta", d["eta0"])
+    for i in range(5):
+        s.step(1)
+        assert rel_l2(s.eta(), d["eta_steps"][i]) < 2e-6
+        assert rel_l2(s.concentration(), d["con_steps"][i]) < 2e-6
+    s.close()
+
+
+def test_precip_fp32_mass_drift(gb):
+    p = precip_base(gb, (32, 32, 32), F32)
+    c0 = gb.initial_c(p, 2).astype(np.float32)
+    e0 = gb.initial_eta(p, 3, 0.3).astype(np.float32)
+    s = gb.Sim(p)
+    s.set_field("concentration", c0)
+    s.set_field("eta", e0)
+    m0 = c0.astype(np.float64).sum()
+    st0 = s.stats()
+    assert abs(st0["mass"] - m0) <= 1e-12 * m0
+    s.step(300)
+    st = s.stats()
+    c = s.concentration()
+    s.close()
+    assert abs(st["mass"] - m0) / m0 < 1e-10
+    assert abs(c.sum() - m0) / m0 < 1e-10
+
+
+def test_precip_stats_match_oracle(gb, orc):
+    p = precip_base(gb, (16, 16, 8), F64)
+    c0 = gb.initial_c(p, 8)
+    e0 = gb.initial_eta(p, 9, 0.8)
+    s = gb.Sim(p)
+    s.set_field("concentration", c0)
+    s.set_field("eta", e0)
+    st = s.stats()
+    s.close()
+    ref = orc.precip_stats(p, c0, e0)
+    for k in ["mass", "c_mean", "eta_mean", "e_el", "e_chem", "e_grad", "e_tot"]:
+        assert abs(st[k] - ref[k]) <= 1e-10 * max(1.0, abs(ref[k])), k
+    assert np.allclose(st["eta2"], ref["eta2"], rtol=1e-12) and st["vf"] == ref["vf"]
+
+
+def run_stress(gb, p, e0):
+    s = gb.Sim(p)
+    try:
+        s.set_field("eta", e0)
+        s.step(1)
+        n = p.nx * p.ny * p.nz
+        return (s.get_field("stress", 6 * n).reshape(6, p.nx, p.ny, p.nz),
+                s.get_field("defect", n).reshape(p.nx, p.ny, p.nz))
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_stress_fp64_matches_oracle(gb, orc, mode):
+    p = gb.default_params(gb.GS_MODEL_STRESS, mode)
+    p.dtype = F64
+    p.nx, p.ny, p.nz = 12, 16, 8
+    p.nvariants = 3
+    p.set_eigenstrain(gb.tetragonal_eigenstrains(3, 0.01, -0.004))
+    e0 = gb.initial_eta(p, 10, 1.0)
+    sr, dr = orc.stress(p, e0)
+    sg, dg = run_stress(gb, p, e0)
+    assert rel_l2(sg, sr) < 1e-11
+    assert np.array_equal(dg, dr)
+
+
+def test_stress_fp32_matches_reference_fixture(gb):
+    d = rc.load("stress")
+    p = rc.stress_params(gb, str(d["log"]))
+    sg, dg = run_stress(gb, p, d["eta0"])
+    assert rel_l2(sg, d["stress"]) < 2e-6
+    assert np.array_equal(dg, d["defect"])
