@@ -68,6 +68,20 @@ def build_lib(jobs: int = 8, verbose: bool = False) -> str:
     return LIB
 
 
+HOST_SOURCES = ["gs_script.cpp", "gs_driver.cpp", "gs_plugins.cpp", "gs_main.cpp"]
+GSI = os.path.join(HERE, "gsi")
+
+
+def build_frontend() -> str:
+    """The script interpreter (C++17), linked against libgsb200.so."""
+    srcs = [os.path.join(HOST, f) for f in HOST_SOURCES]
+    deps = srcs + [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")] + [LIB]
+    if _stale(GSI, deps):
+        _run(["g++", "-O2", "-std=c++17", "-Wall", "-o", GSI, *srcs, "-L" + HERE, "-lgsb200",
+              "-Wl,-rpath,$ORIGIN"])
+    return GSI
+
+
 def build_oracle() -> str:
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
     return os.path.join(ROOT, "oracle", "liboracle.so")
@@ -75,6 +89,7 @@ def build_oracle() -> str:
 
 def build_all(jobs: int = 8) -> None:
     build_lib(jobs)
+    build_frontend()
     build_oracle()
 
 

@@ -53,6 +53,11 @@ extern "C" int gs_version(void) { return GS_CAPI_VERSION; }
 extern "C" size_t gs_sizeof_params(void) { return sizeof(gs_params); }
 extern "C" size_t gs_sizeof_stats(void) { return sizeof(gs_stats); }
 
+extern "C" int gs_set_device(int device) {
+  GS_CU(cudaSetDevice(device), "cudaSetDevice");
+  return GS_OK;
+}
+
 extern "C" int gs_last_error(char* buf, size_t len) {
   if (!buf || len == 0) return GS_EINVAL;
   snprintf(buf, len, "%s", g_err);

@@ -138,6 +138,9 @@ size_t gs_sizeof_params(void);
 size_t gs_sizeof_stats(void);
 /* Copy the calling thread's last error message into buf. */
 int gs_last_error(char* buf, size_t len);
+/* Select the CUDA device of the calling thread (the script command
+ * `device N` and `gsi script N`, src/input.cu:244-251, src/main.cu:23-28). */
+int gs_set_device(int device);
 /* Fill p with the defaults of model/mode (the reference's defaults for
  * GS_MODE_REFCOMPAT, src/dynamics_mart.cu:20-27,80-89 and
  * src/dynamics_precipitate.cu:21-29,55; the BASELINE configs otherwise). */

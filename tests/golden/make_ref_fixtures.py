@@ -65,25 +65,18 @@ def read_binary_field(path: str) -> np.ndarray:
     return vals.reshape(dims)
 
 
-def run_gsi(workdir: str, script: str, name: str) -> str:
-    path = os.path.join(workdir, name)
-    with open(path, "w") as f:
-        f.write(script)
-    r = subprocess.run([GSI, name], cwd=workdir, capture_output=True, text=True, timeout=600)
-    return r.stdout
-
-
-def case_mart(out: str) -> None:
+def mart_inputs():
     rng = np.random.default_rng(7)
     nx, ny, nz = SHAPE
     eta = rng.uniform(0.0, 0.1, (4, nx, ny, nz)).astype(np.float32)
     ds = rng.uniform(-0.05, 0.05, (6, nx, ny, nz)).astype(np.float32)
     defect = (rng.random((nx, ny, nz)) < 0.05).astype(np.float32)
-    with tempfile.TemporaryDirectory() as d:
-        write_text_field(os.path.join(d, "data.eta"), eta)
-        write_text_field(os.path.join(d, "data.stress"), ds)
-        write_text_field(os.path.join(d, "data.defect"), defect)
-        script = f"""sys mart
+    return {"data.eta": eta, "data.stress": ds, "data.defect": defect}
+
+
+def mart_script() -> str:
+    nx, ny, nz = SHAPE
+    return f"""sys mart
 set binary off
 set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
 set deltatime 0.01
@@ -101,21 +94,19 @@ dump dumpdir 5 eta
 set fix temperature 460 300
 run 5
 """
-        log = run_gsi(d, script, "in.mart16")
-        dumps = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"eta.{i}.data")) for i in range(1, 6)])
-    np.savez_compressed(os.path.join(out, "ref_mart.npz"), eta0=eta, dislocationstress=ds, defect=defect,
-                        eta_steps=dumps, log=np.array(log))
 
 
-def case_precipitate(out: str) -> None:
+def precip_inputs():
     rng = np.random.default_rng(8)
     nx, ny, nz = SHAPE
     eta = rng.uniform(0.0, 0.5, (4, nx, ny, nz)).astype(np.float32)
     con = (0.2 + rng.uniform(-0.02, 0.02, (nx, ny, nz))).astype(np.float32)
-    with tempfile.TemporaryDirectory() as d:
-        write_text_field(os.path.join(d, "data.eta"), eta)
-        write_text_field(os.path.join(d, "data.con"), con)
-        script = f"""sys precipitate
+    return {"data.eta": eta, "data.con": con}
+
+
+def precip_script() -> str:
+    nx, ny, nz = SHAPE
+    return f"""sys precipitate
 set binary off
 set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
 set deltatime 0.1
@@ -136,20 +127,17 @@ set binary on
 dump dumpdir 5 eta concentration
 run 5
 """
-        log = run_gsi(d, script, "in.precipitate16")
-        e = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"eta.{i}.data")) for i in range(1, 6)])
-        c = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"concentration.{i}.data")) for i in range(1, 6)])
-    np.savez_compressed(os.path.join(out, "ref_precipitate.npz"), eta0=eta, con0=con, eta_steps=e, con_steps=c,
-                        log=np.array(log))
 
 
-def case_stress(out: str) -> None:
+def stress_inputs():
     rng = np.random.default_rng(9)
     nx, ny, nz = SHAPE
-    eta = rng.uniform(0.0, 1.0, (4, nx, ny, nz)).astype(np.float32)
-    with tempfile.TemporaryDirectory() as d:
-        write_text_field(os.path.join(d, "data.eta"), eta)
-        script = f"""sys stress
+    return {"data.eta": rng.uniform(0.0, 1.0, (4, nx, ny, nz)).astype(np.float32)}
+
+
+def stress_script() -> str:
+    nx, ny, nz = SHAPE
+    return f"""sys stress
 set binary off
 set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
 read eta data.eta
@@ -160,15 +148,54 @@ set binary on
 dump dumpdir 1 stress defect
 run 1
 """
-        log = run_gsi(d, script, "in.stress16")
+
+
+def run_case(gsi: str, workdir: str, inputs: dict, script: str, name: str) -> str:
+    """Write the inputs (text format) and the script, run a gsi binary."""
+    for fn, arr in inputs.items():
+        write_text_field(os.path.join(workdir, fn), arr)
+    path = os.path.join(workdir, name)
+    with open(path, "w") as f:
+        f.write(script)
+    r = subprocess.run([gsi, name], cwd=workdir, capture_output=True, text=True, timeout=600)
+    return r.stdout
+
+
+def case_mart(out: str) -> None:
+    inputs = mart_inputs()
+    with tempfile.TemporaryDirectory() as d:
+        log = run_case(GSI, d, inputs, mart_script(), "in.mart16")
+        dumps = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"eta.{i}.data")) for i in range(1, 6)])
+    np.savez_compressed(os.path.join(out, "ref_mart.npz"), eta0=inputs["data.eta"],
+                        dislocationstress=inputs["data.stress"], defect=inputs["data.defect"],
+                        eta_steps=dumps, log=np.array(log))
+
+
+def case_precipitate(out: str) -> None:
+    inputs = precip_inputs()
+    with tempfile.TemporaryDirectory() as d:
+        log = run_case(GSI, d, inputs, precip_script(), "in.precipitate16")
+        e = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"eta.{i}.data")) for i in range(1, 6)])
+        c = np.stack([read_binary_field(os.path.join(d, "dumpdir", f"concentration.{i}.data")) for i in range(1, 6)])
+    np.savez_compressed(os.path.join(out, "ref_precipitate.npz"), eta0=inputs["data.eta"], con0=inputs["data.con"],
+                        eta_steps=e, con_steps=c, log=np.array(log))
+
+
+def case_stress(out: str) -> None:
+    inputs = stress_inputs()
+    with tempfile.TemporaryDirectory() as d:
+        log = run_case(GSI, d, inputs, stress_script(), "in.stress16")
         stress = read_binary_field(os.path.join(d, "dumpdir", "stress.1.data"))
         defect = read_binary_field(os.path.join(d, "dumpdir", "defect.1.data"))
-    np.savez_compressed(os.path.join(out, "ref_stress.npz"), eta0=eta, stress=stress, defect=defect, log=np.array(log))
+    np.savez_compressed(os.path.join(out, "ref_stress.npz"), eta0=inputs["data.eta"], stress=stress, defect=defect,
+                        log=np.array(log))
 
 
 def case_frontend(out: str) -> None:
-    for name in ["in.if.loop.while", "in.pow"]:
+    for name in ["in.if.loop.while", "in.pow", "in.expr"]:
         src = os.path.join(os.environ.get("REF", "/root/reference"), "scripts", name)
+        if not os.path.exists(src):
+            src = os.path.join(HERE, "scripts", name)  # project scripts in the reference's language
         with tempfile.TemporaryDirectory() as d:
             shutil.copy(src, os.path.join(d, name))
             r = subprocess.run([GSI, name], cwd=d, capture_output=True, text=True, timeout=60)

@@ -1,0 +1,153 @@
+"""The C++ script front end (general-simulator_b200/gsi) against the
+reference: known-answer scripts byte for byte on CPU, the three physics
+scripts against the reference's own outputs on the GPU."""
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import refcases as rc
+from conftest import PKG, ROOT, rel_l2
+
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+import make_ref_fixtures as mf  # noqa: E402
+
+GSI = os.path.join(PKG, "gsi")
+
+
+@pytest.fixture(scope="module")
+def gsi():
+    if not os.path.exists(GSI):
+        import build
+
+        build.build_frontend()
+    return GSI
+
+
+def run_script(gsi, tmp_path, name, text, inputs=None):
+    for fn, arr in (inputs or {}).items():
+        mf.write_text_field(str(tmp_path / fn), arr)
+    (tmp_path / name).write_text(text)
+    r = subprocess.run([gsi, name], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    return r.stdout
+
+
+# the reference's front-end scripts, recorded from its own binary
+KAT_IF_LOOP_WHILE = """########################################################
+set log off
+expr a=3
+loop (a*2)
+  print {a}
+  :a=a-1
+end
+print {a}
+
+########################################################
+:a=3
+while a>0
+  expr a=a-1
+  print {a}
+end
+print {a}
+
+########################################################
+:a=2
+if (a>3)
+  print {a*9^2}
+else
+  print {a^2}
+end
+"""
+
+KAT_POW = """########################################################
+sys pow
+########################################################
+expr total_step=20
+########################################################
+set x 2
+########################################################
+readhere matrix
+2 3 3
+3 9 8
+1 2 3
+6 5 4
+########################################################
+info {total_step} x sum_of_matrix
+dump dump_pow_matrix {total_step} matrix
+########################################################
+run {total_step}
+"""
+
+
+@pytest.mark.parametrize("name,text,golden", [("in.if.loop.while", KAT_IF_LOOP_WHILE, "frontend_in_if_loop_while.txt"),
+                                              ("in.pow", KAT_POW, "frontend_in_pow.txt")])
+def test_known_answer_scripts_identical(gsi, tmp_path, name, text, golden):
+    out = run_script(gsi, tmp_path, name, text)
+    ref = open(os.path.join(rc.GOLDEN, golden)).read()
+    assert out == ref
+    assert (tmp_path / (name + ".log")).read_text() == ref  # the log tee
+
+
+def test_pow_dump_files(gsi, tmp_path):
+    run_script(gsi, tmp_path, "in.pow", KAT_POW)
+    f = (tmp_path / "dump_pow_matrix" / "matrix.20.data").read_text().split()
+    assert f[:3] == ["2", "3", "3"]
+    assert float(f[3]) == pytest.approx(3 * 2 ** 20, rel=1e-6)
+
+
+def test_expressions_and_blocks(gsi, tmp_path):
+    # arithmetic, $globals, nested loops, if/else, division by zero and the
+    # reference's own reading of `z+=4` (split at the later `=`: assigns "z+")
+    text = open(os.path.join(rc.GOLDEN, "scripts", "in.expr")).read()
+    out = run_script(gsi, tmp_path, "in.expr", text)
+    assert out == open(os.path.join(rc.GOLDEN, "frontend_in_expr.txt")).read()
+
+
+def test_errors_are_reported(gsi, tmp_path):
+    out = run_script(gsi, tmp_path, "in.e", "sys nosuch\n")
+    assert 'Error: unknown system "nosuch"' in out and "Error: error in command" in out
+    out = run_script(gsi, tmp_path, "in.e2", "run 3\n")
+    assert "Error: system not set" in out
+    out = run_script(gsi, tmp_path, "in.e3", "sys mart\nrun 1\n")
+    assert "strain tensor does not set" in out
+
+
+@pytest.mark.gpu
+def test_mart_script_matches_reference(gsi, tmp_path):
+    out = run_script(gsi, tmp_path, "in.mart16", mf.mart_script(), mf.mart_inputs())
+    mine = rc.info_rows(out)
+    ref = rc.info_rows(str(rc.load("mart")["log"]))
+    assert len(mine) == 5
+    for a, b in zip(mine, ref):
+        assert a[0] == b[0]  # temperature
+        for j in (1, 3, 4, 5):  # eta, chemical, elastic, dislocation means
+            assert abs(a[j] - b[j]) <= 2e-5 * abs(b[j]), (j, a[j], b[j])
+    # unlike the reference (stale host copy), the dump holds the evolved field
+    d = mf.read_binary_field(str(tmp_path / "dumpdir" / "eta.5.data"))
+    assert not np.array_equal(d, mf.mart_inputs()["data.eta"])
+
+
+@pytest.mark.gpu
+def test_precipitate_script_matches_reference(gsi, tmp_path):
+    run_script(gsi, tmp_path, "in.precipitate16", mf.precip_script(), mf.precip_inputs())
+    ref = rc.load("precipitate")
+    for i in range(1, 6):
+        e = mf.read_binary_field(str(tmp_path / "dumpdir" / f"eta.{i}.data"))
+        c = mf.read_binary_field(str(tmp_path / "dumpdir" / f"concentration.{i}.data"))
+        assert rel_l2(e, ref["eta_steps"][i - 1]) < 2e-6
+        assert rel_l2(c, ref["con_steps"][i - 1]) < 2e-6
+
+
+@pytest.mark.gpu
+def test_stress_script_matches_reference(gsi, tmp_path):
+    out = run_script(gsi, tmp_path, "in.stress16", mf.stress_script(), mf.stress_inputs())
+    ref = rc.load("stress")
+    assert out[out.find(">>>writehere"):out.find(">>>set binary on")] == \
+        str(ref["log"])[str(ref["log"]).find(">>>writehere"):str(ref["log"]).find(">>>set binary on")]
+    s = mf.read_binary_field(str(tmp_path / "dumpdir" / "stress.1.data"))
+    d = mf.read_binary_field(str(tmp_path / "dumpdir" / "defect.1.data"))
+    assert rel_l2(s, ref["stress"]) < 2e-6
+    assert np.array_equal(d, ref["defect"])
