@@ -335,8 +335,11 @@ static double contract33(const double a[3][3], const double b[3][3]) {
   return s;
 }
 
-template <typename T> void build_mart(const gs_sim* s, MartConst<T>& mc) {
-  const gs_params& p = s->p;
+template <typename T> static void build_mart_p(const gs_sim* s, const gs_params& p, int64_t step, MartConst<T>& mc);
+
+template <typename T> void build_mart(const gs_sim* s, MartConst<T>& mc) { build_mart_p<T>(s, s->p, s->step, mc); }
+
+template <typename T> static void build_mart_p(const gs_sim* s, const gs_params& p, int64_t step, MartConst<T>& mc) {
   memset(&mc, 0, sizeof(mc));
   const bool ref = p.mode == GS_MODE_REFCOMPAT;
   mc.V = p.nvariants;
@@ -380,7 +383,7 @@ template <typename T> void build_mart(const gs_sim* s, MartConst<T>& mc) {
   mc.k0 = (uint32_t)(p.seed & 0xffffffffu);
   mc.k1 = (uint32_t)(p.seed >> 32);
   mc.sim = p.sim_id;
-  mc.step = (uint32_t)s->step;
+  mc.step = (uint32_t)step;
 }
 
 // twiddle tables w_n^m = exp(-2 pi i m / n), m < n, for n2, h, n1, n0
@@ -1115,4 +1118,312 @@ extern "C" int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int
   }
   *npass = n;
   return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched ensembles: many independent martensite simulations, one launch per
+// pass per shape group, optionally replayed as a captured CUDA graph
+// ---------------------------------------------------------------------------
+struct gs_batch {
+  std::vector<gs_sim*> groups;
+  std::vector<std::pair<int, int>> where;  // sim -> (group, slot)
+  cudaStream_t stream = nullptr;
+  int use_graph = 0;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t exec_stream = nullptr;
+  std::vector<int> exec_cur;  // which field of each pair the graph reads first
+  int64_t launches = 0;
+};
+
+// ratio r with b = r a for every eigenstrain component (-1 if not proportional)
+static double strain_ratio(const gs_params& a, const gs_params& b) {
+  double na = 0, dot = 0;
+  for (int v = 0; v < a.nvariants; ++v)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        na += a.eigenstrain[v][i][j] * a.eigenstrain[v][i][j];
+        dot += a.eigenstrain[v][i][j] * b.eigenstrain[v][i][j];
+      }
+  if (na == 0) return -1;
+  const double r = dot / na;
+  for (int v = 0; v < a.nvariants; ++v)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        if (std::fabs(b.eigenstrain[v][i][j] - r * a.eigenstrain[v][i][j]) > 1e-12 * (1 + std::fabs(r)))
+          return -1;
+  return r;
+}
+
+static bool same_group(const gs_params& a, const gs_params& b) {
+  return a.model == b.model && a.mode == b.mode && a.dtype == b.dtype && a.nvariants == b.nvariants &&
+         a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.dx == b.dx && a.dy == b.dy && a.dz == b.dz &&
+         a.dt == b.dt && memcmp(a.cijkl, b.cijkl, sizeof(a.cijkl)) == 0 && strain_ratio(a, b) > 0;
+}
+
+template <typename T> static int batch_upload_consts(gs_sim* g) {
+  std::vector<MartConst<T>> mcs(g->nb);
+  std::vector<T> sc(g->nb);
+  for (int k = 0; k < g->nb; ++k) {
+    build_mart_p<T>(g, g->bp[k], g->bstep[k], mcs[k]);
+    const double r = strain_ratio(g->bp[0], g->bp[k]);
+    sc[k] = (T)(r * r);  // B is bilinear in the eigenstrains
+  }
+  GS_CU(cudaMemcpy(g->d_mcs, mcs.data(), sizeof(MartConst<T>) * g->nb, cudaMemcpyHostToDevice), "upload constants");
+  GS_CU(cudaMemcpy(g->d_simscale, sc.data(), sizeof(T) * g->nb, cudaMemcpyHostToDevice), "upload scales");
+  return GS_OK;
+}
+
+template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
+  const int V = g->p.nvariants, VT = V * g->nb;
+  const long long rows = (long long)g->n0 * g->n1;
+  T* in = reinterpret_cast<T*>(g->eta[g->cur]);
+  T* out = reinterpret_cast<T*>(g->eta[g->cur ^ 1]);
+  ZfwdArgs<T> za;
+  memset(&za, 0, sizeof(za));
+  za.src0 = in;
+  za.fstride = g->N;
+  za.square0 = 1;
+  za.dst = reinterpret_cast<cplx<T>*>(g->spec);
+  za.rows_per_field = rows;
+  za.nrows = rows * VT;
+  za.tw_h = twp<T>(g, 1);
+  za.tw_n2 = twp<T>(g, 0);
+  GS_CU(launch_zfwd<T>(za, g->h, st), "batch z forward");
+  YArgs<T> ya;
+  ya.spec = reinterpret_cast<cplx<T>*>(g->spec);
+  ya.n0 = g->n0;
+  ya.n1 = g->n1;
+  ya.h = g->h;
+  ya.tw = twp<T>(g, 2);
+  GS_CU(launch_ypass<T>(ya, g->n1, VT, -1, st), "batch y forward");
+  XArgs<T> xa;
+  memset(&xa, 0, sizeof(xa));
+  xa.in = reinterpret_cast<cplx<T>*>(g->spec);
+  xa.out = reinterpret_cast<cplx<T>*>(g->spec);
+  xa.n0 = g->n0;
+  xa.n1 = g->n1;
+  xa.n2 = g->n2;
+  xa.h = g->h;
+  xa.F = V;
+  xa.G = V;
+  xa.nsim = g->nb;
+  xa.simscale = reinterpret_cast<const T*>(g->d_simscale);
+  xa.tw = twp<T>(g, 3);
+  build_elastic<T>(g, 0, 1.0 / (double)g->N, xa.ec);
+  GS_CU(launch_xcontract<T>(xa, st), "batch x pass");
+  GS_CU(launch_ypass<T>(ya, g->n1, VT, 1, st), "batch y inverse");
+  MartArgs<T> ma;
+  fill_mart_args<T>(g, ma, in, out);
+  ma.mcs = reinterpret_cast<MartConst<T>*>(g->d_mcs);
+  GS_CU(launch_mart_update<T>(ma, g->h, false, st, nullptr, g->nb), "batch update");
+  GS_CU(launch_bump_step<T>(reinterpret_cast<MartConst<T>*>(g->d_mcs), g->nb, st), "batch step counter");
+  g->launches += 4 + (g->n1 > 1 ? 2 : 0);
+  g->cur ^= 1;
+  g->step += 1;
+  for (auto& k : g->bstep) k += 1;
+  return GS_OK;
+}
+
+static int batch_step_once(gs_batch* b, cudaStream_t st) {
+  for (gs_sim* g : b->groups) {
+    int rc = g->p.dtype == GS_DTYPE_F64 ? batch_group_step<double>(g, st) : batch_group_step<float>(g, st);
+    if (rc != GS_OK) return rc;
+  }
+  return GS_OK;
+}
+
+extern "C" int gs_batch_create(const gs_params* params, int nsims, gs_batch** out) {
+  if (!params || !out || nsims < 1) return gs_set_error(GS_EINVAL, "gs_batch_create: bad arguments");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return gs_set_error(GS_ENODEV, "no CUDA device visible");
+  }
+  gs_batch* b = new gs_batch();
+  auto fail = [&](int rc) {
+    gs_batch_destroy(b);
+    return rc;
+  };
+  for (int i = 0; i < nsims; ++i) {
+    const gs_params& p = params[i];
+    if (p.model != GS_MODEL_MART) return fail(gs_set_error(GS_ENOTSUP, "batches hold martensite simulations"));
+    if (p.nvariants < 1 || p.nvariants > GS_MAX_V) return fail(gs_set_error(GS_EINVAL, "sim %d: nvariants", i));
+    int gi = -1;
+    for (size_t k = 0; k < b->groups.size(); ++k)
+      if (same_group(b->groups[k]->bp[0], p)) gi = (int)k;
+    if (gi < 0) {
+      gs_sim* g = new gs_sim();
+      g->p = p;
+      g->nb = 0;
+      int rc = canonicalize(g);
+      if (rc != GS_OK) {
+        delete g;
+        return fail(rc);
+      }
+      b->groups.push_back(g);
+      gi = (int)b->groups.size() - 1;
+    }
+    gs_sim* g = b->groups[gi];
+    b->where.push_back({gi, g->nb});
+    g->bp.push_back(p);
+    g->bstep.push_back(0);
+    g->nb += 1;
+  }
+  if (gs_cuda_check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream") != GS_OK)
+    return fail(GS_ECUDA);
+  for (gs_sim* g : b->groups) {
+    const size_t fb = (size_t)g->N * elt(g) * g->p.nvariants * g->nb;
+    int rc;
+    if ((rc = dalloc(&g->eta[0], fb, "batch eta")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&g->eta[1], fb, "batch eta pair")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&g->spec, fb, "batch spectrum")) != GS_OK) return fail(rc);
+    const size_t mcb = g->p.dtype == GS_DTYPE_F64 ? sizeof(MartConst<double>) : sizeof(MartConst<float>);
+    if ((rc = dalloc(&g->d_mcs, mcb * g->nb, "batch constants")) != GS_OK) return fail(rc);
+    if ((rc = dalloc(&g->d_simscale, elt(g) * g->nb, "batch scales")) != GS_OK) return fail(rc);
+    rc = g->p.dtype == GS_DTYPE_F64 ? build_twiddles<double>(g) : build_twiddles<float>(g);
+    if (rc != GS_OK) return fail(rc);
+    rc = g->p.dtype == GS_DTYPE_F64 ? batch_upload_consts<double>(g) : batch_upload_consts<float>(g);
+    if (rc != GS_OK) return fail(rc);
+    g->partials_cap = (size_t)g->n0 * g->n1 + 148 * 16 + 1;
+    if ((rc = gs_cuda_check(cudaMalloc(&g->partials, g->partials_cap * ACC_N * sizeof(double)), "partials")) != GS_OK)
+      return fail(rc);
+    if ((rc = gs_cuda_check(cudaMalloc(&g->red, 64 * sizeof(double)), "reduce out")) != GS_OK) return fail(rc);
+    g->own_stream = nullptr;
+  }
+  *out = b;
+  return GS_OK;
+}
+
+extern "C" int gs_batch_destroy(gs_batch* b) {
+  if (!b) return GS_OK;
+  cudaDeviceSynchronize();
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (gs_sim* g : b->groups) {
+    if (g->d_mcs) cudaFree(g->d_mcs);
+    if (g->d_simscale) cudaFree(g->d_simscale);
+    free_sim(g);
+  }
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return GS_OK;
+}
+
+extern "C" int gs_batch_groups(const gs_batch* b) { return b ? (int)b->groups.size() : 0; }
+extern "C" int64_t gs_batch_launch_count(const gs_batch* b) { return b ? b->launches : 0; }
+
+extern "C" int gs_batch_use_graph(gs_batch* b, int on) {
+  if (!b) return gs_set_error(GS_EINVAL, "null batch");
+  b->use_graph = on;
+  return GS_OK;
+}
+
+static int batch_slot(gs_batch* b, int sim, gs_sim** g, int* slot) {
+  if (!b || sim < 0 || sim >= (int)b->where.size()) return gs_set_error(GS_EINVAL, "sim index %d", sim);
+  *g = b->groups[b->where[sim].first];
+  *slot = b->where[sim].second;
+  return GS_OK;
+}
+
+extern "C" int gs_batch_set_field(gs_batch* b, int sim, const char* name, const void* host, size_t count, int dtype) {
+  gs_sim* g;
+  int slot;
+  GS_TRY(batch_slot(b, sim, &g, &slot));
+  if (!name || !host || std::string(name) != "eta") return gs_set_error(GS_EINVAL, "batches take the field eta");
+  const size_t n = (size_t)g->N * g->p.nvariants;
+  if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
+  GS_CU(cudaStreamSynchronize(b->stream), "sync");
+  char* dst = static_cast<char*>(g->eta[g->cur]) + (size_t)slot * n * elt(g);
+  return upload(g, dst, host, count, dtype);
+}
+
+extern "C" int gs_batch_get_field(gs_batch* b, int sim, const char* name, void* host, size_t count, int dtype) {
+  gs_sim* g;
+  int slot;
+  GS_TRY(batch_slot(b, sim, &g, &slot));
+  if (!name || !host || std::string(name) != "eta") return gs_set_error(GS_EINVAL, "batches hold the field eta");
+  const size_t n = (size_t)g->N * g->p.nvariants;
+  if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
+  GS_CU(cudaStreamSynchronize(b->stream), "sync");
+  const char* src = static_cast<const char*>(g->eta[g->cur]) + (size_t)slot * n * elt(g);
+  return download(g, src, host, count, dtype);
+}
+
+extern "C" int gs_batch_step(gs_batch* b, int nsteps, void* stream) {
+  if (!b || nsteps < 0) return gs_set_error(GS_EINVAL, "gs_batch_step: bad arguments");
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  for (gs_sim* g : b->groups) g->launches = 0;
+  int done = 0;
+  if (b->use_graph && nsteps >= 2) {
+    // the first steps run directly (kernel attributes are set outside any
+    // capture); then a graph of two steps (the field pair swaps back) replays
+    if (!b->exec || b->exec_stream != st) {
+      if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+      }
+      GS_TRY(batch_step_once(b, st));
+      GS_TRY(batch_step_once(b, st));
+      done = 2;
+      std::vector<int> cur;
+      std::vector<int64_t> steps;
+      std::vector<std::vector<int64_t>> bsteps;
+      for (gs_sim* g : b->groups) {
+        cur.push_back(g->cur);
+        steps.push_back(g->step);
+        bsteps.push_back(g->bstep);
+      }
+      cudaGraph_t graph;
+      GS_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+      int rc = batch_step_once(b, st);
+      if (rc == GS_OK) rc = batch_step_once(b, st);
+      cudaError_t e = cudaStreamEndCapture(st, &graph);
+      if (rc != GS_OK) return rc;
+      GS_CU(e, "end capture");
+      GS_CU(cudaGraphInstantiate(&b->exec, graph, 0), "instantiate graph");
+      cudaGraphDestroy(graph);
+      b->exec_stream = st;
+      for (size_t k = 0; k < b->groups.size(); ++k) {  // the capture did not run
+        b->groups[k]->cur = cur[k];
+        b->groups[k]->step = steps[k];
+        b->groups[k]->bstep = bsteps[k];
+      }
+      b->exec_cur = cur;
+    }
+    // the graph's buffers are fixed: after an odd number of direct steps the
+    // field pairs are swapped, and one more direct step swaps them back
+    if (nsteps - done >= 1 && !b->groups.empty() && b->groups[0]->cur != b->exec_cur[0]) {
+      GS_TRY(batch_step_once(b, st));
+      ++done;
+    }
+    while (nsteps - done >= 2) {
+      GS_CU(cudaGraphLaunch(b->exec, st), "graph launch");
+      for (gs_sim* g : b->groups) {
+        g->step += 2;
+        for (auto& k : g->bstep) k += 2;
+      }
+      done += 2;
+    }
+  }
+  for (; done < nsteps; ++done) GS_TRY(batch_step_once(b, st));
+  b->launches = 0;
+  for (gs_sim* g : b->groups) b->launches += g->launches;
+  return GS_OK;
+}
+
+extern "C" int gs_batch_stats(gs_batch* b, int sim, gs_stats* out, void* stream) {
+  gs_sim* g;
+  int slot;
+  GS_TRY(batch_slot(b, sim, &g, &slot));
+  if (!out) return gs_set_error(GS_EINVAL, "null stats");
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  // a single-simulation view of slot `slot`
+  gs_sim view = *g;
+  view.p = g->bp[slot];
+  view.nb = 1;
+  view.step = g->bstep[slot];
+  const size_t n = (size_t)g->N * g->p.nvariants * elt(g);
+  view.eta[view.cur] = static_cast<char*>(g->eta[g->cur]) + slot * n;
+  int rc = g->p.dtype == GS_DTYPE_F64 ? mart_stats<double>(&view, out, st) : mart_stats<float>(&view, out, st);
+  return rc;  // the view shares g's buffers: nothing to free
 }

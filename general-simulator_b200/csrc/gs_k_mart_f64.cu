@@ -1,5 +1,9 @@
 // gs_k_mart_f64.cu -- double instances of the fused martensite update.
 #include "gs_k_mart_impl.cuh"
 namespace gs {
-template cudaError_t launch_mart_update<double>(MartArgs<double>&, int, bool, cudaStream_t, int*);
+template cudaError_t launch_mart_update<double>(MartArgs<double>&, int, bool, cudaStream_t, int*, int);
+template <> cudaError_t launch_bump_step<double>(MartConst<double>* mcs, int n, cudaStream_t s) {
+  k_bump_step<double><<<(n + 127) / 128, 128, 0, s>>>(mcs, n);
+  return cudaGetLastError();
+}
 }  // namespace gs

@@ -6,7 +6,8 @@
 
 namespace gs {
 
-template <typename T, int H, int VM, bool ST> cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks) {
+template <typename T, int H, int VM, bool ST, bool BA> cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks,
+                                                                       int nsim) {
   using L = Line<T, H>;
   const int per = L::P * a.mc.V;
   long long lr = 256 / per;
@@ -14,26 +15,29 @@ template <typename T, int H, int VM, bool ST> cudaError_t mu_n(MartArgs<T>& a, c
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;
   const size_t smem = (size_t)lr * a.mc.V * L::PAD * sizeof(cplx<T>);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_mart_update<T, H, VM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_smem<k_mart_update<T, H, VM, ST, BA>>();
   const long long grid = (a.nrows + lr - 1) / lr;
   if (nblocks) *nblocks = (int)grid;
-  k_mart_update<T, H, VM, ST><<<(unsigned)grid, (unsigned)(per * lr), smem, s>>>(a);
+  k_mart_update<T, H, VM, ST, BA><<<dim3((unsigned)grid, (unsigned)nsim), (unsigned)(per * lr), smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaStream_t s, int* nb) {
+template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaStream_t s, int* nb, int nsim) {
+  if (nsim > 0) {  // batched simulations (device-resident constants)
+    if (a.mc.V <= 4) return mu_n<T, H, 4, false, true>(a, s, nb, nsim);
+    return mu_n<T, H, 8, false, true>(a, s, nb, nsim);
+  }
   if (a.mc.V <= 4)
-    return stats ? mu_n<T, H, 4, true>(a, s, nb) : mu_n<T, H, 4, false>(a, s, nb);
-  return stats ? mu_n<T, H, 8, true>(a, s, nb) : mu_n<T, H, 8, false>(a, s, nb);
+    return stats ? mu_n<T, H, 4, true, false>(a, s, nb, 1) : mu_n<T, H, 4, false, false>(a, s, nb, 1);
+  return stats ? mu_n<T, H, 8, true, false>(a, s, nb, 1) : mu_n<T, H, 8, false, false>(a, s, nb, 1);
 }
 
 template <typename T>
-cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks) {
+cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks, int nsim) {
   switch (H) {
 #define GS_C(N_) \
   case N_:       \
-    return mu_h<T, N_>(a, stats, s, nblocks);
+    return mu_h<T, N_>(a, stats, s, nblocks, nsim);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:

@@ -12,7 +12,7 @@ template <typename T, int H> static cudaError_t zinv_n(ZinvArgs<T>& a, cudaStrea
   if (lpc > a.nrows) lpc = a.nrows;
   a.lpc = (int)lpc;
   const size_t smem = (size_t)lpc * L::PAD * sizeof(cplx<T>);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv<T, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_smem<k_zinv<T, H>>();
   const long long grid = (a.nrows + lpc - 1) / lpc;
   k_zinv<T, H><<<(unsigned)grid, (unsigned)(L::P * lpc), smem, s>>>(a);
   return cudaGetLastError();

@@ -24,17 +24,15 @@ template <typename T, int N0, int FM, int GM, class Op> static cudaError_t xc_n(
   a.tz = tz;
   a.groups = groups;
   const size_t smem = smem_of(tz);
-  dim3 grid(a.h / tz, a.n1);
+  dim3 grid(a.h / tz, a.n1, a.nsim > 1 ? a.nsim : 1);
   if constexpr (sizeof(T) == 4 && N0 >= 64) {
     if (tz == 8) {
-      if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 8, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      allow_max_smem<k_xpass<T, N0, FM, GM, 8, Op>>();
       k_xpass<T, N0, FM, GM, 8, Op><<<grid, tz * L::P * groups, smem, s>>>(a);
       return cudaGetLastError();
     }
   }
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_xpass<T, N0, FM, GM, 0, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_smem<k_xpass<T, N0, FM, GM, 0, Op>>();
   k_xpass<T, N0, FM, GM, 0, Op><<<grid, tz * L::P * groups, smem, s>>>(a);
   return cudaGetLastError();
 }

@@ -6,9 +6,6 @@
 
 namespace gs {
 
-template <typename K> static void allow_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
 
 template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStream_t s) {
   using L = Line<T, H>;
@@ -17,7 +14,7 @@ template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStrea
   if (lpc > a.nrows) lpc = a.nrows;
   a.lpc = (int)lpc;
   const size_t smem = (size_t)lpc * L::PAD * sizeof(cplx<T>);
-  allow_smem(k_zfwd<T, H>, smem);
+  allow_max_smem<k_zfwd<T, H>>();
   const long long grid = (a.nrows + lpc - 1) / lpc;
   k_zfwd<T, H><<<(unsigned)grid, (unsigned)(L::P * lpc), smem, s>>>(a);
   return cudaGetLastError();
@@ -38,7 +35,7 @@ template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_
 template <typename T, int N1, int DIR> static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s) {
   using L = Line<T, N1>;
   const size_t smem = (size_t)a.tz * L::PAD * sizeof(cplx<T>);
-  allow_smem(k_ypass<T, N1, DIR>, smem);
+  allow_max_smem<k_ypass<T, N1, DIR>>();
   dim3 grid(a.h / a.tz, a.n0, F);
   k_ypass<T, N1, DIR><<<grid, a.tz * L::P, smem, s>>>(a);
   return cudaGetLastError();

@@ -29,7 +29,22 @@ template <typename T> cudaError_t launch_precip_local(PrecipLocalArgs<T>& a, cud
 template <typename T> cudaError_t launch_defect(const T* eta, T* defect, long long N, int V, cudaStream_t s);
 template <typename T> cudaError_t launch_precip_stats(PrecipStatsArgs<T>& a, cudaStream_t s, int* nblocks);
 // returns the number of blocks through nblocks (statistics partial rows)
-template <typename T> cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks);
+// nsim > 0: nsim batched simulations with constants in a.mcs
+template <typename T>
+cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s, int* nblocks, int nsim = 0);
+template <typename T> struct MartConst;
+template <typename T> cudaError_t launch_bump_step(MartConst<T>* mcs, int n, cudaStream_t s);
+
+// opt a kernel in to the largest dynamic shared memory once (the launch
+// still asks only for what it needs); no attribute calls during capture
+// (one flag per kernel: the template is instantiated per function)
+template <auto Kernel> inline void allow_max_smem() {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    done = true;
+  }
+}
 cudaError_t launch_reduce(const double* partials, int nb, int n, double* out, cudaStream_t s);
 
 #define GS_SIZE_CASES(M) \

@@ -50,7 +50,15 @@ template <typename T> struct MartArgs {
   MartConst<T> mc;
   double* partials;  // [gridDim.x][ACC_N], statistics sweep only
   FastDiv fd_n1, fd_upr, fd_v;  // y extent, update runs per row, variants
+  MartConst<T>* mcs;  // batched: constants of sim blockIdx.y in device memory
 };
+
+// advance the step counter of every batched simulation (keeps a captured
+// graph of one step replayable: the noise counter lives in device memory)
+template <typename T> __global__ void k_bump_step(MartConst<T>* mcs, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) mcs[i].step += 1;
+}
 
 struct Neu {  // Neumaier compensated sum (Neumaier 1974)
   double s = 0, c = 0;
@@ -118,14 +126,20 @@ template <int CW> __device__ __forceinline__ void stv(double* p, const double (&
 // cells (a quad, or a pair when n2 = 2) for all variants at once, so the
 // Landau coupling, the defect mask and one Philox block per variant serve
 // the whole run.
-template <typename T, int H, int VM, bool STATS>
+template <typename T, int H, int VM, bool STATS, bool BATCH>
 __global__ void k_mart_update(MartArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
   constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* smb = reinterpret_cast<V*>(smraw);
-  const MartConst<T>& mc = a.mc;
+  const MartConst<T>& mc = BATCH ? a.mcs[blockIdx.y] : a.mc;
+  if (BATCH) {  // fields of sim blockIdx.y
+    const long long off = (long long)blockIdx.y * mc.V * a.nrows * a.n2;
+    a.spec += off / 2;
+    a.eta_in += off;
+    a.eta_out += off;
+  }
   const int Vn = mc.V;
   {
     const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;

@@ -122,7 +122,7 @@ __device__ __forceinline__ int fold_idx(int i, int n, int refcompat) {
 // inverse, which sees both signs through the conjugate partner).
 template <typename T, int FM, int GM>
 __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int (&nn)[3], int ix, int iy, int iz,
-                                            const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+                                            const cplx<T> (&in)[FM], cplx<T> (&out)[GM], T mult = (T)1) {
   const int id[3] = {ix, iy, iz};
   int m[3];
   bool nyq = false;
@@ -135,7 +135,7 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
   }
 #pragma unroll
   for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
-  const T w = nyq ? (T)0.5 * ec.scale : ec.scale;
+  const T w = (nyq ? (T)0.5 * ec.scale : ec.scale) * mult;
   const int trips = nyq ? 2 : 1;
 #pragma unroll 1
   for (int trip = 0; trip < trips; ++trip) {
@@ -152,6 +152,9 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
 template <typename T> struct ZfwdArgs {
   const T* src[2 * GS_MAXF];   // row source of each field (n0*n1 rows of n2)
   int square[2 * GS_MAXF];     // 1: transform src^2 (eta^2), 0: src
+  const T* src0;               // when set: field f at src0 + f * fstride (batches)
+  long long fstride;
+  int square0;
   cplx<T>* dst;            // [F][n0][n1][h]
   long long rows_per_field;
   long long nrows;         // F * rows_per_field
@@ -175,8 +178,8 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
   if (act) {
     const int f = (int)(row / a.rows_per_field);
     const long long rin = row - (long long)f * a.rows_per_field;
-    const V* src = reinterpret_cast<const V*>(a.src[f]) + rin * H;
-    const int sq = a.square[f];
+    const V* src = reinterpret_cast<const V*>(a.src0 ? a.src0 + f * a.fstride : a.src[f]) + rin * H;
+    const int sq = a.src0 ? a.square0 : a.square[f];
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) {
       V x = src[L::in_pos(t, r)];
@@ -330,6 +333,8 @@ template <typename T> struct XArgs {
   const cplx<T>* tw;  // w_n0^m
   ElasticConst<T> ec;
   PrecipUpd<T> pu;
+  const T* simscale;  // batched: contraction multiplier of sim blockIdx.z (null: 1)
+  int nsim;           // batched simulations (grid z), 0 or 1 for one
 };
 
 // per-point operations of the x pass
@@ -337,7 +342,7 @@ struct ContractOp {
   template <typename T, int FM, int GM>
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
                                                const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
-    contract_at<T, FM, GM>(a.ec, nn, ix, iy, iz, in, out);
+    contract_at<T, FM, GM>(a.ec, nn, ix, iy, iz, in, out, a.simscale ? a.simscale[blockIdx.z] : (T)1);
   }
 };
 struct PrecipOp {
@@ -381,13 +386,16 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const int rstride = n1 * h;
   const int region = L::PAD * TZ;
   V* rg = smb + grp * region + c;
+  // batched simulations: one sim per blockIdx.z, fields stored sim after sim
+  const V* in_base = a.in + (long long)blockIdx.z * a.F * fstride;
+  V* out_base = a.out + (long long)blockIdx.z * a.G * fstride;
   auto sm = [rg, TZ](int pos) -> V& { return rg[pos * TZ]; };
   V* part = smb + a.groups * region;  // GM x N0 results of the packed column
   V v[L::R1];
   // forward FFT, group grp takes field grp
   const bool fw = grp < a.F;
   {
-    const V* src = a.in + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
+    const V* src = in_base + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
   }
@@ -472,7 +480,7 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   __syncthreads();
   L::template run<1>(v, t, sm, a.tw);
   if (iv) {
-    V* dst = a.out + grp * fstride + (long long)ky * h + kz0 + c;
+    V* dst = out_base + grp * fstride + (long long)ky * h + kz0 + c;
 #pragma unroll
     for (int i = 0; i < L::R1; ++i) dst[(long long)L::out_pos(t, i) * rstride] = v[i];
   }

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/gs_capi.h"
 
 struct gs_plain_state;  // cuFFT comparator buffers (gs_plain.cu)
@@ -37,6 +39,13 @@ struct gs_sim {
   int64_t launches = 0;
   int use_graph = 0;
   gs_plain_state* plain = nullptr;
+  // batched group: nb simulations of one shape with their own coefficients,
+  // fields stored sim after sim; per-sim constants live on the device
+  int nb = 1;
+  std::vector<gs_params> bp;
+  std::vector<int64_t> bstep;
+  void* d_mcs = nullptr;
+  void* d_simscale = nullptr;
   // per-pass event marks of gs_sim_profile_step
   static constexpr int kMaxMarks = 32;
   cudaEvent_t marks[kMaxMarks] = {};

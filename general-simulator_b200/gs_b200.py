@@ -135,6 +135,16 @@ def lib() -> C.CDLL:
         "gs_sim_launch_count": (C.c_int64, [vp]),
         "gs_sim_profile_step": (C.c_int, [vp, vp, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
         "gs_sim_use_graph": (C.c_int, [vp, C.c_int]),
+        "gs_set_device": (C.c_int, [C.c_int]),
+        "gs_batch_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
+        "gs_batch_destroy": (C.c_int, [vp]),
+        "gs_batch_set_field": (C.c_int, [vp, C.c_int, C.c_char_p, vp, C.c_size_t, C.c_int]),
+        "gs_batch_get_field": (C.c_int, [vp, C.c_int, C.c_char_p, vp, C.c_size_t, C.c_int]),
+        "gs_batch_step": (C.c_int, [vp, C.c_int, vp]),
+        "gs_batch_stats": (C.c_int, [vp, C.c_int, S, vp]),
+        "gs_batch_use_graph": (C.c_int, [vp, C.c_int]),
+        "gs_batch_groups": (C.c_int, [vp]),
+        "gs_batch_launch_count": (C.c_int64, [vp]),
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
     }
@@ -249,6 +259,61 @@ class Sim:
         check(lib().gs_sim_use_graph(self.h, 1 if on else 0), "use_graph")
 
 
+class Batch:
+    """Many independent martensite simulations advanced together (gs_batch*)."""
+
+    def __init__(self, params: list):
+        arr = (GsParams * len(params))()
+        for i, p in enumerate(params):
+            C.memmove(C.byref(arr[i]), C.byref(p), C.sizeof(GsParams))
+        self.params = [p.copy() for p in params]
+        h = C.c_void_p()
+        check(lib().gs_batch_create(arr, len(params), C.byref(h)), "gs_batch_create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().gs_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_eta(self, sim: int, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr)
+        code = GS_DTYPE_F64 if a.dtype == np.float64 else GS_DTYPE_F32
+        a = np.ascontiguousarray(a, dtype=_np_dtype(code))
+        check(lib().gs_batch_set_field(self.h, sim, b"eta", a.ctypes.data, a.size, code), "batch set_field")
+
+    def eta(self, sim: int, dtype=np.float64) -> np.ndarray:
+        p = self.params[sim]
+        n = p.nvariants * p.ncells
+        out = np.empty(n, dtype=dtype)
+        code = GS_DTYPE_F64 if dtype == np.float64 else GS_DTYPE_F32
+        check(lib().gs_batch_get_field(self.h, sim, b"eta", out.ctypes.data, n, code), "batch get_field")
+        return out.reshape(p.nvariants, p.nx, p.ny, p.nz)
+
+    def step(self, n: int = 1, stream: int = 0) -> None:
+        check(lib().gs_batch_step(self.h, n, C.c_void_p(stream)), "gs_batch_step")
+
+    def stats(self, sim: int) -> dict:
+        s = GsStats()
+        check(lib().gs_batch_stats(self.h, sim, C.byref(s), None), "gs_batch_stats")
+        return s.as_dict(self.params[sim].nvariants)
+
+    def use_graph(self, on: bool) -> None:
+        check(lib().gs_batch_use_graph(self.h, 1 if on else 0), "use_graph")
+
+    def groups(self) -> int:
+        return int(lib().gs_batch_groups(self.h))
+
+    def launch_count(self) -> int:
+        return int(lib().gs_batch_launch_count(self.h))
+
+
 # ---------------------------------------------------------------------------
 # workload builders: the configurations the step is measured and tested on
 # ---------------------------------------------------------------------------
@@ -326,6 +391,38 @@ def precip3d_params(n: int = 256, dtype: int = GS_DTYPE_F32) -> GsParams:
     p.nvariants = 4
     p.nx = p.ny = p.nz = n
     return p
+
+
+def ensemble_params(dtype: int = GS_DTYPE_F32, steps_noise: float = 1e-3, seed0: int = 100,
+                    counts=(32, 16, 12, 4)) -> list:
+    """64 uneven martensite simulations: 32 x 128^2 and 16 x 256^2 (2D, 2
+    variants), 12 x 64^3 and 4 x 128^3 (3D, 3 variants); per-simulation
+    seeds seed0.., coefficients drawn uniformly (A2 in [0.1,0.4], A4 in
+    [2,4], kappa in [0.5,2], eigenstrain magnitude in [0.01,0.03]) from a
+    seeded host generator; noise 1e-3, dt 0.005."""
+    rng = np.random.default_rng(2024)
+    shapes = [((128, 128, 1), 2)] * counts[0] + [((256, 256, 1), 2)] * counts[1] + \
+             [((64, 64, 64), 3)] * counts[2] + [((128, 128, 128), 3)] * counts[3]
+    out = []
+    for i, (shape, V) in enumerate(shapes):
+        if V == 2:
+            p = mart2d_params(shape[0], dtype=dtype)
+            base = np.zeros((2, 3, 3))
+            base[0, 0, 0], base[0, 1, 1], base[1, 0, 0], base[1, 1, 1] = 1, -1, -1, 1
+        else:
+            p = mart3d_params(shape[0], dtype=dtype, noise=steps_noise)
+            base = tetragonal_eigenstrains(3, 1.0, -0.5)
+        p.nx, p.ny, p.nz = shape
+        p.dt = 0.005
+        p.noise_amp = steps_noise
+        p.landau[0] = rng.uniform(0.1, 0.4)
+        p.landau[1] = rng.uniform(2.0, 4.0)
+        p.kappa = rng.uniform(0.5, 2.0)
+        p.set_eigenstrain(base * rng.uniform(0.01, 0.03))
+        p.seed = seed0 + i
+        p.sim_id = i
+        out.append(p)
+    return out
 
 
 def initial_eta(p: GsParams, seed: int, amp: float = 0.01) -> np.ndarray:

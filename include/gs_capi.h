@@ -180,6 +180,24 @@ int64_t gs_sim_launch_count(const gs_sim* s);
  * the passes directly (0, default). */
 int gs_sim_use_graph(gs_sim* s, int on);
 
+/* ---- batched ensembles ------------------------------------------------- */
+/* Many independent martensite simulations advanced together.  Simulations
+ * of one grid, variant count, modulus and eigenstrain direction form a group
+ * and share every launch (one per pass per group); each keeps its own
+ * Landau coefficients, kappa, mobility, eigenstrain magnitude, applied
+ * stress, noise amplitude and seed.  With gs_batch_use_graph(b, 1) the step
+ * is captured once as a CUDA graph of two steps and replayed. */
+typedef struct gs_batch gs_batch;
+int gs_batch_create(const gs_params* params, int nsims, gs_batch** out);
+int gs_batch_destroy(gs_batch* b);
+int gs_batch_set_field(gs_batch* b, int sim, const char* name, const void* host, size_t count, int dtype);
+int gs_batch_get_field(gs_batch* b, int sim, const char* name, void* host, size_t count, int dtype);
+int gs_batch_step(gs_batch* b, int nsteps, void* stream);
+int gs_batch_stats(gs_batch* b, int sim, gs_stats* out, void* stream);
+int gs_batch_use_graph(gs_batch* b, int on);
+int gs_batch_groups(const gs_batch* b);
+int64_t gs_batch_launch_count(const gs_batch* b);
+
 /* ---- comparator: the same step with cuFFT C2C and unfused sweeps ------ */
 /* The plain GPU step in the reference's structure (cufftPlanMany C2C batch
  * V, B streamed from a [V][V][N] array, one sweep per term); used only as a
