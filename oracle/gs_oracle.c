@@ -765,3 +765,117 @@ int or_stress(const gs_params* p, const double* eta, double* stress, double* def
   free(S);
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* adjoint of the baseline martensite step                             */
+/* ------------------------------------------------------------------ */
+/* Phi(eta) = eta + dt RHS(eta) (+ noise), RHS_p = L kappa lap eta_p
+ *   - L f'_p(eta) + el eta_p R_p + lin_p eta_p, el = -2 L w_el,
+ *   lin_p = 2 L sigma_a:eps_p, R = B conv (eta^2).
+ * (dPhi/deta)^T lam = lam + dt [L kappa lap lam - L H lam
+ *   + el (R lam + 2 eta Q) + lin lam],  Q = B conv (eta lam),
+ * H the Landau Hessian.  Parameter derivatives of Phi_p: kappa: dt L lap
+ * eta_p; A2: -dt L eta_p; A4: dt L eta_p^3; A6: -dt L S^2 eta_p; Ac: -dt L
+ * 2 eta_p (S - eta_p^2); eigenstrain scale s (eps -> s eps at s = 1):
+ * dt (2 el eta_p R_p + lin_p eta_p).
+ * Loss J = sum (eta_T - target)^2 + lam_el (E_el(T) - E_target)^2, or,
+ * with seed != NULL, J = <seed, eta_T> + seed_e E_el(T). */
+int or_mart_adjoint(const gs_params* p, const double* eta0, int nsteps, const double* target, double lam_el,
+                    double e_target, const double* seed, double seed_e, double* grads, double* grad_eta0,
+                    double* loss_out) {
+  const int n0 = p->nx, n1 = p->ny, n2 = p->nz, V = p->nvariants;
+  const long long N = (long long)n0 * n1 * n2;
+  const double dV = p->dx * p->dy * p->dz;
+  double* st = (double*)malloc(sizeof(double) * N * V * (nsteps + 1));
+  memcpy(st, eta0, sizeof(double) * N * V);
+  for (int n = 0; n < nsteps; ++n) {
+    memcpy(st + (long long)(n + 1) * N * V, st + (long long)n * N * V, sizeof(double) * N * V);
+    or_mart_run(p, st + (long long)(n + 1) * N * V, NULL, NULL, 1, n);
+  }
+  const double* eT = st + (long long)nsteps * N * V;
+  double* R = (double*)malloc(sizeof(double) * N * V);
+  double* Q = (double*)malloc(sizeof(double) * N * V);
+  double* u = (double*)malloc(sizeof(double) * N * V);
+  double* lam = (double*)malloc(sizeof(double) * N * V);
+  double* lnew = (double*)malloc(sizeof(double) * N * V);
+  or_mart_potential(p, eT, R);
+  double eel = 0, lf = 0;
+  for (long long i = 0; i < N * V; ++i) eel += 0.5 * p->weight_elastic * eT[i] * eT[i] * R[i];
+  eel *= dV;
+  double ce;
+  if (seed) {
+    for (long long i = 0; i < N * V; ++i) lam[i] = seed[i];
+    ce = seed_e;
+  } else {
+    for (long long i = 0; i < N * V; ++i) {
+      const double d = eT[i] - target[i];
+      lf += d * d;
+      lam[i] = 2.0 * d;
+    }
+    ce = 2.0 * lam_el * (eel - e_target);
+  }
+  /* dE_el/deta_p = w_el dV 2 eta_p R_p */
+  for (long long i = 0; i < N * V; ++i) lam[i] += ce * p->weight_elastic * dV * 2.0 * eT[i] * R[i];
+  for (int g = 0; g < 6; ++g) grads[g] = 0;
+  grads[5] += ce * 2.0 * eel; /* dE_el/ds = 2 E_el */
+  if (loss_out) {
+    loss_out[0] = seed ? 0.0 : lf + lam_el * (eel - e_target) * (eel - e_target);
+    loss_out[1] = lf;
+    loss_out[2] = eel;
+  }
+  const double L = p->mobility, dt = p->dt, kap = p->kappa;
+  const double A2 = p->landau[0], A4 = p->landau[1], A6 = p->landau[2], Ac = p->landau[3];
+  const double el = -2.0 * L * p->weight_elastic;
+  double lin[GS_MAX_V];
+  for (int v = 0; v < V; ++v) lin[v] = 2.0 * L * contract33(p->applied_stress, p->eigenstrain[v]);
+  double cg[3] = {1.0 / (p->dx * p->dx), 1.0 / (p->dy * p->dy), 1.0 / (p->dz * p->dz)};
+  for (int n = nsteps - 1; n >= 0; --n) {
+    const double* e = st + (long long)n * N * V;
+    or_mart_potential(p, e, R);
+    for (long long i = 0; i < N * V; ++i) u[i] = e[i] * lam[i];
+    elastic_potential(p, 0, u, V, Q, V);
+    double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+#pragma omp parallel for schedule(static) reduction(+ : g0, g1, g2, g3, g4, g5)
+    for (long long idx = 0; idx < N; ++idx) {
+      int x = (int)(idx / ((long long)n1 * n2)), y = (int)((idx / n2) % n1), z = (int)(idx % n2);
+      double S = 0, el_dot = 0;
+      for (int q = 0; q < V; ++q) {
+        S += e[q * N + idx] * e[q * N + idx];
+        el_dot += e[q * N + idx] * lam[q * N + idx];
+      }
+      for (int r = 0; r < V; ++r) {
+        const double er = e[r * N + idx], lr = lam[r * N + idx];
+        const double lapl = lap7(lam + (long long)r * N, n0, n1, n2, x, y, z, cg);
+        double off = 0;
+        for (int q = 0; q < V; ++q)
+          if (q != r) off += e[q * N + idx] * lam[q * N + idx];
+        const double Hl = (A2 - 3 * A4 * er * er + A6 * S * S + 2 * Ac * (S - er * er)) * lr +
+                          4 * er * (A6 * S * el_dot + Ac * off);
+        const double Rr = R[r * N + idx], Qr = Q[r * N + idx];
+        lnew[r * N + idx] = lr + dt * (L * kap * lapl - L * Hl + el * (Rr * lr + 2 * er * Qr) + lin[r] * lr);
+        const double lape = lap7(e + (long long)r * N, n0, n1, n2, x, y, z, cg);
+        g0 += dt * L * lape * lr;
+        g1 += -dt * L * er * lr;
+        g2 += dt * L * er * er * er * lr;
+        g3 += -dt * L * S * S * er * lr;
+        g4 += -dt * L * 2 * er * (S - er * er) * lr;
+        g5 += dt * (2 * el * er * Rr + lin[r] * er) * lr;
+      }
+    }
+    grads[0] += g0;
+    grads[1] += g1;
+    grads[2] += g2;
+    grads[3] += g3;
+    grads[4] += g4;
+    grads[5] += g5;
+    memcpy(lam, lnew, sizeof(double) * N * V);
+  }
+  if (grad_eta0) memcpy(grad_eta0, lam, sizeof(double) * N * V);
+  free(st);
+  free(R);
+  free(Q);
+  free(u);
+  free(lam);
+  free(lnew);
+  return 0;
+}

@@ -46,6 +46,15 @@ int or_mart_stats(const gs_params* p, const double* eta, const double* defect,
 /* Elastic potential R_p = Re IFFT((1/N) sum_q B_pq FFT(eta_q^2)) of a state. */
 int or_mart_potential(const gs_params* p, const double* eta, double* R);
 
+/* Adjoint of the baseline martensite run from eta0 over nsteps.  Loss
+ * J = sum (eta_T - target)^2 + lam_el (E_el(T) - e_target)^2, or, when seed
+ * is given, J = <seed, eta_T> + seed_e E_el(T).  grads[6]: dJ/d kappa, A2,
+ * A4, A6, Ac, eigenstrain scale s (eps -> s eps at s = 1); grad_eta0 = dJ/d
+ * eta0 ([V][N], may be NULL); loss_out[3] = (J, field term, E_el(T)). */
+int or_mart_adjoint(const gs_params* p, const double* eta0, int nsteps, const double* target, double lam_el,
+                    double e_target, const double* seed, double seed_e, double* grads, double* grad_eta0,
+                    double* loss_out);
+
 /* Precipitate: advance c (N) and eta ([V][N]) nsteps. */
 int or_precip_run(const gs_params* p, double* c, double* eta, int nsteps, int64_t step0);
 int or_precip_stats(const gs_params* p, const double* c, const double* eta, gs_stats* st);

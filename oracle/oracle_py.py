@@ -39,6 +39,7 @@ def lib() -> C.CDLL:
         L.or_precip_run.argtypes = [P, dp, dp, C.c_int, C.c_int64]
         L.or_precip_stats.argtypes = [P, dp, dp, S]
         L.or_stress.argtypes = [P, dp, dp, dp]
+        L.or_mart_adjoint.argtypes = [P, dp, C.c_int, dp, C.c_double, C.c_double, dp, C.c_double, dp, dp, dp]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         _lib = L
@@ -135,3 +136,21 @@ def set_threads(n: int) -> None:
 
 def get_threads() -> int:
     return lib().or_get_threads()
+
+
+def mart_adjoint(p, eta0, nsteps, target=None, lam_el=0.0, e_target=0.0, seed=None, seed_e=0.0):
+    """(loss, field term, E_el(T)), grads[6], dJ/deta0 of the baseline martensite run."""
+    e = _f64(eta0)
+    g = np.zeros(6)
+    ge = np.zeros_like(e)
+    lo = np.zeros(3)
+    t = None if target is None else _f64(target)
+    sd = None if seed is None else _f64(seed)
+    lib().or_mart_adjoint(C.byref(p), _dp(e), nsteps, _dp(t), lam_el, e_target, _dp(sd), seed_e, _dp(g), _dp(ge), _dp(lo))
+    return lo, g, ge
+
+
+def mart_loss(p, eta0, nsteps, target, lam_el, e_target):
+    eT = mart_run(p, eta0, nsteps)
+    st = mart_stats(p, eT)
+    return ((eT - target) ** 2).sum() + lam_el * (st["e_el"] - e_target) ** 2

@@ -124,3 +124,41 @@ def test_stress_uniform_eta_is_zero_baseline(gb, orc):
     s, d = orc.stress(p, eta)
     assert np.abs(s).max() < 1e-15  # B(0) = 0: a uniform field is stress free
     assert d.max() == 0.0
+
+
+def test_mart_adjoint_matches_central_differences(gb, orc):
+    """The oracle's hand-written adjoint of the baseline martensite run against
+    central differences of the forward run: all six parameter gradients and a
+    random directional derivative in eta0."""
+    p = gb.mart3d_params(8, dtype=1, noise=0.0)
+    p.nx, p.ny, p.nz = 6, 8, 4
+    p.weight_elastic = 200.0
+    eta0 = gb.initial_eta(p, 4, 0.3)
+    tgt = gb.initial_eta(p, 5, 0.3)
+    lam_el, et, ns, h = 0.1, 0.0, 4, 1e-6
+    _, g, ge = orc.mart_adjoint(p, eta0, ns, tgt, lam_el, et)
+
+    def loss(q, e0=eta0):
+        return orc.mart_loss(q, e0, ns, tgt, lam_el, et)
+
+    def with_param(k, v):
+        q = p.copy()
+        if k == 0:
+            q.kappa = v
+        else:
+            q.landau[k - 1] = v
+        return q
+
+    vals = [p.kappa] + [p.landau[i] for i in range(4)]
+    for k in range(5):
+        fd = (loss(with_param(k, vals[k] + h)) - loss(with_param(k, vals[k] - h))) / (2 * h)
+        assert abs(g[k] - fd) <= 1e-5 * abs(fd) + 1e-9, (k, g[k], fd)
+    eps = p.get_eigenstrain()
+    q1, q2 = p.copy(), p.copy()
+    q1.set_eigenstrain(eps * (1 + h))
+    q2.set_eigenstrain(eps * (1 - h))
+    fd = (loss(q1) - loss(q2)) / (2 * h)
+    assert abs(g[5] - fd) <= 1e-5 * abs(fd) + 1e-9
+    d = np.random.default_rng(1).standard_normal(eta0.shape)
+    fd = (loss(p, eta0 + h * d) - loss(p, eta0 - h * d)) / (2 * h)
+    assert abs((ge * d).sum() - fd) <= 1e-6 * abs(fd)
