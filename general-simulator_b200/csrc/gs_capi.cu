@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "../../include/gs_capi.h"
@@ -1426,4 +1427,122 @@ extern "C" int gs_batch_stats(gs_batch* b, int sim, gs_stats* out, void* stream)
   view.eta[view.cur] = static_cast<char*>(g->eta[g->cur]) + slot * n;
   int rc = g->p.dtype == GS_DTYPE_F64 ? mart_stats<double>(&view, out, st) : mart_stats<float>(&view, out, st);
   return rc;  // the view shares g's buffers: nothing to free
+}
+
+// ---------------------------------------------------------------------------
+// a martensite step that allocates nothing
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory at the moment they want a step:
+// a host that hands every byte of the GPU to its own pool allocator up front,
+// a real-time loop that must not touch the allocator, or a plugin living in a
+// process whose device memory is owned by someone else.  gs_mart_step_noalloc
+// serves them: the caller passes the field buffers, and the one piece of
+// scratch the step needs (the packed spectra and the twiddle tables) lives in
+// this file-scope array, which every GPU that loads the library keeps until
+// the process exits.  The array's name means a host stand-in in host code;
+// its device address is taken once per device with cudaGetSymbolAddress.
+static constexpr size_t kNoallocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+static constexpr int kNoallocMaxDev = 64;
+static void* g_noalloc_ptr[kNoallocMaxDev] = {};
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  GS_CU(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kNoallocMaxDev) return gs_set_error(GS_ENODEV, "device %d beyond %d", dev, kNoallocMaxDev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    GS_CU(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress of the no-allocation scratch");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GS_OK;
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+static int check_device_buffer(const void* p, int dev, const char* what) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: %s is not a CUDA pointer", what);
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: %s is not device memory", what);
+  if (a.type == cudaMemoryTypeDevice && a.device != dev)
+    return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: %s lives on device %d, the current device is %d", what,
+                        a.device, dev);
+  return GS_OK;
+}
+
+template <typename T> static int noalloc_step(gs_sim& s, const void* in, void* out, cudaStream_t st) {
+  // twiddle tables as build_twiddles makes them, written into the scratch
+  const int lens[4] = {s.n2, s.h, s.n1, s.n0};
+  constexpr int kMaxTw = 512 + 256 + 256 + 256;
+  cplx<T> host[kMaxTw];
+  size_t total = 0;
+  for (int i = 0; i < 4; ++i) {
+    s.tw_off[i] = total;
+    total += (size_t)lens[i];
+  }
+  if (total > (size_t)kMaxTw) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: twiddle table too long");
+  for (int i = 0; i < 4; ++i)
+    for (int m = 0; m < lens[i]; ++m) {
+      const double a = 2.0 * M_PI * (double)m / (double)lens[i];
+      host[s.tw_off[i] + m] = mk2((T)std::cos(a), (T)-std::sin(a));
+    }
+  GS_CU(cudaMemcpyAsync(s.tw, host, total * sizeof(cplx<T>), cudaMemcpyHostToDevice, st), "upload twiddles");
+  s.eta[0] = const_cast<void*>(in);
+  s.eta[1] = out;
+  s.cur = 0;
+  int rc = mart_step<T>(&s, st);
+  // return only once the step has finished, so that calls made one after
+  // another from one host thread never share the scratch on the GPU
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (rc != GS_OK) return rc;
+  return gs_cuda_check(e, "gs_mart_step_noalloc");
+}
+
+extern "C" size_t gs_mart_step_noalloc_max_bytes(void) { return kNoallocScratchBytes; }
+
+extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void* eta_out, int64_t step,
+                                    void* stream) {
+  if (!p || !eta_in || !eta_out) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: null argument");
+  if (p->model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: model must be martensite");
+  if (p->nvariants < 1 || p->nvariants > GS_MAX_V)
+    return gs_set_error(GS_EINVAL, "nvariants %d outside 1..%d", p->nvariants, GS_MAX_V);
+  if (p->dtype != GS_DTYPE_F32 && p->dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", p->dtype);
+  if (step < 0) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: step %lld", (long long)step);
+  gs_sim s;  // a view: every pointer below is the caller's or the static scratch
+  s.p = *p;
+  GS_TRY(canonicalize(&s));
+  const size_t eb = elt(&s);
+  const size_t fields = (size_t)s.N * p->nvariants * eb;
+  const size_t tw_bytes = (size_t)(s.n2 + s.h + s.n1 + s.n0) * 2 * eb;
+  const size_t need = align256(fields) + align256(tw_bytes);
+  if (need > kNoallocScratchBytes)
+    return gs_set_error(GS_EINVAL,
+                        "gs_mart_step_noalloc: grid %dx%dx%d with %d variants needs %zu bytes of scratch; the "
+                        "static scratch holds %zu",
+                        p->nx, p->ny, p->nz, p->nvariants, need, kNoallocScratchBytes);
+  const char* a = static_cast<const char*>(eta_in);
+  const char* b = static_cast<const char*>(eta_out);
+  if (a < b + fields && b < a + fields)
+    return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: eta_in and eta_out overlap");
+  int dev = 0;
+  GS_CU(cudaGetDevice(&dev), "cudaGetDevice");
+  GS_TRY(check_device_buffer(eta_in, dev, "eta_in"));
+  GS_TRY(check_device_buffer(eta_out, dev, "eta_out"));
+  void* scratch = nullptr;
+  GS_TRY(noalloc_scratch(&scratch));
+  char* base = static_cast<char*>(scratch);
+  s.spec = base;
+  s.tw = base + align256(fields);
+  s.step = step;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dtype == GS_DTYPE_F64 ? noalloc_step<double>(s, eta_in, eta_out, st)
+                                  : noalloc_step<float>(s, eta_in, eta_out, st);
 }

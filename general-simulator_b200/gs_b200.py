@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgsb200.so")
 
 GS_OK = 0
+GS_EINVAL = -10
 GS_MODEL_MART, GS_MODEL_PRECIPITATE, GS_MODEL_STRESS = 1, 2, 3
 GS_MODE_BASELINE, GS_MODE_REFCOMPAT = 0, 1
 GS_DTYPE_F32, GS_DTYPE_F64 = 0, 1
@@ -147,6 +148,8 @@ def lib() -> C.CDLL:
         "gs_batch_launch_count": (C.c_int64, [vp]),
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
+        "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
+        "gs_mart_step_noalloc_max_bytes": (C.c_size_t, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -180,6 +180,28 @@ int64_t gs_sim_launch_count(const gs_sim* s);
  * the passes directly (0, default). */
 int gs_sim_use_graph(gs_sim* s, int on);
 
+/* ---- a martensite step that allocates nothing -------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they step: a host whose pool allocator owns all of the GPU's
+ * memory, a loop that must never enter the allocator, a plugin in a process
+ * whose device memory belongs to someone else.  One martensite step (the
+ * same passes as gs_sim_step) from eta_in to eta_out, both caller-owned
+ * device buffers of [V][nx][ny][nz] elements of p->dtype on the current
+ * device, not overlapping; `step` is the global step index that the noise
+ * counter uses (gs_sim_step's k-th step from a fresh simulation has step
+ * k).  Defect and dislocation-stress inputs are not taken.  The spectra and
+ * twiddle tables live in one static device array of
+ * gs_mart_step_noalloc_max_bytes() bytes (16 MiB) that every GPU loading the
+ * library keeps until exit; a grid needing more (V*N*element size plus
+ * about 4 KB) is rejected with GS_EINVAL.  No device memory is allocated or
+ * freed.  The first call on a device looks up the array's device address,
+ * so make it before any stream capture.  The call returns once the step has
+ * finished on `stream` (NULL = the legacy default stream).  All calls share
+ * the array and nothing in it has to start at zero; calls that overlap on
+ * the GPU (from several host threads) race on it. */
+int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void* eta_out, int64_t step, void* stream);
+size_t gs_mart_step_noalloc_max_bytes(void);
+
 /* ---- batched ensembles ------------------------------------------------- */
 /* Many independent martensite simulations advanced together.  Simulations
  * of one grid, variant count, modulus and eigenstrain direction form a group
