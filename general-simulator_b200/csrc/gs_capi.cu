@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/gs_capi.h"
+#include "gs_adjoint.cuh"
 #include "gs_launch.h"
 #include "gs_mart.cuh"
 #include "gs_precip.cuh"
@@ -417,13 +418,14 @@ template <typename T> static const cplx<T>* twp(const gs_sim* s, int which) {
 // (B contraction, F inputs -> G outputs, into out_spec) -> y inverse.
 template <typename T>
 static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, int F, int which, double scale,
-                           void* out_spec, int G, cudaStream_t st) {
+                           void* out_spec, int G, cudaStream_t st, const T* const* mul = nullptr) {
   const long long rows = (long long)s->n0 * s->n1;
   ZfwdArgs<T> za;
   memset(&za, 0, sizeof(za));
   for (int f = 0; f < F; ++f) {
     za.src[f] = src[f];
     za.square[f] = square[f];
+    za.mul[f] = mul ? mul[f] : nullptr;
   }
   za.dst = reinterpret_cast<cplx<T>*>(s->spec);
   za.rows_per_field = rows;
@@ -899,6 +901,7 @@ static int upload(gs_sim* s, void* dst, const void* host, size_t count, int dtyp
   const int want = s->p.dtype;
   if (dtype == want) {
     GS_CU(cudaMemcpy(dst, host, count * elt(s), cudaMemcpyHostToDevice), "upload");
+    GS_CU(cudaDeviceSynchronize(), "upload sync");
     return GS_OK;
   }
   if (want == GS_DTYPE_F64) {
@@ -908,6 +911,9 @@ static int upload(gs_sim* s, void* dst, const void* host, size_t count, int dtyp
     auto v = to_type<float>(host, count, dtype);
     GS_CU(cudaMemcpy(dst, v.data(), count * 4, cudaMemcpyHostToDevice), "upload");
   }
+  // a pageable cudaMemcpy may return before its last DMA lands; the passes
+  // run on non-blocking streams, so wait for it here
+  GS_CU(cudaDeviceSynchronize(), "upload sync");
   return GS_OK;
 }
 
@@ -1546,3 +1552,323 @@ extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void
   return p->dtype == GS_DTYPE_F64 ? noalloc_step<double>(s, eta_in, eta_out, st)
                                   : noalloc_step<float>(s, eta_in, eta_out, st);
 }
+
+// ---------------------------------------------------------------------------
+// adjoint of the martensite run (checkpoint every K steps, recompute)
+// ---------------------------------------------------------------------------
+// Forward: the trajectory eta_0 .. eta_T with eta_{jK} kept as checkpoints
+// and the last segment's states and elastic potentials kept whole.
+// Backward, segment by segment from the last: recompute the segment's states
+// eta_n and potentials R_n from its checkpoint (the same passes as the
+// forward step, with R written out by the update), then per step n the chain
+// Q = B * (eta_n lam) and the transposed update (gs_adjoint.cuh), whose
+// per-step FP64 sums give the parameter gradients.
+struct gs_adjoint {
+  gs_sim* s = nullptr;
+  int nsteps = 0, K = 0, nseg = 0;
+  std::vector<void*> ckpt, seg_eta, seg_R;
+  void* lam[2] = {nullptr, nullptr};
+  void* target = nullptr;
+  void* etaT = nullptr;
+  void* RT = nullptr;
+  double* gsum = nullptr;  // [nsteps][ADJ_N]
+  int seg_valid = -1;      // segment held in seg_eta / seg_R
+  bool forward_done = false, have_target = false;
+  double lam_el = 0, e_target = 0, e_el_T = 0;
+  size_t bytes = 0;
+};
+
+static void free_adjoint(gs_adjoint* a) {
+  if (!a) return;
+  auto f = [](void* p) {
+    if (p) cudaFree(p);
+  };
+  for (void* p : a->ckpt) f(p);
+  for (void* p : a->seg_eta) f(p);
+  for (void* p : a->seg_R) f(p);
+  f(a->lam[0]);
+  f(a->lam[1]);
+  f(a->target);
+  f(a->etaT);
+  f(a->RT);
+  f(a->gsum);
+  if (a->s) {
+    cudaDeviceSynchronize();
+    free_sim(a->s);
+  }
+  delete a;
+}
+
+static int adj_check_params(const gs_params* p) {
+  if (p->model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "adjoint: martensite model only");
+  if (p->mode != GS_MODE_BASELINE) return gs_set_error(GS_ENOTSUP, "adjoint: baseline mode only");
+  return GS_OK;
+}
+
+extern "C" int gs_adjoint_create(const gs_params* p, int nsteps, int checkpoint_every, gs_adjoint** out) {
+  if (!p || !out) return gs_set_error(GS_EINVAL, "gs_adjoint_create: null argument");
+  *out = nullptr;
+  GS_TRY(adj_check_params(p));
+  if (nsteps < 1) return gs_set_error(GS_EINVAL, "adjoint: nsteps %d", nsteps);
+  if (checkpoint_every < 1) return gs_set_error(GS_EINVAL, "adjoint: checkpoint_every %d", checkpoint_every);
+  gs_adjoint* a = new gs_adjoint();
+  int rc = gs_sim_create(p, &a->s);
+  if (rc != GS_OK) {
+    delete a;
+    return rc;
+  }
+  a->nsteps = nsteps;
+  a->K = checkpoint_every < nsteps ? checkpoint_every : nsteps;
+  a->nseg = (nsteps + a->K - 1) / a->K;
+  const size_t fb = (size_t)a->s->N * p->nvariants * elt(a->s);
+  auto fail = [&](int code) {
+    free_adjoint(a);
+    return code;
+  };
+  auto get = [&](void** q, size_t b, const char* what) {
+    const int r = dalloc(q, b, what);
+    if (r == GS_OK) a->bytes += b;
+    return r;
+  };
+  a->ckpt.assign(a->nseg, nullptr);
+  a->seg_eta.assign(a->K, nullptr);
+  a->seg_R.assign(a->K, nullptr);
+  for (int j = 0; j < a->nseg; ++j)
+    if ((rc = get(&a->ckpt[j], fb, "adjoint checkpoint")) != GS_OK) return fail(rc);
+  for (int i = 0; i < a->K; ++i) {
+    if (i > 0 && (rc = get(&a->seg_eta[i], fb, "adjoint segment")) != GS_OK) return fail(rc);
+    if ((rc = get(&a->seg_R[i], fb, "adjoint potentials")) != GS_OK) return fail(rc);
+  }
+  if ((rc = get(&a->lam[0], fb, "adjoint lambda")) != GS_OK) return fail(rc);
+  if ((rc = get(&a->lam[1], fb, "adjoint lambda")) != GS_OK) return fail(rc);
+  if ((rc = get(&a->etaT, fb, "final state")) != GS_OK) return fail(rc);
+  if ((rc = get(&a->RT, fb, "final potentials")) != GS_OK) return fail(rc);
+  if ((rc = get(reinterpret_cast<void**>(&a->gsum), (size_t)nsteps * ADJ_N * sizeof(double), "adjoint sums")) !=
+      GS_OK)
+    return fail(rc);
+  // the handle's own simulation buffers
+  a->bytes += fb * 3 + a->s->partials_cap * ACC_N * sizeof(double);
+  *out = a;
+  return GS_OK;
+}
+
+extern "C" int gs_adjoint_destroy(gs_adjoint* a) {
+  free_adjoint(a);
+  return GS_OK;
+}
+
+extern "C" size_t gs_adjoint_device_bytes(const gs_adjoint* a) { return a ? a->bytes : 0; }
+
+extern "C" int gs_adjoint_set_params(gs_adjoint* a, const gs_params* p) {
+  if (!a || !p) return gs_set_error(GS_EINVAL, "gs_adjoint_set_params: null argument");
+  GS_TRY(adj_check_params(p));
+  const gs_params& o = a->s->p;
+  if (p->nx != o.nx || p->ny != o.ny || p->nz != o.nz || p->nvariants != o.nvariants || p->dtype != o.dtype)
+    return gs_set_error(GS_EINVAL, "adjoint: grid, variant count and dtype are fixed at creation");
+  a->s->p = *p;
+  a->forward_done = false;
+  return GS_OK;
+}
+
+extern "C" int gs_adjoint_set_loss(gs_adjoint* a, const void* target, int dtype, double lam_el, double e_target) {
+  if (!a || !target) return gs_set_error(GS_EINVAL, "gs_adjoint_set_loss: null argument");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  if (!a->target) {
+    const size_t fb = (size_t)a->s->N * a->s->p.nvariants * elt(a->s);
+    GS_TRY(dalloc(&a->target, fb, "adjoint target"));
+    a->bytes += fb;
+  }
+  GS_TRY(upload(a->s, a->target, target, (size_t)a->s->N * a->s->p.nvariants, dtype));
+  a->lam_el = lam_el;
+  a->e_target = e_target;
+  a->have_target = true;
+  return GS_OK;
+}
+
+// location of eta_n during the forward run or a recompute of seg_valid
+static void* adj_eta(gs_adjoint* a, int n) {
+  if (n == a->nsteps) return a->etaT;
+  const int j = n / a->K, i = n % a->K;
+  if (i == 0) return a->ckpt[j];
+  if (j == a->seg_valid) return a->seg_eta[i];
+  return a->s->eta[n & 1];
+}
+
+template <typename T>
+static int adj_fwd_step(gs_adjoint* a, const void* in, void* out, void* r_out, int n, cudaStream_t st) {
+  gs_sim* s = a->s;
+  s->step = n;
+  GS_TRY(elastic_chain<T>(s, reinterpret_cast<const T*>(in), st));
+  MartArgs<T> ma;
+  fill_mart_args<T>(s, ma, reinterpret_cast<const T*>(in), reinterpret_cast<T*>(out));
+  ma.r_out = reinterpret_cast<T*>(r_out);
+  GS_CU(launch_mart_update<T>(ma, s->h, false, st, nullptr), "update pass");
+  s->launches += 1;
+  return GS_OK;
+}
+
+template <typename T> static int adj_forward(gs_adjoint* a, cudaStream_t st) {
+  gs_sim* s = a->s;
+  a->seg_valid = a->nseg - 1;
+  for (int n = 0; n < a->nsteps; ++n) {
+    void* r_out = n / a->K == a->nseg - 1 ? a->seg_R[n % a->K] : nullptr;
+    GS_TRY(adj_fwd_step<T>(a, adj_eta(a, n), adj_eta(a, n + 1), r_out, n, st));
+  }
+  // E_el and R at the final state
+  GS_TRY(elastic_chain<T>(s, reinterpret_cast<const T*>(a->etaT), st));
+  MartArgs<T> ma;
+  fill_mart_args<T>(s, ma, reinterpret_cast<const T*>(a->etaT), nullptr);
+  ma.r_out = reinterpret_cast<T*>(a->RT);
+  int nb = 0;
+  GS_CU(launch_mart_update<T>(ma, s->h, true, st, &nb), "final statistics");
+  GS_CU(launch_reduce(s->partials, nb, ACC_N, s->red, st), "reduce");
+  double acc[ACC_N];
+  GS_CU(cudaMemcpyAsync(acc, s->red, sizeof(acc), cudaMemcpyDeviceToHost, st), "stats D2H");
+  GS_CU(cudaStreamSynchronize(st), "forward sync");
+  a->e_el_T = acc[ACC_EEL] * s->p.dx * s->p.dy * s->p.dz;
+  s->step = a->nsteps;
+  a->forward_done = true;
+  return GS_OK;
+}
+
+extern "C" int gs_adjoint_forward(gs_adjoint* a, const void* eta0, int dtype, void* eta_final, double* e_el_final,
+                                  void* stream) {
+  if (!a || !eta0) return gs_set_error(GS_EINVAL, "gs_adjoint_forward: null argument");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  gs_sim* s = a->s;
+  const size_t count = (size_t)s->N * s->p.nvariants;
+  GS_TRY(upload(s, a->ckpt[0], eta0, count, dtype));
+  cudaStream_t st = pick_stream(s, stream);
+  s->launches = 0;
+  GS_TRY(s->p.dtype == GS_DTYPE_F64 ? adj_forward<double>(a, st) : adj_forward<float>(a, st));
+  if (e_el_final) *e_el_final = a->e_el_T;
+  if (eta_final) GS_TRY(download(s, a->etaT, eta_final, count, dtype));
+  return GS_OK;
+}
+
+template <typename T>
+static int adj_backward(gs_adjoint* a, const void* seed_dev, double seed_e, double* loss, double* grads,
+                        cudaStream_t st) {
+  gs_sim* s = a->s;
+  const gs_params& p = s->p;
+  const int V = p.nvariants;
+  const long long N = s->N;
+  const double dV = p.dx * p.dy * p.dz;
+  const double ce = seed_dev ? seed_e : 2.0 * a->lam_el * (a->e_el_T - a->e_target);
+  AdjSeedArgs<T> sa;
+  memset(&sa, 0, sizeof(sa));
+  sa.eta = reinterpret_cast<const T*>(a->etaT);
+  sa.R = reinterpret_cast<const T*>(a->RT);
+  sa.target = seed_dev ? nullptr : reinterpret_cast<const T*>(a->target);
+  sa.seed = reinterpret_cast<const T*>(seed_dev);
+  sa.lam = reinterpret_cast<T*>(a->lam[0]);
+  sa.n = N * V;
+  sa.c = ce * p.weight_elastic * dV;
+  sa.partials = s->partials;
+  int nb = 0;
+  GS_CU(launch_adj_seed<T>(sa, st, &nb), "adjoint seed");
+  GS_CU(launch_reduce(s->partials, nb, 1, s->red, st), "reduce");
+  double field = 0;
+  GS_CU(cudaMemcpyAsync(&field, s->red, sizeof(double), cudaMemcpyDeviceToHost, st), "loss D2H");
+  int c = 0;
+  const T* src[GS_MAXF];
+  const T* mul[GS_MAXF];
+  int sq[GS_MAXF];
+  for (int j = a->nseg - 1; j >= 0; --j) {
+    const int n0 = j * a->K, len = (j == a->nseg - 1) ? a->nsteps - n0 : a->K;
+    if (a->seg_valid != j) {  // recompute eta_n and R_n of the segment
+      a->seg_valid = j;
+      for (int i = 0; i < len; ++i) {
+        void* in = i == 0 ? a->ckpt[j] : a->seg_eta[i];
+        void* out = i + 1 < len ? a->seg_eta[i + 1] : s->eta[0];
+        GS_TRY(adj_fwd_step<T>(a, in, out, a->seg_R[i], n0 + i, st));
+      }
+    }
+    for (int i = len - 1; i >= 0; --i) {
+      const int n = n0 + i;
+      const T* eta = reinterpret_cast<const T*>(i == 0 ? a->ckpt[j] : a->seg_eta[i]);
+      const T* lin = reinterpret_cast<const T*>(a->lam[c]);
+      for (int f = 0; f < V; ++f) {
+        src[f] = eta + (long long)f * N;
+        mul[f] = lin + (long long)f * N;
+        sq[f] = 0;
+      }
+      GS_TRY(elastic_chain_g<T>(s, src, sq, V, 0, 1.0 / (double)N, s->spec, V, st, mul));
+      AdjArgs<T> aa;
+      memset(&aa, 0, sizeof(aa));
+      aa.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+      aa.eta = eta;
+      aa.lam_in = lin;
+      aa.lam_out = reinterpret_cast<T*>(a->lam[c ^ 1]);
+      aa.R = reinterpret_cast<const T*>(a->seg_R[i]);
+      aa.n0 = s->n0;
+      aa.n1 = s->n1;
+      aa.n2 = s->n2;
+      aa.nrows = (long long)s->n0 * s->n1;
+      aa.tw_h = twp<T>(s, 1);
+      aa.tw_n2 = twp<T>(s, 0);
+      s->step = n;
+      build_mart<T>(s, aa.mc);
+      aa.partials = s->partials;
+      aa.fd_n1 = FastDiv((uint32_t)s->n1);
+      aa.fd_upr = FastDiv((uint32_t)(s->n2 % 4 == 0 ? s->n2 / 4 : s->n2 / 2));
+      aa.fd_v = FastDiv((uint32_t)V);
+      int nbk = 0;
+      GS_CU(launch_adj_update<T>(aa, s->h, st, &nbk), "adjoint update");
+      GS_CU(launch_reduce(s->partials, nbk, ADJ_N, a->gsum + (size_t)n * ADJ_N, st), "adjoint reduce");
+      s->launches += 2;
+      c ^= 1;
+    }
+  }
+  std::vector<double> h((size_t)a->nsteps * ADJ_N);
+  GS_CU(cudaMemcpyAsync(h.data(), a->gsum, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "sums D2H");
+  GS_CU(cudaStreamSynchronize(st), "adjoint sync");
+  // Neumaier sums over the steps
+  double sum[ADJ_N], cmp[ADJ_N];
+  for (int k = 0; k < ADJ_N; ++k) sum[k] = cmp[k] = 0;
+  for (int n = 0; n < a->nsteps; ++n)
+    for (int k = 0; k < ADJ_N; ++k) {
+      const double x = h[(size_t)n * ADJ_N + k], t = sum[k] + x;
+      cmp[k] += std::fabs(sum[k]) >= std::fabs(x) ? (sum[k] - t) + x : (x - t) + sum[k];
+      sum[k] = t;
+    }
+  for (int k = 0; k < ADJ_N; ++k) sum[k] += cmp[k];
+  const double dt = p.dt, L = p.mobility;
+  grads[0] = dt * L * sum[ADJ_ETA_LAP];
+  grads[1] = -dt * L * sum[ADJ_ETA_LAM];
+  grads[2] = dt * L * sum[ADJ_ETA3_LAM];
+  grads[3] = -dt * L * sum[ADJ_S2_ETA_LAM];
+  grads[4] = -dt * L * sum[ADJ_AC_LAM];
+  grads[5] = dt * sum[ADJ_S_LAM] + ce * 2.0 * a->e_el_T;
+  if (loss) {
+    loss[1] = seed_dev ? 0.0 : field;
+    loss[2] = a->e_el_T;
+    loss[0] = seed_dev ? 0.0 : field + a->lam_el * (a->e_el_T - a->e_target) * (a->e_el_T - a->e_target);
+  }
+  return c;  // index of the buffer holding dJ/deta_0
+}
+
+extern "C" int gs_adjoint_backward(gs_adjoint* a, const void* seed, int seed_dtype, double seed_e, double* loss,
+                                   double* grads, void* grad_eta0, int grad_dtype, void* stream) {
+  if (!a || !grads) return gs_set_error(GS_EINVAL, "gs_adjoint_backward: null argument");
+  if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_adjoint_backward: run gs_adjoint_forward first");
+  if (!seed && !a->have_target) return gs_set_error(GS_EINVAL, "gs_adjoint_backward: no seed and no loss set");
+  gs_sim* s = a->s;
+  const size_t count = (size_t)s->N * s->p.nvariants;
+  if (seed) {
+    if (seed_dtype != GS_DTYPE_F32 && seed_dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", seed_dtype);
+    GS_TRY(upload(s, a->lam[1], seed, count, seed_dtype));
+  }
+  if (grad_eta0 && grad_dtype != GS_DTYPE_F32 && grad_dtype != GS_DTYPE_F64)
+    return gs_set_error(GS_EINVAL, "dtype %d", grad_dtype);
+  cudaStream_t st = pick_stream(s, stream);
+  s->launches = 0;
+  const void* sd = seed ? a->lam[1] : nullptr;
+  const int c = s->p.dtype == GS_DTYPE_F64 ? adj_backward<double>(a, sd, seed_e, loss, grads, st)
+                                           : adj_backward<float>(a, sd, seed_e, loss, grads, st);
+  if (c < 0) return c;
+  if (grad_eta0) GS_TRY(download(s, a->lam[c], grad_eta0, count, grad_dtype));
+  return GS_OK;
+}
+
+extern "C" int64_t gs_adjoint_launch_count(const gs_adjoint* a) { return a && a->s ? a->s->launches : 0; }

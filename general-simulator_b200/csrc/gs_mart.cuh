@@ -51,6 +51,7 @@ template <typename T> struct MartArgs {
   double* partials;  // [gridDim.x][ACC_N], statistics sweep only
   FastDiv fd_n1, fd_upr, fd_v;  // y extent, update runs per row, variants
   MartConst<T>* mcs;  // batched: constants of sim blockIdx.y in device memory
+  T* r_out;           // when set: R_p written out [V][N] (adjoint checkpoints)
 };
 
 // advance the step counter of every batched simulation (keeps a captured
@@ -187,6 +188,12 @@ __global__ void k_mart_update(MartArgs<T> a) {
     const T el_ = eq[rowb + (z0 == 0 ? n2 - 1 : z0 - 1)];
     const T er_ = eq[rowb + (z0 + CW == n2 ? 0 : z0 + CW)];
     const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
+    if (!BATCH && a.r_out) {
+      T rv[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) rv[j] = Rq[j];
+      stv<CW>(a.r_out + (long long)q * N + cell, rv);
+    }
     T Kq[CW], dfc[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {

@@ -152,6 +152,7 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
 template <typename T> struct ZfwdArgs {
   const T* src[2 * GS_MAXF];   // row source of each field (n0*n1 rows of n2)
   int square[2 * GS_MAXF];     // 1: transform src^2 (eta^2), 0: src
+  const T* mul[2 * GS_MAXF];   // when set: transform src * mul (eta lam, adjoint)
   const T* src0;               // when set: field f at src0 + f * fstride (batches)
   long long fstride;
   int square0;
@@ -180,10 +181,15 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
     const long long rin = row - (long long)f * a.rows_per_field;
     const V* src = reinterpret_cast<const V*>(a.src0 ? a.src0 + f * a.fstride : a.src[f]) + rin * H;
     const int sq = a.src0 ? a.square0 : a.square[f];
+    const T* mp = a.src0 ? nullptr : a.mul[f];
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) {
       V x = src[L::in_pos(t, r)];
       if (sq) x = mk2(x.x * x.x, x.y * x.y);
+      if (mp) {
+        const V m = reinterpret_cast<const V*>(mp)[rin * H + L::in_pos(t, r)];
+        x = mk2(x.x * m.x, x.y * m.y);
+      }
       v[r] = x;
     }
   } else {

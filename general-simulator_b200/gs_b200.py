@@ -148,6 +148,15 @@ def lib() -> C.CDLL:
         "gs_batch_launch_count": (C.c_int64, [vp]),
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
+        "gs_adjoint_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),
+        "gs_adjoint_destroy": (C.c_int, [vp]),
+        "gs_adjoint_set_params": (C.c_int, [vp, P]),
+        "gs_adjoint_set_loss": (C.c_int, [vp, vp, C.c_int, C.c_double, C.c_double]),
+        "gs_adjoint_forward": (C.c_int, [vp, vp, C.c_int, vp, C.POINTER(C.c_double), vp]),
+        "gs_adjoint_backward": (C.c_int, [vp, vp, C.c_int, C.c_double, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), vp, C.c_int, vp]),
+        "gs_adjoint_device_bytes": (C.c_size_t, [vp]),
+        "gs_adjoint_launch_count": (C.c_int64, [vp]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
         "gs_mart_step_noalloc_max_bytes": (C.c_size_t, []),
     }
@@ -182,6 +191,71 @@ def default_params(model: int, mode: int = GS_MODE_BASELINE) -> GsParams:
 
 def _np_dtype(code: int):
     return np.float64 if code == GS_DTYPE_F64 else np.float32
+
+
+class Adjoint:
+    """Checkpointed adjoint of a martensite run (gs_adjoint*): forward() runs
+    eta0 -> eta_T keeping a checkpoint every `checkpoint_every` steps;
+    backward() returns (loss[3], grads[6], dJ/deta0) with grads over
+    (kappa, A2, A4, A6, Ac, eigenstrain scale s)."""
+
+    PARAM_NAMES = ("kappa", "A2", "A4", "A6", "Ac", "s")
+
+    def __init__(self, params: GsParams, nsteps: int, checkpoint_every: int):
+        self.params = params.copy()
+        self.nsteps = nsteps
+        h = C.c_void_p()
+        check(lib().gs_adjoint_create(C.byref(self.params), nsteps, checkpoint_every, C.byref(h)), "gs_adjoint_create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().gs_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        p = self.params
+        return (p.nvariants, p.nx, p.ny, p.nz)
+
+    def set_params(self, params: GsParams) -> None:
+        self.params = params.copy()
+        check(lib().gs_adjoint_set_params(self.h, C.byref(self.params)), "gs_adjoint_set_params")
+
+    def set_loss(self, target: np.ndarray, lam_el: float, e_target: float) -> None:
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        check(lib().gs_adjoint_set_loss(self.h, t.ctypes.data, GS_DTYPE_F64, lam_el, e_target), "gs_adjoint_set_loss")
+
+    def forward(self, eta0: np.ndarray, stream: int = 0):
+        e = np.ascontiguousarray(eta0, dtype=np.float64)
+        out = np.empty(self.shape, dtype=np.float64)
+        eel = C.c_double()
+        check(lib().gs_adjoint_forward(self.h, e.ctypes.data, GS_DTYPE_F64, out.ctypes.data, C.byref(eel),
+                                       C.c_void_p(stream)), "gs_adjoint_forward")
+        return out, eel.value
+
+    def backward(self, seed: Optional[np.ndarray] = None, seed_e: float = 0.0, stream: int = 0):
+        loss = (C.c_double * 3)()
+        g = (C.c_double * 6)()
+        ge = np.empty(self.shape, dtype=np.float64)
+        sd = None
+        if seed is not None:
+            sd = np.ascontiguousarray(seed, dtype=np.float64)
+        check(lib().gs_adjoint_backward(self.h, None if sd is None else sd.ctypes.data, GS_DTYPE_F64, seed_e, loss, g,
+                                        ge.ctypes.data, GS_DTYPE_F64, C.c_void_p(stream)), "gs_adjoint_backward")
+        return np.array(loss[:]), np.array(g[:]), ge
+
+    def device_bytes(self) -> int:
+        return int(lib().gs_adjoint_device_bytes(self.h))
+
+    def launch_count(self) -> int:
+        return int(lib().gs_adjoint_launch_count(self.h))
 
 
 class Sim:

@@ -202,6 +202,34 @@ int gs_sim_use_graph(gs_sim* s, int on);
 int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void* eta_out, int64_t step, void* stream);
 size_t gs_mart_step_noalloc_max_bytes(void);
 
+/* ---- adjoint of the martensite run ------------------------------------ */
+/* The reference has no adjoint; this is the transpose of its explicit step
+ * (Dynamics_mart::Calculate, src/dynamics_mart.cu:348-417) in baseline mode,
+ * noise included (it is additive) and defect/dislocation inputs excluded.
+ * A handle holds a fixed grid and step count: gs_adjoint_forward runs eta_0
+ * -> eta_T keeping every checkpoint_every-th state, gs_adjoint_backward
+ * recomputes each segment from its checkpoint and sweeps the adjoint back to
+ * eta_0.  Loss mode (gs_adjoint_set_loss, seed == NULL):
+ *   J = sum (eta_T - target)^2 + lam_el (E_el(T) - e_target)^2;
+ * seed mode: J = <seed, eta_T> + seed_e E_el(T) (a vector-Jacobian product).
+ * grads[6] = dJ/d(kappa, A2, A4, A6, Ac, s), s the eigenstrain scale
+ * (eps_p -> s eps_p at s = 1); grad_eta0 = dJ/deta_0 ([V][N], may be NULL);
+ * loss[3] = (J, field term, E_el(T)) (NULL allowed). */
+typedef struct gs_adjoint gs_adjoint;
+int gs_adjoint_create(const gs_params* p, int nsteps, int checkpoint_every, gs_adjoint** out);
+int gs_adjoint_destroy(gs_adjoint* a);
+/* New coefficients for the next forward run (grid, V and dtype fixed). */
+int gs_adjoint_set_params(gs_adjoint* a, const gs_params* p);
+int gs_adjoint_set_loss(gs_adjoint* a, const void* target, int dtype, double lam_el, double e_target);
+int gs_adjoint_forward(gs_adjoint* a, const void* eta0, int dtype, void* eta_final, double* e_el_final,
+                       void* stream);
+int gs_adjoint_backward(gs_adjoint* a, const void* seed, int seed_dtype, double seed_e, double* loss,
+                        double* grads, void* grad_eta0, int grad_dtype, void* stream);
+/* Device bytes held by the handle (checkpoints, segment, adjoint fields). */
+size_t gs_adjoint_device_bytes(const gs_adjoint* a);
+/* Kernel launches issued by the last forward or backward call. */
+int64_t gs_adjoint_launch_count(const gs_adjoint* a);
+
 /* ---- batched ensembles ------------------------------------------------- */
 /* Many independent martensite simulations advanced together.  Simulations
  * of one grid, variant count, modulus and eigenstrain direction form a group
