@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the comparator, adjoint and ensemble measurements (1 GPU only)")
     return ap.parse_args()
 
 
@@ -171,6 +173,134 @@ def committed_traffic() -> dict | None:
         return None
     with open(path) as f:
         return json.load(f)
+
+
+# ---------------------------------------------------------------------------
+# secondary measurements of the metric (1 GPU): cuFFT comparator, adjoint,
+# batched ensemble; device time with CUDA events on the launching stream
+# ---------------------------------------------------------------------------
+def _timed(stream, fn) -> float:
+    import torch
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def extra_comparator(n: int, ours_ms: float, steps: int = 50) -> dict:
+    """The same step in the reference's structure with cuFFT C2C (plain)."""
+    import torch
+
+    import gs_b200 as gb
+
+    p = gb.mart3d_params(n, dtype=gb.GS_DTYPE_F32, noise=1e-3)
+    sim = gb.Sim(p, plain=True)
+    sim.set_field("eta", gb.initial_eta(p, 1).astype(np.float32))
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        sim.step(5, stream.cuda_stream)
+        ms = _timed(stream, lambda: sim.step(steps, stream.cuda_stream)) / steps
+    sim.close()
+    return {"what": "plain GPU step: cuFFT C2C batch V, B(n) streamed from a [V][V][N] array, unfused sweeps",
+            "ms_per_step": ms, "ours_ms_per_step": ours_ms, "speedup": ms / ours_ms, "steps": steps}
+
+
+def extra_adjoint(steps_fwd: int = 200) -> dict:
+    """Calibration workload: 96^3, 3 variants, FP32, 200 steps, checkpoint
+    every 20, noise off.  forward = 200 plain steps (gs_sim_step); backward
+    = gs_adjoint_backward (segment recompute + adjoint sweeps + gradient
+    sums), both device time on one stream."""
+    import ctypes as C
+
+    import torch
+
+    import gs_b200 as gb
+    import gs_torch as gt
+
+    run, th0, eta0, target, et = gt.calibration_setup(96, steps_fwd, gb.GS_DTYPE_F32, 20)
+    a = run.adj
+    p = run.params_for(th0)
+    a.set_params(p)
+    a.set_loss(target, 0.1, et)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    L = gb.lib()
+    loss = (C.c_double * 3)()
+    g = (C.c_double * 6)()
+
+    def back():
+        gb.check(L.gs_adjoint_backward(a.h, None, 0, 0.0, loss, g, None, 0, C.c_void_p(sh)), "backward")
+
+    with torch.cuda.stream(stream):
+        a.forward(eta0, sh)
+        back()
+        bwd = min(_timed(stream, back) for _ in range(3))
+        launches = a.launch_count()
+        sim = gb.Sim(p)
+        sim.set_field("eta", eta0.astype(np.float32))
+        sim.step(20, sh)
+        fwd = min(_timed(stream, lambda: sim.step(steps_fwd, sh)) for _ in range(3))
+        sim.close()
+    mem = a.device_bytes()
+    run.close()
+    return {"workload": "96^3, 3 variants, FP32, 200 steps, checkpoint every 20, noise off",
+            "forward_ms": fwd, "backward_ms": bwd, "adjoint_to_forward": bwd / fwd,
+            "backward_launches": launches, "device_bytes": mem,
+            "note": "backward includes recomputing every segment from its checkpoint"}
+
+
+def extra_ensemble(steps: int = 100, total_steps: int = 2000) -> dict:
+    """64 uneven simulations in grouped launches with CUDA-graph replay
+    against the same simulations run one after another with the plain
+    (cuFFT) step and with the hand-written single-simulation step."""
+    import torch
+
+    import gs_b200 as gb
+
+    ps = gb.ensemble_params(gb.GS_DTYPE_F32)
+    b = gb.Batch(ps)
+    for i, p in enumerate(ps):
+        b.set_eta(i, gb.initial_eta(p, 200 + i).astype(np.float32))
+    b.use_graph(True)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        b.step(4, sh)
+        ms = _timed(stream, lambda: b.step(steps, sh)) / steps
+    groups = b.groups()
+    b.close()
+    cells = sum(p.ncells for p in ps)
+    shapes = {}
+    for p in ps:
+        shapes.setdefault((p.nx, p.ny, p.nz, p.nvariants), []).append(p)
+    seq = {"plain": 0.0, "ours": 0.0}
+    per_shape = {}
+    with torch.cuda.stream(stream):
+        for key, plist in shapes.items():
+            row = {}
+            for kind in ("plain", "ours"):
+                sim = gb.Sim(plist[0], plain=kind == "plain")
+                sim.set_field("eta", gb.initial_eta(plist[0], 7).astype(np.float32))
+                sim.step(3, sh)
+                t = _timed(stream, lambda: sim.step(20, sh)) / 20
+                sim.close()
+                row[kind] = t
+                seq[kind] += t * len(plist)
+            per_shape["x".join(map(str, key[:3])) + f"/V{key[3]}"] = {**row, "count": len(plist)}
+    sims_s = len(ps) / (ms * total_steps / 1e3)
+    return {"workload": "64 sims: 32 x 128^2 + 16 x 256^2 (V=2), 12 x 64^3 + 4 x 128^3 (V=3), FP32, "
+                        f"noise 1e-3, {total_steps} steps each",
+            "batched_ms_per_step": ms, "groups": groups, "sims_per_s": sims_s,
+            "cell_updates_per_s": cells * 1e3 / ms,
+            "sequential_plain_sims_per_s": len(ps) / (seq["plain"] * total_steps / 1e3),
+            "sequential_ours_sims_per_s": len(ps) / (seq["ours"] * total_steps / 1e3),
+            "vs_sequential_plain": seq["plain"] / ms, "vs_sequential_ours": seq["ours"] / ms,
+            "per_shape_ms_per_step": per_shape, "timed_steps": steps}
 
 
 # ---------------------------------------------------------------------------
@@ -331,6 +461,11 @@ def run_ours(args, ws, rank, local):
 
     if rank != 0:
         return
+    extras = {}
+    if ws == 1 and not args.no_extras:
+        extras["comparator"] = extra_comparator(n, ms / args.steps)
+        extras["adjoint"] = extra_adjoint()
+        extras["ensemble"] = extra_ensemble()
     cpu = None
     if ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(n, args.cpu_seconds)
@@ -350,6 +485,7 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
+        **extras,
     }
     print(json.dumps(line), flush=True)
 

@@ -149,8 +149,10 @@ template <typename T> int plain_init(gs_sim* s) {
   if (gs_cuda_check(cudaMalloc(&ps->chem, rb), "plain chem") != GS_OK) return GS_ENOMEM;
   if (gs_cuda_check(cudaMalloc(&ps->elf, rb), "plain elastic") != GS_OK) return GS_ENOMEM;
   int n[3] = {s->n0, s->n1, s->n2};
+  // unit axes lead the canonical grid: plan over the remaining ones
+  const int rank = s->n0 > 1 ? 3 : (s->n1 > 1 ? 2 : 1);
   const cufftType ty = sizeof(T) == 8 ? CUFFT_Z2Z : CUFFT_C2C;
-  if (cufftPlanMany(&ps->plan, 3, n, nullptr, 1, (int)N, nullptr, 1, (int)N, ty, V) != CUFFT_SUCCESS)
+  if (cufftPlanMany(&ps->plan, rank, n + (3 - rank), nullptr, 1, (int)N, nullptr, 1, (int)N, ty, V) != CUFFT_SUCCESS)
     return gs_set_error(GS_ECUDA, "cufftPlanMany failed");
   PGeo g{s->n0, s->n1, s->n2, V, N, {s->perm[0], s->perm[1], s->perm[2]}};
   ElasticConst<T> ec;

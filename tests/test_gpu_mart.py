@@ -198,6 +198,15 @@ def test_plain_comparator_matches_oracle(gb, orc, dtype, tol):
     assert rel_l2(got, ref) < tol
 
 
+@pytest.mark.parametrize("shape,V", [((32, 48, 1), 2), ((1, 16, 24), 2)])
+def test_plain_comparator_2d_matches_oracle(gb, orc, shape, V):
+    p = base3d(gb, shape, F64, noise=1e-3, V=V)
+    eta0 = gb.initial_eta(p, 17, 0.4)
+    ref = orc.mart_run(p, eta0, 2)
+    got = gpu_run(gb, p, eta0, 2, plain=True)
+    assert rel_l2(got, ref) < 1e-11
+
+
 def test_step_counter_continues_noise_stream(gb, orc):
     p = base3d(gb, (8, 8, 8), F64, noise=1e-2)
     eta0 = gb.initial_eta(p, 16, 0.2)
