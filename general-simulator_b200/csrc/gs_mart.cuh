@@ -125,10 +125,14 @@ template <int CW> __device__ __forceinline__ void stv(double* p, const double (&
 // One row group per block: the inverse z FFT of R_p for every (variant,
 // row) line leaves R in shared memory; then each thread updates a run of CW
 // cells (a quad, or a pair when n2 = 2) for all variants at once, so the
-// Landau coupling, the defect mask and one Philox block per variant serve
-// the whole run.
+// centre values, the Landau coupling sums and the defect mask are loaded and
+// formed once per run, and one Philox block per variant serves the run.
+template <int VM, bool STATS> struct UpdBlocks {  // resident blocks asked of the register allocator
+  static constexpr int v = (VM <= 4 && !STATS) ? 3 : 1;
+};
+
 template <typename T, int H, int VM, bool STATS, bool BATCH>
-__global__ void k_mart_update(MartArgs<T> a) {
+__global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(MartArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
   constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
@@ -160,13 +164,12 @@ __global__ void k_mart_update(MartArgs<T> a) {
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const long long N = a.nrows * n2;
   const int upr = n2 / CW;
-  const int nunits = a.lr * Vn * upr;
-  // unit w -> (row rr, variant q, run u); runs of one (row, variant) are
-  // consecutive so neighbouring threads touch neighbouring cells
+  const int nunits = a.lr * upr;
+  // unit w -> (row rr, run u); runs of one row are consecutive so
+  // neighbouring threads touch neighbouring cells
 #pragma unroll 1
   for (int w = threadIdx.x; w < nunits; w += blockDim.x) {
-    const int rq = (int)a.fd_upr.div((uint32_t)w), u = w - rq * upr;
-    const int rr = (int)a.fd_v.div((uint32_t)rq), q = rq - rr * Vn;
+    const int rr = (int)a.fd_upr.div((uint32_t)w), u = w - rr * upr;
     const long long row = (long long)blockIdx.x * a.lr + rr;
     if (row >= a.nrows) continue;
     const int x = (int)a.fd_n1.div((uint32_t)row), y = (int)(row - (long long)x * n1);
@@ -174,96 +177,106 @@ __global__ void k_mart_update(MartArgs<T> a) {
     const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
     const int z0 = u * CW;
     const long long rowb = row * n2, cell = rowb + z0;
+    // neighbour offsets relative to the run, the same for every variant
+    const long long oxp = ((long long)xp * n1 + y) * n2 + z0 - cell, oxm = ((long long)xm * n1 + y) * n2 + z0 - cell;
+    const long long oyp = ((long long)x * n1 + yp) * n2 + z0 - cell, oym = ((long long)x * n1 + ym) * n2 + z0 - cell;
+    const int ozl = (z0 == 0 ? n2 - 1 : z0 - 1) - z0, ozr = (z0 + CW == n2 ? 0 : z0 + CW) - z0;
     T e[VM][CW];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
       if (p < Vn) ldv<CW>(a.eta_in + (long long)p * N + cell, e[p]);
-    const T* eq = a.eta_in + (long long)q * N;
-    T vxp[CW], vxm[CW], vyp[CW], vym[CW], et_[CW];
-    ldv<CW>(eq + ((long long)xp * n1 + y) * n2 + z0, vxp);
-    ldv<CW>(eq + ((long long)xm * n1 + y) * n2 + z0, vxm);
-    ldv<CW>(eq + ((long long)x * n1 + yp) * n2 + z0, vyp);
-    ldv<CW>(eq + ((long long)x * n1 + ym) * n2 + z0, vym);
-    ldv<CW>(eq + cell, et_);
-    const T el_ = eq[rowb + (z0 == 0 ? n2 - 1 : z0 - 1)];
-    const T er_ = eq[rowb + (z0 + CW == n2 ? 0 : z0 + CW)];
-    const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
-    if (!BATCH && a.r_out) {
-      T rv[CW];
-#pragma unroll
-      for (int j = 0; j < CW; ++j) rv[j] = Rq[j];
-      stv<CW>(a.r_out + (long long)q * N + cell, rv);
-    }
-    T Kq[CW], dfc[CW];
+    T s2[CW], s4[CW], pr[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
-      Kq[j] = 0;
-      dfc[j] = 1;
+      T a2 = 0, a4 = 0, ap = 0;
+#pragma unroll
+      for (int p = 0; p < VM; ++p)
+        if (p < Vn) {
+          const T e2 = e[p][j] * e[p][j];
+          ap += a2 * e2;
+          a2 += e2;
+          a4 += e2 * e2;
+        }
+      s2[j] = a2;
+      s4[j] = a4;
+      pr[j] = ap;
     }
-    if (mc.has_K) ldv<CW>(a.K + (long long)q * N + cell, Kq);
+    T dfc[CW];
+#pragma unroll
+    for (int j = 0; j < CW; ++j) dfc[j] = 1;
     if (mc.has_defect) {
       ldv<CW>(a.defect + cell, dfc);
 #pragma unroll
       for (int j = 0; j < CW; ++j) dfc[j] = (T)1 - dfc[j];
     }
-    T xi[4] = {0, 0, 0, 0};
-    if (!STATS && mc.noise != (T)0) normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
-    const int xo = (int)(cell & 3);
-    T lq = 0;
+    // a run of 2 (n2 = 2 mod 4) may sit in the upper half of its Philox quad
+    const bool hi_pair = CW == 2 && (cell & 2);
 #pragma unroll
-    for (int p = 0; p < VM; ++p)
-      if (p == q) lq = mc.lin[p];
-    T out[CW];
+    for (int q = 0; q < VM; ++q) {
+      if (q >= Vn) break;
+      const T* eq = a.eta_in + (long long)q * N + cell;
+      T vxp[CW], vxm[CW], vyp[CW], vym[CW];
+      ldv<CW>(eq + oxp, vxp);
+      ldv<CW>(eq + oxm, vxm);
+      ldv<CW>(eq + oyp, vyp);
+      ldv<CW>(eq + oym, vym);
+      const T el_ = eq[ozl], er_ = eq[ozr];
+      const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
+      T Kq[CW];
 #pragma unroll
-    for (int j = 0; j < CW; ++j) {
-      T s2 = 0, s4 = 0, pr = 0;
+      for (int j = 0; j < CW; ++j) Kq[j] = 0;
+      if (mc.has_K) ldv<CW>(a.K + (long long)q * N + cell, Kq);
+      T xi[4] = {0, 0, 0, 0};
+      if (!STATS && mc.noise != (T)0)
+        normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
+      const T lq = mc.lin[q];
+      T out[CW], rv[CW];
 #pragma unroll
-      for (int p = 0; p < VM; ++p)
-        if (p < Vn) {
-          const T e2 = e[p][j] * e[p][j];
-          pr += s2 * e2;
-          s2 += e2;
-          s4 += e2 * e2;
+      for (int j = 0; j < CW; ++j) {
+        const T et = e[q][j];
+        const T zlv = j == 0 ? el_ : e[q][j - 1];
+        const T zrv = j == CW - 1 ? er_ : e[q][j + 1];
+        const T d0 = vxp[j] + vxm[j] - 2 * et, d1 = vyp[j] + vym[j] - 2 * et, d2 = zlv + zrv - 2 * et;
+        const T grad = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;
+        T chem;
+        if (mc.refcompat) {
+          const T se = mc.s * et;
+          chem = et >= (T)0 ? -mc.wC * se * (mc.a1 - mc.a2 * se * se + mc.a3 * mc.s * mc.s * s2[j])
+                            : (T)1000 * mc.wC * mc.a2 * et * et;
+        } else {
+          const T e2 = et * et;
+          chem = -mc.L * (mc.A2 * et - mc.A4 * e2 * et + mc.A6 * s2[j] * s2[j] * et +
+                          (T)2 * mc.Ac * et * (s2[j] - e2));
         }
-      const T et = et_[j];
-      const T zlv = j == 0 ? el_ : et_[j - 1];
-      const T zrv = j == CW - 1 ? er_ : et_[j + 1];
-      const T d0 = vxp[j] + vxm[j] - 2 * et, d1 = vyp[j] + vym[j] - 2 * et, d2 = zlv + zrv - 2 * et;
-      const T grad = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;
-      T chem;
-      if (mc.refcompat) {
-        const T se = mc.s * et;
-        chem = et >= (T)0 ? -mc.wC * se * (mc.a1 - mc.a2 * se * se + mc.a3 * mc.s * mc.s * s2)
-                          : (T)1000 * mc.wC * mc.a2 * et * et;
-      } else {
-        const T e2 = et * et;
-        chem = -mc.L * (mc.A2 * et - mc.A4 * e2 * et + mc.A6 * s2 * s2 * et + (T)2 * mc.Ac * et * (s2 - e2));
+        const T Rv = Rq[j];
+        rv[j] = Rv;
+        const T el = mc.el * Rv * et;
+        const T lin = (lq + mc.kc * Kq[j]) * et;
+        const T rhs = grad + chem + el + lin;
+        const T xij = CW == 2 ? (hi_pair ? xi[j + 2 < 4 ? j + 2 : 3] : xi[j]) : xi[j];
+        T en = et + mc.dt * rhs + mc.noise * xij;
+        if (mc.has_defect) en *= dfc[j];
+        out[j] = en;
+        if (STATS) {
+          acc[ACC_MASS].add((double)et);
+          acc[ACC_ETA2 + q].add((double)et * (double)et);
+          acc[ACC_VF + q].add(fabs((double)et) > 0.5 ? 1.0 : 0.0);
+          acc[ACC_EEL].add((double)mc.wel_half * (double)et * (double)et * (double)Rv);
+          const double lg = (double)mc.gcoef[0] * d0 + (double)mc.gcoef[1] * d1 + (double)mc.gcoef[2] * d2;
+          acc[ACC_EGRAD].add(-0.5 * (double)mc.kappa * (double)et * lg);
+          acc[ACC_EAPPL].add(-((double)mc.appl[q] + (double)mc.wD * Kq[j]) * (double)et * (double)et);
+          if (q == 0)
+            acc[ACC_ECHEM].add((double)mc.A2 / 2 * s2[j] - (double)mc.A4 / 4 * s4[j] +
+                               (double)mc.A6 / 6 * (double)s2[j] * s2[j] * s2[j] + (double)mc.Ac * pr[j]);
+          acc[ACC_FGRAD].add((double)grad);
+          acc[ACC_FCHEM].add((double)chem);
+          acc[ACC_FEL].add((double)el);
+          acc[ACC_FDISL].add((double)lin);
+        }
       }
-      const T Rv = Rq[j];
-      const T el = mc.el * Rv * et;
-      const T lin = (lq + mc.kc * Kq[j]) * et;
-      const T rhs = grad + chem + el + lin;
-      T en = et + mc.dt * rhs + mc.noise * xi[(xo + j) & 3];
-      if (mc.has_defect) en *= dfc[j];
-      out[j] = en;
-      if (STATS) {
-        acc[ACC_MASS].add((double)et);
-        acc[ACC_ETA2 + q].add((double)et * (double)et);
-        acc[ACC_VF + q].add(fabs((double)et) > 0.5 ? 1.0 : 0.0);
-        acc[ACC_EEL].add((double)mc.wel_half * (double)et * (double)et * (double)Rv);
-        const double lg = (double)mc.gcoef[0] * d0 + (double)mc.gcoef[1] * d1 + (double)mc.gcoef[2] * d2;
-        acc[ACC_EGRAD].add(-0.5 * (double)mc.kappa * (double)et * lg);
-        acc[ACC_EAPPL].add(-((double)mc.appl[q] + (double)mc.wD * Kq[j]) * (double)et * (double)et);
-        if (q == 0)
-          acc[ACC_ECHEM].add((double)mc.A2 / 2 * s2 - (double)mc.A4 / 4 * s4 +
-                             (double)mc.A6 / 6 * (double)s2 * s2 * s2 + (double)mc.Ac * pr);
-        acc[ACC_FGRAD].add((double)grad);
-        acc[ACC_FCHEM].add((double)chem);
-        acc[ACC_FEL].add((double)el);
-        acc[ACC_FDISL].add((double)lin);
-      }
+      if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
+      if (!BATCH && a.r_out) stv<CW>(a.r_out + (long long)q * N + cell, rv);
     }
-    if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
   }
   if (STATS) block_reduce_store(acc, ACC_N, a.partials);
 }
