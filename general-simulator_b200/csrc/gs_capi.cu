@@ -412,6 +412,69 @@ template <typename T> static const cplx<T>* twp(const gs_sim* s, int which) {
 }
 
 // ---------------------------------------------------------------------------
+// octant table of B(k)
+// ---------------------------------------------------------------------------
+// B(k) is even in axis c when reflecting that axis maps the problem onto
+// itself: the stresses sigma = C:eps have no shear component coupling c with
+// another axis, and the quadratic form Omega^-1(n) keeps its parity.  Axes of
+// extent 1 carry k = 0 only and need no check.
+static bool btab_symmetric(const gs_sim* s) {
+  ElasticConst<double> ec;
+  build_elastic<double>(s, 0, 1.0, ec);
+  const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
+  const int nc[3] = {s->n0, s->n1, s->n2};
+  for (int c = 0; c < 3; ++c) {
+    if (nc[c] == 1) continue;
+    for (int f = 0; f < ec.nb; ++f)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          if ((i == c) != (j == c) && (ec.sa[f][i][j] != 0.0 || ec.sb[f][i][j] != 0.0)) return false;
+    for (int e = 0; e < 6; ++e)
+      for (int q = 0; q < 6; ++q) {
+        const int pe = (pa[e] == c) + (pb[e] == c), pq = (pa[q] == c) + (pb[q] == c);
+        if ((pe + pq) % 2 != 0 && ec.qs[e][q] != 0.0) return false;
+      }
+  }
+  return true;
+}
+
+// (Re)build the table of the handle's current parameters (martensite only).
+template <typename T> static int build_btab(gs_sim* s, cudaStream_t st) {
+  if (s->p.model != GS_MODEL_MART || s->btab_state == -1) return GS_OK;
+  if (!btab_symmetric(s)) {
+    s->btab_state = -2;
+    return GS_OK;
+  }
+  const size_t npt = (size_t)(s->n0 / 2 + 1) * (s->n1 / 2 + 1) * (s->n2 / 2 + 1);
+  const size_t bytes = npt * btab_stride(s->p.nvariants) * sizeof(T);
+  if (s->btab && s->btab_bytes != bytes) {
+    cudaFree(s->btab);
+    s->btab = nullptr;
+  }
+  if (!s->btab) {
+    GS_CU(cudaMalloc(&s->btab, bytes), "cudaMalloc B table");
+    s->btab_bytes = bytes;
+  }
+  ElasticConst<T> ec;
+  build_elastic<T>(s, 0, 1.0 / (double)s->N, ec);
+  GS_CU(launch_btab_fill<T>(ec, s->n0, s->n1, s->n2, reinterpret_cast<T*>(s->btab), st), "B table fill");
+  GS_CU(cudaStreamSynchronize(st), "B table sync");
+  s->btab_state = 1;
+  return GS_OK;
+}
+
+static int ensure_btab(gs_sim* s, cudaStream_t st) {
+  return s->p.dtype == GS_DTYPE_F64 ? build_btab<double>(s, st) : build_btab<float>(s, st);
+}
+
+template <typename T> static void set_btab(const gs_sim* s, XArgs<T>& xa) {
+  xa.btab = reinterpret_cast<const T*>(s->btab);
+  xa.bt_d1 = s->n1 / 2 + 1;
+  xa.bt_d2 = s->n2 / 2 + 1;
+  xa.bt_stride = btab_stride(s->p.nvariants);
+}
+
+// ---------------------------------------------------------------------------
 // the martensite step
 // ---------------------------------------------------------------------------
 // z forward (with the eta^2 prologue where square[f]) -> y forward -> x pass
@@ -454,6 +517,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   xa.G = G;
   xa.tw = twp<T>(s, 3);
   build_elastic<T>(s, which, scale, xa.ec);
+  if (which == 0 && s->btab_state == 1) set_btab<T>(s, xa);
   GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
   gs_mark(s, st);
   YArgs<T> yb = ya;
@@ -789,7 +853,7 @@ static size_t elt(const gs_sim* s) { return s->p.dtype == GS_DTYPE_F64 ? 8 : 4; 
 static void free_sim(gs_sim* s) {
   if (!s) return;
   void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->rbuf, s->mubuf,
-                  s->stressbuf, s->ktab, s->tw, s->partials, s->red};
+                  s->stressbuf, s->ktab, s->tw, s->partials, s->red, s->btab};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -874,6 +938,7 @@ extern "C" int gs_sim_create(const gs_params* p, gs_sim** out) {
   if ((rc = gs_cuda_check(cudaMalloc(&s->partials, s->partials_cap * ACC_N * sizeof(double)), "partials")) != GS_OK)
     return fail(rc);
   if ((rc = gs_cuda_check(cudaMalloc(&s->red, 64 * sizeof(double)), "reduce out")) != GS_OK) return fail(rc);
+  if ((rc = ensure_btab(s, s->own_stream)) != GS_OK) return fail(rc);
   *out = s;
   return GS_OK;
 }
@@ -1088,6 +1153,12 @@ extern "C" int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, siz
     if (bytes) *bytes = fb * s->p.nvariants;
     return GS_OK;
   }
+  if (nm == "btable") {  // octant table of B(k); NULL when B is formed on the fly
+    const bool on = s->btab_state == 1;
+    *dptr = on ? s->btab : nullptr;
+    if (bytes) *bytes = on ? s->btab_bytes : 0;
+    return GS_OK;
+  }
   return gs_set_error(GS_EINVAL, "unknown device field '%s'", name);
 }
 
@@ -1217,6 +1288,7 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   xa.simscale = reinterpret_cast<const T*>(g->d_simscale);
   xa.tw = twp<T>(g, 3);
   build_elastic<T>(g, 0, 1.0 / (double)g->N, xa.ec);
+  if (g->btab_state == 1) set_btab<T>(g, xa);
   GS_CU(launch_xcontract<T>(xa, st), "batch x pass");
   GS_CU(launch_ypass<T>(ya, g->n1, VT, 1, st), "batch y inverse");
   MartArgs<T> ma;
@@ -1296,6 +1368,7 @@ extern "C" int gs_batch_create(const gs_params* params, int nsims, gs_batch** ou
     if ((rc = gs_cuda_check(cudaMalloc(&g->partials, g->partials_cap * ACC_N * sizeof(double)), "partials")) != GS_OK)
       return fail(rc);
     if ((rc = gs_cuda_check(cudaMalloc(&g->red, 64 * sizeof(double)), "reduce out")) != GS_OK) return fail(rc);
+    if ((rc = ensure_btab(g, b->stream)) != GS_OK) return fail(rc);
     g->own_stream = nullptr;
   }
   *out = b;
@@ -1428,6 +1501,7 @@ extern "C" int gs_batch_stats(gs_batch* b, int sim, gs_stats* out, void* stream)
   gs_sim view = *g;
   view.p = g->bp[slot];
   view.nb = 1;
+  view.btab_state = -2;  // the group's table holds the group's B, not this sim's
   view.step = g->bstep[slot];
   const size_t n = (size_t)g->N * g->p.nvariants * elt(g);
   view.eta[view.cur] = static_cast<char*>(g->eta[g->cur]) + slot * n;
@@ -1524,6 +1598,7 @@ extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void
   if (step < 0) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: step %lld", (long long)step);
   gs_sim s;  // a view: every pointer below is the caller's or the static scratch
   s.p = *p;
+  s.btab_state = -1;  // B formed on the fly: no table to allocate
   GS_TRY(canonicalize(&s));
   const size_t eb = elt(&s);
   const size_t fields = (size_t)s.N * p->nvariants * eb;
@@ -1667,7 +1742,8 @@ extern "C" int gs_adjoint_set_params(gs_adjoint* a, const gs_params* p) {
     return gs_set_error(GS_EINVAL, "adjoint: grid, variant count and dtype are fixed at creation");
   a->s->p = *p;
   a->forward_done = false;
-  return GS_OK;
+  a->s->btab_state = 0;
+  return ensure_btab(a->s, a->s->own_stream);
 }
 
 extern "C" int gs_adjoint_set_loss(gs_adjoint* a, const void* target, int dtype, double lam_el, double e_target) {

@@ -7,6 +7,12 @@ namespace gs {
 template <typename T, int FM, int GM, class Op> cudaError_t launch_x_class(XArgs<T>& a, cudaStream_t s);
 
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s) {
+  if (a.btab) {  // B from the octant table (square contraction, F = G)
+    if (a.F != a.G) return cudaErrorInvalidValue;
+    if (a.F <= 3) return launch_x_class<T, 3, 3, TableOp>(a, s);
+    if (a.F <= 5) return launch_x_class<T, 5, 5, TableOp>(a, s);
+    return launch_x_class<T, 9, 9, TableOp>(a, s);
+  }
   if (a.F <= 3 && a.G <= 3) return launch_x_class<T, 3, 3, ContractOp>(a, s);
   if (a.F <= 5 && a.G <= 5) return launch_x_class<T, 5, 5, ContractOp>(a, s);
   if (a.F <= 8 && a.G <= 6) return launch_x_class<T, 8, 6, ContractOp>(a, s);

@@ -24,6 +24,15 @@ template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_
 template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s);
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s);
+// field-count class (3, 5 or 9) of the B octant table of V variants
+inline int btab_class(int V) { return V <= 3 ? 3 : (V <= 5 ? 5 : 9); }
+inline int btab_stride(int V) {
+  const int c = btab_class(V);
+  return ((c * (c + 1) / 2) + 1) & ~1;
+}
+template <typename T> struct ElasticConst;
+template <typename T>
+cudaError_t launch_btab_fill(const ElasticConst<T>& ec, int n0, int n1, int n2, T* tab, cudaStream_t s);
 template <typename T> cudaError_t launch_zinv(ZinvArgs<T>& a, int H, cudaStream_t s);
 template <typename T> cudaError_t launch_precip_local(PrecipLocalArgs<T>& a, cudaStream_t s);
 template <typename T> cudaError_t launch_defect(const T* eta, T* defect, long long N, int V, cudaStream_t s);

@@ -341,6 +341,10 @@ template <typename T> struct XArgs {
   PrecipUpd<T> pu;
   const T* simscale;  // batched: contraction multiplier of sim blockIdx.z (null: 1)
   int nsim;           // batched simulations (grid z), 0 or 1 for one
+  // octant table of B (TableOp): entry of |folded index| (mx, my, mz) at
+  // btab + ((mx * bt_d1 + my) * bt_d2 + mz) * bt_stride
+  const T* btab;
+  int bt_d1, bt_d2, bt_stride;
 };
 
 // per-point operations of the x pass
@@ -351,6 +355,78 @@ struct ContractOp {
     contract_at<T, FM, GM>(a.ec, nn, ix, iy, iz, in, out, a.simscale ? a.simscale[blockIdx.z] : (T)1);
   }
 };
+// Upper triangle of a symmetric FM x FM matrix, row by row: slot of (i, j), i <= j.
+template <int FM> __host__ __device__ constexpr int tri_slot(int i, int j) {
+  return i <= j ? i * FM - i * (i - 1) / 2 + (j - i) : j * FM - j * (j - 1) / 2 + (i - j);
+}
+template <int FM> struct TriStride {  // entries per table point, rounded to an even count
+  static constexpr int v = ((FM * (FM + 1) / 2) + 1) & ~1;
+};
+
+// B(k) read from the octant table (B even in every axis: see the table fill).
+struct TableOp {
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    static_assert(FM == GM, "square tables only");
+    constexpr int S = TriStride<FM>::v;
+    const int rc = a.ec.refcompat;
+    int mx = fold_idx(ix, nn[0], rc), my = fold_idx(iy, nn[1], rc), mz = fold_idx(iz, nn[2], rc);
+    mx = mx < 0 ? -mx : mx;
+    my = my < 0 ? -my : my;
+    mz = mz < 0 ? -mz : mz;
+    const cplx<T>* b2 = reinterpret_cast<const cplx<T>*>(a.btab + (((long long)mx * a.bt_d1 + my) * a.bt_d2 + mz) * S);
+    T bv[S];
+#pragma unroll
+    for (int i = 0; i < S / 2; ++i) {
+      const cplx<T> w = __ldg(b2 + i);
+      bv[2 * i] = w.x;
+      bv[2 * i + 1] = w.y;
+    }
+    const T mult = a.simscale ? a.simscale[blockIdx.z] : (T)1;
+#pragma unroll
+    for (int g = 0; g < GM; ++g) {
+      cplx<T> acc = mk2((T)0, (T)0);
+#pragma unroll
+      for (int f = 0; f < FM; ++f)
+        if (f < a.F) acc = acc + in[f] * bv[tri_slot<FM>(g, f)];
+      out[g] = acc * mult;
+    }
+  }
+};
+
+// Octant table of the scaled, Nyquist-averaged B(k) of a square contraction
+// (F = G = V, B symmetric): one point per |folded index| triple, filled by
+// contracting unit inputs with contract_at, so that it holds exactly the
+// numbers the on-the-fly contraction forms.  Valid when B is even in each
+// axis separately (checked on the host: no shear coupling of any axis with
+// extent > 1 in the stresses or the modulus), which makes B(+-mx, +-my,
+// +-mz) one value.
+template <typename T, int FM>
+__global__ void k_btab_fill(ElasticConst<T> ec, int n0, int n1, int n2, int d0, int d1, int d2, T* tab) {
+  constexpr int S = TriStride<FM>::v;
+  const long long npt = (long long)d0 * d1 * d2;
+  const int nn[3] = {n0, n1, n2};
+  const int V = ec.nb;
+  for (long long pt = (long long)blockIdx.x * blockDim.x + threadIdx.x; pt < npt;
+       pt += (long long)gridDim.x * blockDim.x) {
+    const int mz = (int)(pt % d2), my = (int)((pt / d2) % d1), mx = (int)(pt / ((long long)d1 * d2));
+    T* o = tab + pt * S;
+#pragma unroll 1
+    for (int i = 0; i < S; ++i) o[i] = (T)0;
+#pragma unroll 1
+    for (int f = 0; f < V; ++f) {
+      cplx<T> in[FM], out[FM];
+#pragma unroll
+      for (int q = 0; q < FM; ++q) in[q] = mk2(q == f ? (T)1 : (T)0, (T)0);
+      contract_at<T, FM, FM>(ec, nn, mx, my, mz, in, out);
+#pragma unroll
+      for (int g = 0; g < FM; ++g)
+        if (g <= f) o[tri_slot<FM>(g, f)] = out[g].x;
+    }
+  }
+}
+
 struct PrecipOp {
   template <typename T, int FM, int GM>
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,

@@ -39,6 +39,12 @@ struct gs_sim {
   int64_t launches = 0;
   int use_graph = 0;
   gs_plain_state* plain = nullptr;
+  // octant table of B(k) of the martensite contraction: state 1 = valid,
+  // 0 = to build, -1 = never (handles that must not allocate), -2 = B is not
+  // even in every axis (the contraction is formed on the fly)
+  void* btab = nullptr;
+  size_t btab_bytes = 0;
+  int btab_state = 0;
   // batched group: nb simulations of one shape with their own coefficients,
   // fields stored sim after sim; per-sim constants live on the device
   int nb = 1;

@@ -167,7 +167,9 @@ int gs_sim_set_scalar(gs_sim* s, const char* name, double value);
 int gs_sim_step(gs_sim* s, int nsteps, void* stream);
 /* Dynamics_*::Get statistics of the current state, FP64. */
 int gs_sim_stats(gs_sim* s, gs_stats* out, void* stream);
-/* Device pointer of a resident field, for callers that keep data on the GPU. */
+/* Device pointer of a resident field, for callers that keep data on the GPU:
+ * "eta", "spectrum", and "btable" (the octant table of B(k) when the
+ * martensite contraction reads one, else NULL and 0 bytes). */
 int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes);
 /* Run one step with a CUDA event between consecutive passes on the step's
  * stream; pass_ms[i] receives the device time of pass i (in launch order:

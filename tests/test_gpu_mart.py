@@ -75,6 +75,46 @@ def test_fp64_variant_counts(gb, orc, V):
     assert rel_l2(gpu_run(gb, p, eta0, 2), orc.mart_run(p, eta0, 2)) < 1e-11
 
 
+def _btable(gb, p):
+    s = gb.Sim(p)
+    try:
+        return s.device_field("btable")
+    finally:
+        s.close()
+
+
+def test_btable_used_when_b_is_even_in_every_axis(gb):
+    p = base3d(gb, (8, 12, 16), F64)
+    ptr, nbytes = _btable(gb, p)
+    assert ptr and nbytes == (8 // 2 + 1) * (12 // 2 + 1) * (16 // 2 + 1) * 6 * 8
+
+
+def _rot_z(C4, deg):
+    t = np.deg2rad(deg)
+    R = np.array([[np.cos(t), -np.sin(t), 0], [np.sin(t), np.cos(t), 0], [0, 0, 1]])
+    return np.einsum("ia,jb,kc,ld,abcd->ijkl", R, R, R, R, C4)
+
+
+@pytest.mark.parametrize("case", ["shear_eigenstrain", "rotated_modulus"])
+@pytest.mark.parametrize("dtype,tol", [(F64, 1e-11), (F32, 2e-6)])
+def test_asymmetric_b_formed_on_the_fly_matches_oracle(gb, orc, case, dtype, tol):
+    """B(k) not even in an axis: no table, the contraction is formed per k."""
+    p = base3d(gb, (8, 12, 16), dtype)
+    if case == "shear_eigenstrain":
+        eps = p.get_eigenstrain()
+        eps[0, 0, 1] = eps[0, 1, 0] = 0.007
+        eps[2, 1, 2] = eps[2, 2, 1] = -0.004
+        p.set_eigenstrain(eps)
+    else:
+        p.set_cijkl(_rot_z(gb.cubic_cijkl(1.4, 0.84, 0.56), 30.0))
+    ptr, nbytes = _btable(gb, p)
+    assert not ptr and nbytes == 0
+    eta0 = gb.initial_eta(p, 21, 0.6)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    assert rel_l2(gpu_run(gb, p, eta0, 2), orc.mart_run(p, eta0, 2)) < tol
+
+
 def test_fp32_one_step(gb, orc):
     p = base3d(gb, (32, 32, 32), F32)
     eta0 = gb.initial_eta(p, 1, 0.01)
