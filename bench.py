@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the launchers' default tile sizes")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the comparator, adjoint and ensemble measurements (1 GPU only)")
     return ap.parse_args()
@@ -270,6 +271,7 @@ def extra_ensemble(steps: int = 100, total_steps: int = 2000) -> dict:
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     with torch.cuda.stream(stream):
+        scheds = b.autotune(reps=3, stream=sh)
         b.step(4, sh)
         ms = _timed(stream, lambda: b.step(steps, sh)) / steps
     groups = b.groups()
@@ -295,7 +297,7 @@ def extra_ensemble(steps: int = 100, total_steps: int = 2000) -> dict:
     sims_s = len(ps) / (ms * total_steps / 1e3)
     return {"workload": "64 sims: 32 x 128^2 + 16 x 256^2 (V=2), 12 x 64^3 + 4 x 128^3 (V=3), FP32, "
                         f"noise 1e-3, {total_steps} steps each",
-            "batched_ms_per_step": ms, "groups": groups, "sims_per_s": sims_s,
+            "batched_ms_per_step": ms, "groups": groups, "group_schedules": scheds, "sims_per_s": sims_s,
             "cell_updates_per_s": cells * 1e3 / ms,
             "sequential_plain_sims_per_s": len(ps) / (seq["plain"] * total_steps / 1e3),
             "sequential_ours_sims_per_s": len(ps) / (seq["ours"] * total_steps / 1e3),
@@ -390,6 +392,8 @@ def run_ours(args, ws, rank, local):
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     with torch.cuda.stream(stream):
+        # tile schedule from the library's autotuner (trial steps leave the state as it was)
+        schedule = sim.autotune(reps=3, stream=sh) if not args.no_tune else sim.schedule()
         sim.step(args.warmup, sh)
         launches_per_step = sim.launch_count() / max(args.warmup, 1)
         torch.cuda.synchronize()
@@ -474,6 +478,7 @@ def run_ours(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(n, args.steps, {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                                                   "tile_schedule": schedule,
                                                    "step_bytes_algorithmic": step_bytes,
                                                    "step_gbs_algorithmic": step_gbs}),
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peaks["hbm_gbs"],

@@ -495,7 +495,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   za.nrows = rows * F;
   za.tw_h = twp<T>(s, 1);
   za.tw_n2 = twp<T>(s, 0);
-  GS_CU(launch_zfwd<T>(za, s->h, st), "z forward pass");
+  GS_CU(launch_zfwd<T>(za, s->h, st, s->sched.z_lines), "z forward pass");
   gs_mark(s, st);
   YArgs<T> ya;
   ya.spec = reinterpret_cast<cplx<T>*>(s->spec);
@@ -503,7 +503,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   ya.n1 = s->n1;
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
-  GS_CU(launch_ypass<T>(ya, s->n1, F, -1, st), "y forward pass");
+  GS_CU(launch_ypass<T>(ya, s->n1, F, -1, st, s->sched.y_cols), "y forward pass");
   if (s->n1 > 1) gs_mark(s, st);
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
@@ -518,11 +518,12 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   xa.tw = twp<T>(s, 3);
   build_elastic<T>(s, which, scale, xa.ec);
   if (which == 0 && s->btab_state == 1) set_btab<T>(s, xa);
+  xa.tz_req = s->sched.x_cols;
   GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
   gs_mark(s, st);
   YArgs<T> yb = ya;
   yb.spec = reinterpret_cast<cplx<T>*>(out_spec);
-  GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st), "y inverse pass");
+  GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st, s->sched.y_cols), "y inverse pass");
   if (s->n1 > 1) gs_mark(s, st);
   s->launches += 2 + (s->n1 > 1 ? 2 : 0);
   return GS_OK;
@@ -557,6 +558,7 @@ template <typename T> static void fill_mart_args(gs_sim* s, MartArgs<T>& ma, con
   ma.fd_n1 = FastDiv((uint32_t)s->n1);
   ma.fd_upr = FastDiv((uint32_t)(s->n2 % 4 == 0 ? s->n2 / 4 : s->n2 / 2));
   ma.fd_v = FastDiv((uint32_t)s->p.nvariants);
+  ma.lr_req = s->sched.update_rows;
 }
 
 template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {
@@ -568,8 +570,10 @@ template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {
   GS_CU(launch_mart_update<T>(ma, s->h, false, st, nullptr), "update pass");
   gs_mark(s, st);
   s->launches += 1;
-  s->cur ^= 1;
-  s->step += 1;
+  if (!s->trial) {  // a trial step wrote only the spare field and the spectra
+    s->cur ^= 1;
+    s->step += 1;
+  }
   return GS_OK;
 }
 
@@ -1266,14 +1270,14 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   za.nrows = rows * VT;
   za.tw_h = twp<T>(g, 1);
   za.tw_n2 = twp<T>(g, 0);
-  GS_CU(launch_zfwd<T>(za, g->h, st), "batch z forward");
+  GS_CU(launch_zfwd<T>(za, g->h, st, g->sched.z_lines), "batch z forward");
   YArgs<T> ya;
   ya.spec = reinterpret_cast<cplx<T>*>(g->spec);
   ya.n0 = g->n0;
   ya.n1 = g->n1;
   ya.h = g->h;
   ya.tw = twp<T>(g, 2);
-  GS_CU(launch_ypass<T>(ya, g->n1, VT, -1, st), "batch y forward");
+  GS_CU(launch_ypass<T>(ya, g->n1, VT, -1, st, g->sched.y_cols), "batch y forward");
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
   xa.in = reinterpret_cast<cplx<T>*>(g->spec);
@@ -1289,12 +1293,14 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   xa.tw = twp<T>(g, 3);
   build_elastic<T>(g, 0, 1.0 / (double)g->N, xa.ec);
   if (g->btab_state == 1) set_btab<T>(g, xa);
+  xa.tz_req = g->sched.x_cols;
   GS_CU(launch_xcontract<T>(xa, st), "batch x pass");
-  GS_CU(launch_ypass<T>(ya, g->n1, VT, 1, st), "batch y inverse");
+  GS_CU(launch_ypass<T>(ya, g->n1, VT, 1, st, g->sched.y_cols), "batch y inverse");
   MartArgs<T> ma;
   fill_mart_args<T>(g, ma, in, out);
   ma.mcs = reinterpret_cast<MartConst<T>*>(g->d_mcs);
   GS_CU(launch_mart_update<T>(ma, g->h, false, st, nullptr, g->nb), "batch update");
+  if (g->trial) return GS_OK;  // the state (fields, counters) is left as it was
   GS_CU(launch_bump_step<T>(reinterpret_cast<MartConst<T>*>(g->d_mcs), g->nb, st), "batch step counter");
   g->launches += 4 + (g->n1 > 1 ? 2 : 0);
   g->cur ^= 1;
@@ -1948,3 +1954,108 @@ extern "C" int gs_adjoint_backward(gs_adjoint* a, const void* seed, int seed_dty
 }
 
 extern "C" int64_t gs_adjoint_launch_count(const gs_adjoint* a) { return a && a->s ? a->s->launches : 0; }
+
+// ---------------------------------------------------------------------------
+// autotuner of the tile schedule
+// ---------------------------------------------------------------------------
+// Coordinate descent over the four tile sizes of the martensite passes (z
+// lines per block, y and x columns per block, update rows per block): each
+// candidate is timed with CUDA events over `reps` trial steps, which write
+// only the spare field of the pair and the spectra, so the simulation's
+// state is untouched.  Candidates a launcher cannot take fall back to its
+// default and time the same.  Two sweeps; the fastest schedule is kept.
+template <class StepFn> static int tune(gs_sim* s, int reps, cudaStream_t st, StepFn trial_step, gs_schedule* out) {
+  cudaEvent_t e0, e1;
+  GS_CU(cudaEventCreate(&e0), "event");
+  GS_CU(cudaEventCreate(&e1), "event");
+  s->trial = true;
+  auto time_sched = [&](const gs_schedule& sc, float* ms) -> int {
+    s->sched = sc;
+    GS_TRY(trial_step());  // warm: attributes, caches
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      GS_CU(cudaEventRecord(e0, st), "record");
+      for (int i = 0; i < reps; ++i) GS_TRY(trial_step());
+      GS_CU(cudaEventRecord(e1, st), "record");
+      GS_CU(cudaEventSynchronize(e1), "sync");
+      float t = 0;
+      GS_CU(cudaEventElapsedTime(&t, e0, e1), "elapsed");
+      if (t < best) best = t;
+    }
+    *ms = best;
+    return GS_OK;
+  };
+  gs_schedule best = s->sched;
+  float best_ms = 0;
+  int rc = time_sched(best, &best_ms);
+  const int cand[] = {1, 2, 4, 8, 16, 32, 64};
+  for (int sweep = 0; sweep < 2 && rc == GS_OK; ++sweep) {
+    for (int knob = 0; knob < 4 && rc == GS_OK; ++knob) {
+      for (int c : cand) {
+        gs_schedule sc = best;
+        int* f = knob == 0 ? &sc.z_lines : knob == 1 ? &sc.y_cols : knob == 2 ? &sc.x_cols : &sc.update_rows;
+        if (*f == c) continue;
+        *f = c;
+        float ms = 0;
+        if ((rc = time_sched(sc, &ms)) != GS_OK) break;
+        if (ms < 0.98f * best_ms) {
+          best = sc;
+          best_ms = ms;
+        }
+      }
+    }
+  }
+  s->trial = false;
+  s->sched = best;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != GS_OK) return rc;
+  if (out) *out = best;
+  return GS_OK;
+}
+
+extern "C" int gs_sim_set_schedule(gs_sim* s, const gs_schedule* sc) {
+  if (!s || !sc) return gs_set_error(GS_EINVAL, "gs_sim_set_schedule: null argument");
+  if (sc->z_lines < 0 || sc->y_cols < 0 || sc->x_cols < 0 || sc->update_rows < 0)
+    return gs_set_error(GS_EINVAL, "gs_sim_set_schedule: negative tile size");
+  s->sched = *sc;
+  return GS_OK;
+}
+
+extern "C" int gs_sim_get_schedule(const gs_sim* s, gs_schedule* sc) {
+  if (!s || !sc) return gs_set_error(GS_EINVAL, "gs_sim_get_schedule: null argument");
+  *sc = s->sched;
+  return GS_OK;
+}
+
+extern "C" int gs_sim_autotune(gs_sim* s, int reps, void* stream, gs_schedule* chosen) {
+  if (!s) return gs_set_error(GS_EINVAL, "gs_sim_autotune: null sim");
+  if (s->p.model != GS_MODEL_MART || s->plain) return gs_set_error(GS_ENOTSUP, "gs_sim_autotune: martensite only");
+  if (reps < 1) reps = 1;
+  cudaStream_t st = pick_stream(s, stream);
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  return tune(s, reps, st, [&]() { return f64 ? mart_step<double>(s, st) : mart_step<float>(s, st); }, chosen);
+}
+
+extern "C" int gs_batch_autotune(gs_batch* b, int reps, void* stream) {
+  if (!b) return gs_set_error(GS_EINVAL, "gs_batch_autotune: null batch");
+  if (reps < 1) reps = 1;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  if (b->exec) {  // a captured step holds the old tile sizes
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  for (gs_sim* g : b->groups) {
+    const bool f64 = g->p.dtype == GS_DTYPE_F64;
+    GS_TRY(tune(g, reps, st,
+                [&]() { return f64 ? batch_group_step<double>(g, st) : batch_group_step<float>(g, st); }, nullptr));
+  }
+  return GS_OK;
+}
+
+extern "C" int gs_batch_get_schedule(const gs_batch* b, int group, gs_schedule* sc) {
+  if (!b || !sc || group < 0 || group >= (int)b->groups.size())
+    return gs_set_error(GS_EINVAL, "gs_batch_get_schedule: bad arguments");
+  *sc = b->groups[group]->sched;
+  return GS_OK;
+}

@@ -11,6 +11,8 @@ template <typename T, int H, int VM, bool ST, bool BA> cudaError_t mu_n(MartArgs
   using L = Line<T, H>;
   const int per = L::P * a.mc.V;
   long long lr = 256 / per;
+  // the kernel's launch bounds allow 256 threads
+  if (a.lr_req > 0 && (long long)a.lr_req * per <= 256) lr = a.lr_req;
   if (lr < 1) lr = 1;
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;

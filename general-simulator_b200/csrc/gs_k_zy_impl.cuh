@@ -7,9 +7,14 @@
 namespace gs {
 
 
-template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStream_t s) {
+template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStream_t s, int lines_req) {
   using L = Line<T, H>;
   long long lpc = 256 / L::P;
+  // a requested line count (autotuner) when the block stays within 1024
+  // threads and the shared-memory opt-in
+  if (lines_req > 0 && (long long)lines_req * L::P <= max_block_threads<k_zfwd<T, H>>() &&
+      (size_t)lines_req * L::PAD * sizeof(cplx<T>) <= 200 * 1024)
+    lpc = lines_req;
   if (lpc < 1) lpc = 1;
   if (lpc > a.nrows) lpc = a.nrows;
   a.lpc = (int)lpc;
@@ -20,11 +25,11 @@ template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStrea
   return cudaGetLastError();
 }
 
-template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s) {
+template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s, int lines_req) {
   switch (H) {
 #define GS_C(N_) \
   case N_:       \
-    return zfwd_n<T, N_>(a, s);
+    return zfwd_n<T, N_>(a, s, lines_req);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:
@@ -32,8 +37,14 @@ template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_
   }
 }
 
-template <typename T, int N1, int DIR> static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s) {
+template <typename T, int N1, int DIR> static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s, int cols_req) {
   using L = Line<T, N1>;
+  // a requested column count (autotuner): a power of two dividing h that the
+  // kernel can launch with and whose tile fits the shared-memory opt-in
+  if (cols_req > 0 && (cols_req & (cols_req - 1)) == 0 && a.h % cols_req == 0 &&
+      (long long)cols_req * L::P <= max_block_threads<k_ypass<T, N1, DIR>>() &&
+      (size_t)cols_req * L::PAD * sizeof(cplx<T>) <= 200 * 1024)
+    a.tz = cols_req;
   const size_t smem = (size_t)a.tz * L::PAD * sizeof(cplx<T>);
   allow_max_smem<k_ypass<T, N1, DIR>>();
   dim3 grid(a.h / a.tz, a.n0, F);
@@ -41,13 +52,13 @@ template <typename T, int N1, int DIR> static cudaError_t ypass_n(YArgs<T>& a, i
   return cudaGetLastError();
 }
 
-template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s) {
+template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req) {
   if (n1 == 1) return cudaSuccess;
   a.tz = pick_tz(a.h);
   switch (n1) {
 #define GS_C(N_) \
   case N_:       \
-    return dir < 0 ? ypass_n<T, N_, -1>(a, F, s) : ypass_n<T, N_, 1>(a, F, s);
+    return dir < 0 ? ypass_n<T, N_, -1>(a, F, s, cols_req) : ypass_n<T, N_, 1>(a, F, s, cols_req);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:

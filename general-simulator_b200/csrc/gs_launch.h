@@ -20,8 +20,10 @@ bool size_supported(int n);
 // columns per block of the y and x passes
 int pick_tz(int h);
 
-template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s);
-template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s);
+// lines_req / cols_req: tile sizes asked by the autotuner (0 = the default
+// choice; values the launch cannot take fall back to it)
+template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s, int lines_req = 0);
+template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req = 0);
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s);
 // field-count class (3, 5 or 9) of the B octant table of V variants
@@ -55,6 +57,21 @@ template <auto Kernel> inline void allow_max_smem() {
   }
 }
 cudaError_t launch_reduce(const double* partials, int nb, int n, double* out, cudaStream_t s);
+
+// the largest block a kernel can be launched with (its register use), once
+template <auto Kernel> inline int max_block_threads() {
+  static int v = 0;
+  if (!v) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, Kernel) == cudaSuccess) {
+      v = fa.maxThreadsPerBlock;
+    } else {
+      cudaGetLastError();
+      v = 256;
+    }
+  }
+  return v;
+}
 
 #define GS_SIZE_CASES(M) \
   M(1) M(2) M(4) M(6) M(8) M(12) M(16) M(24) M(32) M(48) M(64) M(96) M(128) M(256)

@@ -52,6 +52,7 @@ template <typename T> struct MartArgs {
   FastDiv fd_n1, fd_upr, fd_v;  // y extent, update runs per row, variants
   MartConst<T>* mcs;  // batched: constants of sim blockIdx.y in device memory
   T* r_out;           // when set: R_p written out [V][N] (adjoint checkpoints)
+  int lr_req;         // rows per block asked by the autotuner (0 = default)
 };
 
 // advance the step counter of every batched simulation (keeps a captured

@@ -345,6 +345,7 @@ template <typename T> struct XArgs {
   // btab + ((mx * bt_d1 + my) * bt_d2 + mz) * bt_stride
   const T* btab;
   int bt_d1, bt_d2, bt_stride;
+  int tz_req;  // column tile asked by the autotuner (0 = default)
 };
 
 // per-point operations of the x pass

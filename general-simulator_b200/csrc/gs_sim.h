@@ -42,6 +42,10 @@ struct gs_sim {
   // octant table of B(k) of the martensite contraction: state 1 = valid,
   // 0 = to build, -1 = never (handles that must not allocate), -2 = B is not
   // even in every axis (the contraction is formed on the fly)
+  // tile schedule of the passes (0 = each launcher's default); set by the
+  // autotuner or the caller
+  gs_schedule sched = {0, 0, 0, 0};
+  bool trial = false;  // steps that leave the state as it was (autotuner timing)
   void* btab = nullptr;
   size_t btab_bytes = 0;
   int btab_state = 0;

@@ -28,6 +28,13 @@ GS_DTYPE_F32, GS_DTYPE_F64 = 0, 1
 GS_MAX_V = 8
 
 
+class GsSchedule(C.Structure):
+    _fields_ = [("z_lines", C.c_int), ("y_cols", C.c_int), ("x_cols", C.c_int), ("update_rows", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GsParams(C.Structure):
     _fields_ = [
         ("model", C.c_int), ("mode", C.c_int), ("dtype", C.c_int), ("nvariants", C.c_int),
@@ -157,6 +164,11 @@ def lib() -> C.CDLL:
                                           C.POINTER(C.c_double), vp, C.c_int, vp]),
         "gs_adjoint_device_bytes": (C.c_size_t, [vp]),
         "gs_adjoint_launch_count": (C.c_int64, [vp]),
+        "gs_sim_set_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
+        "gs_sim_get_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
+        "gs_sim_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(GsSchedule)]),
+        "gs_batch_autotune": (C.c_int, [vp, C.c_int, vp]),
+        "gs_batch_get_schedule": (C.c_int, [vp, C.c_int, C.POINTER(GsSchedule)]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
         "gs_mart_step_noalloc_max_bytes": (C.c_size_t, []),
     }
@@ -332,6 +344,20 @@ class Sim:
     def launch_count(self) -> int:
         return int(lib().gs_sim_launch_count(self.h))
 
+    def autotune(self, reps: int = 5, stream: int = 0) -> dict:
+        sc = GsSchedule()
+        check(lib().gs_sim_autotune(self.h, reps, C.c_void_p(stream), C.byref(sc)), "gs_sim_autotune")
+        return sc.as_dict()
+
+    def schedule(self) -> dict:
+        sc = GsSchedule()
+        check(lib().gs_sim_get_schedule(self.h, C.byref(sc)), "gs_sim_get_schedule")
+        return sc.as_dict()
+
+    def set_schedule(self, **kw) -> None:
+        sc = GsSchedule(**{k: int(kw.get(k, 0)) for k, _ in GsSchedule._fields_})
+        check(lib().gs_sim_set_schedule(self.h, C.byref(sc)), "gs_sim_set_schedule")
+
     def use_graph(self, on: bool) -> None:
         check(lib().gs_sim_use_graph(self.h, 1 if on else 0), "use_graph")
 
@@ -386,6 +412,15 @@ class Batch:
 
     def groups(self) -> int:
         return int(lib().gs_batch_groups(self.h))
+
+    def autotune(self, reps: int = 5, stream: int = 0) -> list:
+        check(lib().gs_batch_autotune(self.h, reps, C.c_void_p(stream)), "gs_batch_autotune")
+        out = []
+        for g in range(self.groups()):
+            sc = GsSchedule()
+            check(lib().gs_batch_get_schedule(self.h, g, C.byref(sc)), "gs_batch_get_schedule")
+            out.append(sc.as_dict())
+        return out
 
     def launch_count(self) -> int:
         return int(lib().gs_batch_launch_count(self.h))

@@ -182,6 +182,21 @@ int64_t gs_sim_launch_count(const gs_sim* s);
  * the passes directly (0, default). */
 int gs_sim_use_graph(gs_sim* s, int on);
 
+/* ---- tile schedule and autotuner ---------------------------------------- */
+/* Tile sizes of the martensite passes: z lines per block, y and x columns
+ * per block, update rows per block (0 = the launcher's default; sizes a
+ * launch cannot take fall back to it).  The reference has no counterpart
+ * (cuFFT plans internally).  gs_sim_autotune times candidates with CUDA
+ * events over `reps` trial steps that leave the simulation's state as it was
+ * (coordinate descent, two sweeps) and keeps the fastest; gs_batch_autotune
+ * does so per group and drops a captured graph so the next step recaptures. */
+typedef struct gs_schedule {
+  int z_lines, y_cols, x_cols, update_rows;
+} gs_schedule;
+int gs_sim_set_schedule(gs_sim* s, const gs_schedule* sc);
+int gs_sim_get_schedule(const gs_sim* s, gs_schedule* sc);
+int gs_sim_autotune(gs_sim* s, int reps, void* stream, gs_schedule* chosen);
+
 /* ---- a martensite step that allocates nothing -------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory when they step: a host whose pool allocator owns all of the GPU's
@@ -248,6 +263,8 @@ int gs_batch_step(gs_batch* b, int nsteps, void* stream);
 int gs_batch_stats(gs_batch* b, int sim, gs_stats* out, void* stream);
 int gs_batch_use_graph(gs_batch* b, int on);
 int gs_batch_groups(const gs_batch* b);
+int gs_batch_autotune(gs_batch* b, int reps, void* stream);
+int gs_batch_get_schedule(const gs_batch* b, int group, gs_schedule* sc);
 int64_t gs_batch_launch_count(const gs_batch* b);
 
 /* ---- comparator: the same step with cuFFT C2C and unfused sweeps ------ */

@@ -82,3 +82,30 @@ def test_ensemble_builder_shapes(gb):
     b.step(2)
     assert np.isfinite(b.eta(63)).all()
     b.close()
+
+
+def test_sharded_ensemble_equals_single_runs(gb):
+    """Two ranks' shares, run one after the other on this GPU without a
+    process group, give the same statistics as each simulation alone."""
+    import gs_dist
+
+    ps = gb.ensemble_params(gb.GS_DTYPE_F64, counts=(3, 1, 2, 0))
+    for p in ps:
+        p.nx, p.ny = min(p.nx, 32), min(p.ny, 32)
+        if p.nz > 1:
+            p.nz = 16
+    eta0 = [gb.initial_eta(p, 40 + i, 0.3) for i, p in enumerate(ps)]
+    got = {}
+    for rank in range(2):
+        got.update(gs_dist.run_ensemble_shard(ps, eta0, rank, 2, 3, use_graph=False, gather=False))
+    assert sorted(got) == list(range(len(ps)))
+    for i, p in enumerate(ps):
+        s = gb.Sim(p)
+        try:
+            s.set_field("eta", eta0[i])
+            s.step(3)
+            ref = s.stats()
+        finally:
+            s.close()
+        for k in ("mass", "e_el", "e_tot"):
+            assert abs(got[i][k] - ref[k]) <= 1e-10 * abs(ref[k]) + 1e-14, (i, k)
