@@ -404,6 +404,7 @@ template <typename T> static int build_twiddles(gs_sim* s) {
     }
   GS_CU(cudaMalloc(&s->tw, total * sizeof(cplx<T>)), "cudaMalloc twiddles");
   GS_CU(cudaMemcpy(s->tw, host.data(), total * sizeof(cplx<T>), cudaMemcpyHostToDevice), "upload twiddles");
+  GS_CU(cudaDeviceSynchronize(), "upload twiddles sync");
   return GS_OK;
 }
 
@@ -641,6 +642,7 @@ template <typename T> static void fill_ktab(gs_sim* s) {
     }
   }
   cudaMemcpy(s->ktab, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
+  cudaDeviceSynchronize();  // the copy above may return before its DMA lands
 }
 
 template <typename T> static int precip_potential(gs_sim* s, cudaStream_t st) {
@@ -857,7 +859,8 @@ static size_t elt(const gs_sim* s) { return s->p.dtype == GS_DTYPE_F64 ? 8 : 4; 
 static void free_sim(gs_sim* s) {
   if (!s) return;
   void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->rbuf, s->mubuf,
-                  s->stressbuf, s->ktab, s->tw, s->partials, s->red, s->btab};
+                  s->stressbuf, s->ktab, s->tw, s->partials, s->red, s->btab, s->d_mcs, s->d_simscale};
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -1006,8 +1009,17 @@ static int download(gs_sim* s, const void* src, void* host, size_t count, int dt
   return GS_OK;
 }
 
+// drop a captured step (its launches hold pointers and tile sizes)
+static void sim_graph_reset(gs_sim* s) {
+  if (s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
+}
+
 extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, size_t count, int dtype) {
   if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_set_field: null argument");
+  sim_graph_reset(s);
   if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
   const int V = s->p.nvariants;
   const size_t N = (size_t)s->N;
@@ -1112,12 +1124,65 @@ static cudaStream_t pick_stream(gs_sim* s, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : s->own_stream;
 }
 
+template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st);
+template <typename T> static int batch_upload_consts(gs_sim* g);
+
+// gs_sim_use_graph: the martensite step as a one-simulation group whose
+// constants (noise step counter included) live in device memory, so that a
+// captured graph of two steps (the field pair swaps back) replays exactly.
+template <typename T> static int sim_graph_steps(gs_sim* s, int nsteps, cudaStream_t st) {
+  if (!s->d_mcs) {
+    GS_CU(cudaMalloc(&s->d_mcs, sizeof(MartConst<T>)), "cudaMalloc step constants");
+    GS_CU(cudaMalloc(&s->d_simscale, sizeof(T)), "cudaMalloc step scale");
+  }
+  s->nb = 1;
+  s->bp.assign(1, s->p);
+  s->bstep.assign(1, s->step);
+  // steps queued by an earlier call still read the constants: let them finish
+  GS_CU(cudaStreamSynchronize(st), "sync before constants");
+  GS_TRY(batch_upload_consts<T>(s));  // current temperature and step counter
+  int done = 0;
+  if (!s->gexec || s->gexec_stream != st || s->gexec_cur != s->cur) {
+    sim_graph_reset(s);
+    // direct steps first (kernel attributes are set outside any capture)
+    GS_TRY(batch_group_step<T>(s, st));
+    GS_TRY(batch_group_step<T>(s, st));
+    done = 2;
+    const int cur = s->cur;
+    const int64_t step = s->step;
+    const std::vector<int64_t> bstep = s->bstep;
+    cudaGraph_t graph;
+    GS_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int rc = batch_group_step<T>(s, st);
+    if (rc == GS_OK) rc = batch_group_step<T>(s, st);
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    s->cur = cur;  // the capture ran nothing
+    s->step = step;
+    s->bstep = bstep;
+    if (rc != GS_OK) return rc;
+    GS_CU(e, "end capture");
+    GS_CU(cudaGraphInstantiate(&s->gexec, graph, 0), "instantiate graph");
+    cudaGraphDestroy(graph);
+    s->gexec_stream = st;
+    s->gexec_cur = cur;
+  }
+  for (; done + 2 <= nsteps; done += 2) {
+    GS_CU(cudaGraphLaunch(s->gexec, st), "graph launch");
+    s->step += 2;
+    s->bstep[0] += 2;
+  }
+  for (; done < nsteps; ++done) GS_TRY(batch_group_step<T>(s, st));
+  return GS_OK;
+}
+
 extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
   if (!s) return gs_set_error(GS_EINVAL, "gs_sim_step: null sim");
   if (nsteps < 0) return gs_set_error(GS_EINVAL, "nsteps %d", nsteps);
   cudaStream_t st = pick_stream(s, stream);
   s->launches = 0;
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  if (s->use_graph && s->p.model == GS_MODEL_MART && !s->plain && nsteps >= 2)
+    return f64 ? sim_graph_steps<double>(s, nsteps, st) : sim_graph_steps<float>(s, nsteps, st);
   for (int i = 0; i < nsteps; ++i) {
     int rc;
     if (s->p.model == GS_MODEL_MART)
@@ -1171,6 +1236,7 @@ extern "C" int64_t gs_sim_launch_count(const gs_sim* s) { return s ? s->launches
 extern "C" int gs_sim_use_graph(gs_sim* s, int on) {
   if (!s) return gs_set_error(GS_EINVAL, "null sim");
   s->use_graph = on;
+  if (!on) sim_graph_reset(s);
   return GS_OK;
 }
 
@@ -1252,6 +1318,9 @@ template <typename T> static int batch_upload_consts(gs_sim* g) {
   }
   GS_CU(cudaMemcpy(g->d_mcs, mcs.data(), sizeof(MartConst<T>) * g->nb, cudaMemcpyHostToDevice), "upload constants");
   GS_CU(cudaMemcpy(g->d_simscale, sc.data(), sizeof(T) * g->nb, cudaMemcpyHostToDevice), "upload scales");
+  // a pageable copy may return before its DMA lands, and the steps run on
+  // non-blocking streams: wait for it
+  GS_CU(cudaDeviceSynchronize(), "upload constants sync");
   return GS_OK;
 }
 
@@ -1386,9 +1455,7 @@ extern "C" int gs_batch_destroy(gs_batch* b) {
   cudaDeviceSynchronize();
   if (b->exec) cudaGraphExecDestroy(b->exec);
   for (gs_sim* g : b->groups) {
-    if (g->d_mcs) cudaFree(g->d_mcs);
-    if (g->d_simscale) cudaFree(g->d_simscale);
-    free_sim(g);
+    free_sim(g);  // frees the per-sim constants too
   }
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -2016,6 +2083,7 @@ template <class StepFn> static int tune(gs_sim* s, int reps, cudaStream_t st, St
 
 extern "C" int gs_sim_set_schedule(gs_sim* s, const gs_schedule* sc) {
   if (!s || !sc) return gs_set_error(GS_EINVAL, "gs_sim_set_schedule: null argument");
+  sim_graph_reset(s);
   if (sc->z_lines < 0 || sc->y_cols < 0 || sc->x_cols < 0 || sc->update_rows < 0)
     return gs_set_error(GS_EINVAL, "gs_sim_set_schedule: negative tile size");
   s->sched = *sc;
@@ -2032,6 +2100,7 @@ extern "C" int gs_sim_autotune(gs_sim* s, int reps, void* stream, gs_schedule* c
   if (!s) return gs_set_error(GS_EINVAL, "gs_sim_autotune: null sim");
   if (s->p.model != GS_MODEL_MART || s->plain) return gs_set_error(GS_ENOTSUP, "gs_sim_autotune: martensite only");
   if (reps < 1) reps = 1;
+  sim_graph_reset(s);
   cudaStream_t st = pick_stream(s, stream);
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
   return tune(s, reps, st, [&]() { return f64 ? mart_step<double>(s, st) : mart_step<float>(s, st); }, chosen);

@@ -56,6 +56,10 @@ struct gs_sim {
   std::vector<int64_t> bstep;
   void* d_mcs = nullptr;
   void* d_simscale = nullptr;
+  // gs_sim_use_graph: a captured graph of two steps of a one-simulation group
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gexec_stream = nullptr;
+  int gexec_cur = 0;
   // per-pass event marks of gs_sim_profile_step
   static constexpr int kMaxMarks = 32;
   cudaEvent_t marks[kMaxMarks] = {};

@@ -178,8 +178,11 @@ int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes)
 int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int max_pass, int* npass);
 /* Number of kernel launches issued by the last gs_sim_step call. */
 int64_t gs_sim_launch_count(const gs_sim* s);
-/* Make gs_sim_step replay a captured CUDA graph of one step (1) or launch
- * the passes directly (0, default). */
+/* Make gs_sim_step replay a captured CUDA graph of two steps (1) or launch
+ * the passes directly (0, default).  Martensite only; the step constants
+ * (noise counter, temperature) then live in device memory and are refreshed
+ * at every gs_sim_step call, so results equal the direct launches bit for
+ * bit.  Setting a field, a schedule or autotuning drops the captured graph. */
 int gs_sim_use_graph(gs_sim* s, int on);
 
 /* ---- tile schedule and autotuner ---------------------------------------- */

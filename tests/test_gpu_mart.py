@@ -258,3 +258,36 @@ def test_step_counter_continues_noise_stream(gb, orc):
     got = s.eta()
     s.close()
     assert rel_l2(got, ref) < 1e-11
+
+
+@pytest.mark.parametrize("dtype", [F64, F32])
+def test_graph_replay_equals_direct_steps(gb, dtype):
+    """gs_sim_use_graph: replayed two-step graphs, odd step counts, a
+    temperature change between calls (refcompat) and a field upload in the
+    middle give the same bits as direct launches."""
+    p = refcompat_params(gb, (16, 24, 32), dtype)
+    p.noise_amp = 1e-2
+    eta0 = gb.initial_eta(p, 31, 0.01)
+    eta1 = gb.initial_eta(p, 32, 0.01)
+
+    def run(graph):
+        s = gb.Sim(p)
+        try:
+            s.use_graph(graph)
+            s.set_field("eta", eta0)
+            s.step(5)
+            s.set_scalar("temperature", 420.0)
+            s.step(4)
+            a = s.eta(np.float64)
+            s.set_field("eta", eta1)
+            s.step(3)
+            st = s.stats()
+            return a, s.eta(np.float64), st
+        finally:
+            s.close()
+
+    a0, b0, s0 = run(False)
+    a1, b1, s1 = run(True)
+    assert np.all(np.isfinite(a0)) and np.all(np.isfinite(b0))
+    assert np.array_equal(a0, a1) and np.array_equal(b0, b1)
+    assert s0["e_el"] == s1["e_el"] and s0["mass"] == s1["mass"]
