@@ -482,8 +482,10 @@ template <typename T> static void set_btab(const gs_sim* s, XArgs<T>& xa) {
 // (B contraction, F inputs -> G outputs, into out_spec) -> y inverse.
 template <typename T>
 static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, int F, int which, double scale,
-                           void* out_spec, int G, cudaStream_t st, const T* const* mul = nullptr) {
+                           void* out_spec, int G, cudaStream_t st, const T* const* mul = nullptr,
+                           bool z_ready = false) {
   const long long rows = (long long)s->n0 * s->n1;
+  s->spec_ready = false;  // the chain transforms the spectrum buffer in place
   ZfwdArgs<T> za;
   memset(&za, 0, sizeof(za));
   for (int f = 0; f < F; ++f) {
@@ -496,8 +498,11 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   za.nrows = rows * F;
   za.tw_h = twp<T>(s, 1);
   za.tw_n2 = twp<T>(s, 0);
-  GS_CU(launch_zfwd<T>(za, s->h, st, s->sched.z_lines), "z forward pass");
-  gs_mark(s, st);
+  if (!z_ready) {  // else the previous update left the z spectra of src^2 in place
+    GS_CU(launch_zfwd<T>(za, s->h, st, s->sched.z_lines), "z forward pass");
+    gs_mark(s, st);
+    s->launches += 1;
+  }
   YArgs<T> ya;
   ya.spec = reinterpret_cast<cplx<T>*>(s->spec);
   ya.n0 = s->n0;
@@ -526,11 +531,11 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   yb.spec = reinterpret_cast<cplx<T>*>(out_spec);
   GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st, s->sched.y_cols), "y inverse pass");
   if (s->n1 > 1) gs_mark(s, st);
-  s->launches += 2 + (s->n1 > 1 ? 2 : 0);
+  s->launches += 1 + (s->n1 > 1 ? 2 : 0);
   return GS_OK;
 }
 
-template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st) {
+template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st, bool z_ready = false) {
   const int V = s->p.nvariants;
   const T* src[GS_MAXF];
   int sq[GS_MAXF];
@@ -538,7 +543,7 @@ template <typename T> int elastic_chain(gs_sim* s, const T* eta, cudaStream_t st
     src[f] = eta + (long long)f * s->N;
     sq[f] = 1;
   }
-  return elastic_chain_g<T>(s, src, sq, V, 0, 1.0 / (double)s->N, s->spec, V, st);
+  return elastic_chain_g<T>(s, src, sq, V, 0, 1.0 / (double)s->N, s->spec, V, st, nullptr, z_ready);
 }
 
 template <typename T> static void fill_mart_args(gs_sim* s, MartArgs<T>& ma, const T* in, T* out) {
@@ -565,15 +570,21 @@ template <typename T> static void fill_mart_args(gs_sim* s, MartArgs<T>& ma, con
 template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {
   T* in = reinterpret_cast<T*>(s->eta[s->cur]);
   T* out = reinterpret_cast<T*>(s->eta[s->cur ^ 1]);
-  GS_TRY(elastic_chain<T>(s, in, st));
+  const bool z_ready = s->spec_ready && s->spec_cur == s->cur;
+  GS_TRY(elastic_chain<T>(s, in, st, z_ready));
   MartArgs<T> ma;
   fill_mart_args<T>(s, ma, in, out);
+  if (s->fuse) ma.spec_next = reinterpret_cast<cplx<T>*>(s->spec);
   GS_CU(launch_mart_update<T>(ma, s->h, false, st, nullptr), "update pass");
   gs_mark(s, st);
   s->launches += 1;
   if (!s->trial) {  // a trial step wrote only the spare field and the spectra
     s->cur ^= 1;
     s->step += 1;
+  }
+  if (s->fuse) {  // the spectra of the field just written (trial steps: timing only)
+    s->spec_ready = true;
+    s->spec_cur = s->cur;
   }
   return GS_OK;
 }
@@ -1020,6 +1031,7 @@ static void sim_graph_reset(gs_sim* s) {
 extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, size_t count, int dtype) {
   if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_set_field: null argument");
   sim_graph_reset(s);
+  s->spec_ready = false;
   if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
   const int V = s->p.nvariants;
   const size_t N = (size_t)s->N;
@@ -1142,7 +1154,8 @@ template <typename T> static int sim_graph_steps(gs_sim* s, int nsteps, cudaStre
   GS_CU(cudaStreamSynchronize(st), "sync before constants");
   GS_TRY(batch_upload_consts<T>(s));  // current temperature and step counter
   int done = 0;
-  if (!s->gexec || s->gexec_stream != st || s->gexec_cur != s->cur) {
+  const bool ready = !s->fuse || (s->spec_ready && s->spec_cur == s->cur);
+  if (!s->gexec || s->gexec_stream != st || s->gexec_cur != s->cur || !ready) {
     sim_graph_reset(s);
     // direct steps first (kernel attributes are set outside any capture)
     GS_TRY(batch_group_step<T>(s, st));
@@ -1339,7 +1352,12 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   za.nrows = rows * VT;
   za.tw_h = twp<T>(g, 1);
   za.tw_n2 = twp<T>(g, 0);
-  GS_CU(launch_zfwd<T>(za, g->h, st, g->sched.z_lines), "batch z forward");
+  const bool z_ready = g->spec_ready && g->spec_cur == g->cur;
+  g->spec_ready = false;
+  if (!z_ready) {
+    GS_CU(launch_zfwd<T>(za, g->h, st, g->sched.z_lines), "batch z forward");
+    g->launches += 1;
+  }
   YArgs<T> ya;
   ya.spec = reinterpret_cast<cplx<T>*>(g->spec);
   ya.n0 = g->n0;
@@ -1368,13 +1386,20 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   MartArgs<T> ma;
   fill_mart_args<T>(g, ma, in, out);
   ma.mcs = reinterpret_cast<MartConst<T>*>(g->d_mcs);
+  if (g->fuse) ma.spec_next = reinterpret_cast<cplx<T>*>(g->spec);
   GS_CU(launch_mart_update<T>(ma, g->h, false, st, nullptr, g->nb), "batch update");
-  if (g->trial) return GS_OK;  // the state (fields, counters) is left as it was
+  if (g->trial) {  // the state (fields, counters) is left as it was
+    g->spec_ready = g->fuse;
+    g->spec_cur = g->cur;
+    return GS_OK;
+  }
   GS_CU(launch_bump_step<T>(reinterpret_cast<MartConst<T>*>(g->d_mcs), g->nb, st), "batch step counter");
-  g->launches += 4 + (g->n1 > 1 ? 2 : 0);
+  g->launches += 3 + (g->n1 > 1 ? 2 : 0);
   g->cur ^= 1;
   g->step += 1;
   for (auto& k : g->bstep) k += 1;
+  g->spec_ready = g->fuse;
+  g->spec_cur = g->cur;
   return GS_OK;
 }
 
@@ -1487,6 +1512,11 @@ extern "C" int gs_batch_set_field(gs_batch* b, int sim, const char* name, const 
   if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
   GS_CU(cudaStreamSynchronize(b->stream), "sync");
   char* dst = static_cast<char*>(g->eta[g->cur]) + (size_t)slot * n * elt(g);
+  g->spec_ready = false;  // the fused spectra no longer match the field
+  if (b->exec) {          // a captured step starts from fused spectra
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
   return upload(g, dst, host, count, dtype);
 }
 
@@ -1510,7 +1540,9 @@ extern "C" int gs_batch_step(gs_batch* b, int nsteps, void* stream) {
   if (b->use_graph && nsteps >= 2) {
     // the first steps run directly (kernel attributes are set outside any
     // capture); then a graph of two steps (the field pair swaps back) replays
-    if (!b->exec || b->exec_stream != st) {
+    bool ready = true;  // the captured steps start from fused spectra
+    for (gs_sim* g : b->groups) ready = ready && (!g->fuse || (g->spec_ready && g->spec_cur == g->cur));
+    if (!b->exec || b->exec_stream != st || !ready) {
       if (b->exec) {
         cudaGraphExecDestroy(b->exec);
         b->exec = nullptr;
@@ -1672,6 +1704,7 @@ extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void
   gs_sim s;  // a view: every pointer below is the caller's or the static scratch
   s.p = *p;
   s.btab_state = -1;  // B formed on the fly: no table to allocate
+  s.fuse = false;      // nothing carries the spectrum to a next call
   GS_TRY(canonicalize(&s));
   const size_t eb = elt(&s);
   const size_t fields = (size_t)s.N * p->nvariants * eb;
@@ -2073,6 +2106,7 @@ template <class StepFn> static int tune(gs_sim* s, int reps, cudaStream_t st, St
     }
   }
   s->trial = false;
+  s->spec_ready = false;  // the trial steps left other spectra behind
   s->sched = best;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -6,8 +6,8 @@
 
 namespace gs {
 
-template <typename T, int H, int VM, bool ST, bool BA> cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks,
-                                                                       int nsim) {
+template <typename T, int H, int VM, bool ST, bool BA, bool FU = false>
+cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks, int nsim) {
   using L = Line<T, H>;
   const int per = L::P * a.mc.V;
   long long lr = 256 / per;
@@ -17,21 +17,26 @@ template <typename T, int H, int VM, bool ST, bool BA> cudaError_t mu_n(MartArgs
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;
   const size_t smem = (size_t)lr * a.mc.V * L::PAD * sizeof(cplx<T>);
-  allow_max_smem<k_mart_update<T, H, VM, ST, BA>>();
+  allow_max_smem<k_mart_update<T, H, VM, ST, BA, FU>>();
   const long long grid = (a.nrows + lr - 1) / lr;
   if (nblocks) *nblocks = (int)grid;
-  k_mart_update<T, H, VM, ST, BA><<<dim3((unsigned)grid, (unsigned)nsim), (unsigned)(per * lr), smem, s>>>(a);
+  k_mart_update<T, H, VM, ST, BA, FU><<<dim3((unsigned)grid, (unsigned)nsim), (unsigned)(per * lr), smem, s>>>(a);
   return cudaGetLastError();
 }
 
 template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaStream_t s, int* nb, int nsim) {
+  const bool fu = a.spec_next != nullptr && !stats;
   if (nsim > 0) {  // batched simulations (device-resident constants)
-    if (a.mc.V <= 4) return mu_n<T, H, 4, false, true>(a, s, nb, nsim);
-    return mu_n<T, H, 8, false, true>(a, s, nb, nsim);
+    if (a.mc.V <= 4)
+      return fu ? mu_n<T, H, 4, false, true, true>(a, s, nb, nsim) : mu_n<T, H, 4, false, true>(a, s, nb, nsim);
+    return fu ? mu_n<T, H, 8, false, true, true>(a, s, nb, nsim) : mu_n<T, H, 8, false, true>(a, s, nb, nsim);
   }
-  if (a.mc.V <= 4)
-    return stats ? mu_n<T, H, 4, true, false>(a, s, nb, 1) : mu_n<T, H, 4, false, false>(a, s, nb, 1);
-  return stats ? mu_n<T, H, 8, true, false>(a, s, nb, 1) : mu_n<T, H, 8, false, false>(a, s, nb, 1);
+  if (a.mc.V <= 4) {
+    if (stats) return mu_n<T, H, 4, true, false>(a, s, nb, 1);
+    return fu ? mu_n<T, H, 4, false, false, true>(a, s, nb, 1) : mu_n<T, H, 4, false, false>(a, s, nb, 1);
+  }
+  if (stats) return mu_n<T, H, 8, true, false>(a, s, nb, 1);
+  return fu ? mu_n<T, H, 8, false, false, true>(a, s, nb, 1) : mu_n<T, H, 8, false, false>(a, s, nb, 1);
 }
 
 template <typename T>

@@ -53,6 +53,7 @@ template <typename T> struct MartArgs {
   MartConst<T>* mcs;  // batched: constants of sim blockIdx.y in device memory
   T* r_out;           // when set: R_p written out [V][N] (adjoint checkpoints)
   int lr_req;         // rows per block asked by the autotuner (0 = default)
+  cplx<T>* spec_next;  // FUSE: packed z spectra of eta'^2 for the next step (may be spec)
 };
 
 // advance the step counter of every batched simulation (keeps a captured
@@ -132,7 +133,12 @@ template <int VM, bool STATS> struct UpdBlocks {  // resident blocks asked of th
   static constexpr int v = (VM <= 4 && !STATS) ? 3 : 1;
 };
 
-template <typename T, int H, int VM, bool STATS, bool BATCH>
+// FUSE: the next step's z forward runs here too.  Each thread overwrites the
+// R values of its own cells with eta'^2 (only it reads them), and after the
+// sweep every (variant, row) line transforms its shared-memory row into the
+// packed spectrum of the next step, in the rows of the spectrum buffer this
+// block alone read: the next step then starts at the y forward pass.
+template <typename T, int H, int VM, bool STATS, bool BATCH, bool FUSE = false>
 __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(MartArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
@@ -145,6 +151,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     a.spec += off / 2;
     a.eta_in += off;
     a.eta_out += off;
+    if (FUSE) a.spec_next += off / 2;
   }
   const int Vn = mc.V;
   {
@@ -277,9 +284,27 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       }
       if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
       if (!BATCH && a.r_out) stv<CW>(a.r_out + (long long)q * N + cell, rv);
+      if (FUSE) {
+        T* sq = const_cast<T*>(Rq);
+#pragma unroll
+        for (int j = 0; j < CW; ++j) sq[j] = out[j] * out[j];
+      }
     }
   }
   if (STATS) block_reduce_store(acc, ACC_N, a.partials);
+  if (FUSE) {
+    __syncthreads();
+    const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
+    const int v = line % Vn, rr = line / Vn;
+    const long long row = (long long)blockIdx.x * a.lr + rr;
+    const bool act = rr < a.lr && row < a.nrows;
+    V* sl = smb + line * L::PAD;
+    V x[L::R1];
+#pragma unroll
+    for (int r = 0; r < L::R1; ++r) x[r] = sl[L::in_pos(t, r)];
+    __syncthreads();
+    zfwd_line<T, H>(x, t, sl, act ? a.spec_next + ((long long)v * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
+  }
 }
 
 // Sum per-block partials [nb][n] into out[n] with Neumaier compensation.

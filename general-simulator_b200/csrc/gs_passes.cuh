@@ -149,6 +149,41 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
 // ---------------------------------------------------------------------------
 // z forward: real rows -> packed half spectrum, with a fused prologue.
 // ---------------------------------------------------------------------------
+// z forward of one row held as H complex values v (in_pos order: the pairs
+// (r[2m], r[2m+1]) of the real row): the length-H FFT, then the split into
+// the packed half spectrum, written to dst (nullptr: the line is inactive).
+// sl is the line's shared buffer (PAD values).  All threads of the block call it.
+template <typename T, int H>
+__device__ __forceinline__ void zfwd_line(cplx<T> (&v)[Line<T, H>::R1], int t, cplx<T>* sl, cplx<T>* dst,
+                                          const cplx<T>* __restrict__ tw_h, const cplx<T>* __restrict__ tw_n2) {
+  using L = Line<T, H>;
+  using V = cplx<T>;
+  auto sm = [sl](int pos) -> V& { return sl[pos]; };
+  L::template run<-1>(v, t, sm, tw_h);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = v[i];
+  __syncthreads();
+  if (dst) {
+#pragma unroll
+    for (int i = 0; i < L::R1; ++i) {
+      const int k = L::out_pos(t, i);
+      const V zk = sl[k];
+      V s;
+      if (k == 0) {
+        s = mk2(zk.x + zk.y, zk.x - zk.y);
+      } else {
+        const V zm = sl[H - k];
+        const V e = mk2((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+        const V d = mk2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+        const V o = mk2((T)0.5 * d.y, (T)-0.5 * d.x);  // -i d / 2
+        s = e + cmul(o, __ldg(&tw_n2[k]));
+      }
+      dst[k] = s;
+    }
+  }
+}
+
 template <typename T> struct ZfwdArgs {
   const T* src[2 * GS_MAXF];   // row source of each field (n0*n1 rows of n2)
   int square[2 * GS_MAXF];     // 1: transform src^2 (eta^2), 0: src
@@ -174,7 +209,6 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
   const long long row = (long long)blockIdx.x * a.lpc + line;
   const bool act = row < a.nrows;
   V* sl = smb + line * L::PAD;
-  auto sm = [sl](int pos) -> V& { return sl[pos]; };
   V v[L::R1];
   if (act) {
     const int f = (int)(row / a.rows_per_field);
@@ -196,30 +230,7 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) v[r] = mk2((T)0, (T)0);
   }
-  L::template run<-1>(v, t, sm, a.tw_h);
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = v[i];
-  __syncthreads();
-  if (act) {
-    V* dst = a.dst + row * H;
-#pragma unroll
-    for (int i = 0; i < L::R1; ++i) {
-      const int k = L::out_pos(t, i);
-      const V zk = sl[k];
-      V s;
-      if (k == 0) {
-        s = mk2(zk.x + zk.y, zk.x - zk.y);
-      } else {
-        const V zm = sl[H - k];
-        const V e = mk2((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
-        const V d = mk2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
-        const V o = mk2((T)0.5 * d.y, (T)-0.5 * d.x);  // -i d / 2
-        s = e + cmul(o, __ldg(&a.tw_n2[k]));
-      }
-      dst[k] = s;
-    }
-  }
+  zfwd_line<T, H>(v, t, sl, act ? a.dst + row * H : nullptr, a.tw_h, a.tw_n2);
 }
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,11 @@ struct gs_sim {
   // autotuner or the caller
   gs_schedule sched = {0, 0, 0, 0};
   bool trial = false;  // steps that leave the state as it was (autotuner timing)
+  // the martensite update also writes the next step's z spectra (fused z
+  // forward); spec_ready says the spectrum buffer holds those of eta[spec_cur]
+  bool fuse = true;
+  bool spec_ready = false;
+  int spec_cur = -1;
   void* btab = nullptr;
   size_t btab_bytes = 0;
   int btab_state = 0;

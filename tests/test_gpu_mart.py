@@ -291,3 +291,32 @@ def test_graph_replay_equals_direct_steps(gb, dtype):
     assert np.all(np.isfinite(a0)) and np.all(np.isfinite(b0))
     assert np.array_equal(a0, a1) and np.array_equal(b0, b1)
     assert s0["e_el"] == s1["e_el"] and s0["mass"] == s1["mass"]
+
+
+@pytest.mark.parametrize("dtype,shape", [(F32, (32, 32, 32)), (F64, (8, 12, 12)), (F64, (8, 12, 2)), (F32, (1, 64, 96))])
+def test_fused_z_forward_same_bits_as_separate_pass(gb, dtype, shape):
+    """Steps after the first take the z spectra that the previous update
+    wrote (fused z forward); uploading the field before every step forces
+    the separate z-forward pass.  Both give the same bits."""
+    p = base3d(gb, shape, dtype, noise=1e-3)
+    eta0 = gb.initial_eta(p, 41, 0.3)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    s = gb.Sim(p)
+    try:
+        s.set_field("eta", eta0)
+        s.step(4)
+        fused = s.eta(np.float64)
+    finally:
+        s.close()
+    s = gb.Sim(p)
+    try:
+        e = eta0
+        for k in range(4):
+            s.set_field("eta", e)
+            s.set_scalar("step", k)
+            s.step(1)
+            e = s.eta(np.float64)
+    finally:
+        s.close()
+    assert np.array_equal(fused, e)
