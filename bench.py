@@ -215,7 +215,8 @@ def extra_adjoint(steps_fwd: int = 200) -> dict:
     """Calibration workload: 96^3, 3 variants, FP32, 200 steps, checkpoint
     every 20, noise off.  forward = 200 plain steps (gs_sim_step); backward
     = gs_adjoint_backward (segment recompute + adjoint sweeps + gradient
-    sums), both device time on one stream."""
+    sums), both device time on one stream, both replaying captured graphs
+    (the forward also timed with direct launches)."""
     import ctypes as C
 
     import torch
@@ -239,18 +240,26 @@ def extra_adjoint(steps_fwd: int = 200) -> dict:
 
     with torch.cuda.stream(stream):
         a.forward(eta0, sh)
-        back()
-        bwd = min(_timed(stream, back) for _ in range(3))
+        back()  # first run direct; later ones replay captured graphs
+        bwd = []
+        for _ in range(4):
+            a.forward(eta0, sh)
+            bwd.append(_timed(stream, back))
+        bwd = min(bwd)
         launches = a.launch_count()
-        sim = gb.Sim(p)
-        sim.set_field("eta", eta0.astype(np.float32))
-        sim.step(20, sh)
-        fwd = min(_timed(stream, lambda: sim.step(steps_fwd, sh)) for _ in range(3))
-        sim.close()
+        fwd = {}
+        for graph in (False, True):
+            sim = gb.Sim(p)
+            sim.use_graph(graph)
+            sim.set_field("eta", eta0.astype(np.float32))
+            sim.step(20, sh)
+            fwd[graph] = min(_timed(stream, lambda: sim.step(steps_fwd, sh)) for _ in range(3))
+            sim.close()
     mem = a.device_bytes()
     run.close()
     return {"workload": "96^3, 3 variants, FP32, 200 steps, checkpoint every 20, noise off",
-            "forward_ms": fwd, "backward_ms": bwd, "adjoint_to_forward": bwd / fwd,
+            "forward_ms": fwd[True], "forward_direct_ms": fwd[False], "backward_ms": bwd,
+            "adjoint_to_forward": bwd / fwd[True],
             "backward_launches": launches, "device_bytes": mem,
             "note": "backward includes recomputing every segment from its checkpoint"}
 

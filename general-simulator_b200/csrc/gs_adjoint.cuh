@@ -43,7 +43,7 @@ template <typename T> struct AdjArgs {
 };
 
 template <typename T, int H, int VM>
-__global__ void k_adj_update(AdjArgs<T> a) {
+__global__ void __launch_bounds__(256, VM <= 4 ? 2 : 1) k_adj_update(AdjArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
   constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
@@ -71,11 +71,12 @@ __global__ void k_adj_update(AdjArgs<T> a) {
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const long long N = a.nrows * n2;
   const int upr = n2 / CW;
-  const int nunits = a.lr * Vn * upr;
+  const int nunits = a.lr * upr;
+  // one thread per run of CW cells, all variants: the centre values of eta
+  // and lambda and the sums S, eta.lambda are loaded and formed once
 #pragma unroll 1
   for (int w = threadIdx.x; w < nunits; w += blockDim.x) {
-    const int rq = (int)a.fd_upr.div((uint32_t)w), u = w - rq * upr;
-    const int rr = (int)a.fd_v.div((uint32_t)rq), q = rq - rr * Vn;
+    const int rr = (int)a.fd_upr.div((uint32_t)w), u = w - rr * upr;
     const long long row = (long long)blockIdx.x * a.lr + rr;
     if (row >= a.nrows) continue;
     const int x = (int)a.fd_n1.div((uint32_t)row), y = (int)(row - (long long)x * n1);
@@ -83,6 +84,9 @@ __global__ void k_adj_update(AdjArgs<T> a) {
     const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
     const int z0 = u * CW;
     const long long rowb = row * n2, cell = rowb + z0;
+    const long long oxp = ((long long)xp * n1 + y) * n2 + z0 - cell, oxm = ((long long)xm * n1 + y) * n2 + z0 - cell;
+    const long long oyp = ((long long)x * n1 + yp) * n2 + z0 - cell, oym = ((long long)x * n1 + ym) * n2 + z0 - cell;
+    const int ozl = (z0 == 0 ? n2 - 1 : z0 - 1) - z0, ozr = (z0 + CW == n2 ? 0 : z0 + CW) - z0;
     T e[VM][CW], l[VM][CW];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
@@ -90,58 +94,57 @@ __global__ void k_adj_update(AdjArgs<T> a) {
         ldv<CW>(a.eta + (long long)p * N + cell, e[p]);
         ldv<CW>(a.lam_in + (long long)p * N + cell, l[p]);
       }
-    const T* lq_ = a.lam_in + (long long)q * N;
-    T vxp[CW], vxm[CW], vyp[CW], vym[CW], Rq[CW];
-    ldv<CW>(lq_ + ((long long)xp * n1 + y) * n2 + z0, vxp);
-    ldv<CW>(lq_ + ((long long)xm * n1 + y) * n2 + z0, vxm);
-    ldv<CW>(lq_ + ((long long)x * n1 + yp) * n2 + z0, vyp);
-    ldv<CW>(lq_ + ((long long)x * n1 + ym) * n2 + z0, vym);
-    ldv<CW>(a.R + (long long)q * N + cell, Rq);
-    const T zl_ = lq_[rowb + (z0 == 0 ? n2 - 1 : z0 - 1)];
-    const T zr_ = lq_[rowb + (z0 + CW == n2 ? 0 : z0 + CW)];
-    const T* Qq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
-    T linq = 0, eqv[CW], lqv[CW];
-#pragma unroll
-    for (int p = 0; p < VM; ++p)
-      if (p == q) {
-        linq = mc.lin[p];
-#pragma unroll
-        for (int j = 0; j < CW; ++j) {
-          eqv[j] = e[p][j];
-          lqv[j] = l[p][j];
-        }
-      }
-    T out[CW];
+    T S[CW], ed[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
-      T S = 0, ed = 0;
+      T s2 = 0, sd = 0;
 #pragma unroll
       for (int p = 0; p < VM; ++p)
         if (p < Vn) {
-          S += e[p][j] * e[p][j];
-          ed += e[p][j] * l[p][j];
+          s2 += e[p][j] * e[p][j];
+          sd += e[p][j] * l[p][j];
         }
-      const T eq = eqv[j], lq = lqv[j];
-      const T zlv = j == 0 ? zl_ : lqv[j - 1];
-      const T zrv = j == CW - 1 ? zr_ : lqv[j + 1];
-      const T d0 = vxp[j] + vxm[j] - 2 * lq, d1 = vyp[j] + vym[j] - 2 * lq, d2 = zlv + zrv - 2 * lq;
-      const T gl = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;  // L kappa lap lam
-      const T lap = mc.gcoef[0] * d0 + mc.gcoef[1] * d1 + mc.gcoef[2] * d2;
-      const T e2 = eq * eq;
-      const T off = ed - eq * lq;
-      const T Hl = (mc.A2 - 3 * mc.A4 * e2 + mc.A6 * S * S + 2 * mc.Ac * (S - e2)) * lq +
-                   4 * eq * (mc.A6 * S * ed + mc.Ac * off);
-      const T Rv = Rq[j], Qv = Qq[j];
-      out[j] = lq + mc.dt * (gl - mc.L * Hl + mc.el * (Rv * lq + 2 * eq * Qv) + linq * lq);
-      const double el_ = (double)eq * (double)lq;
-      acc[ADJ_ETA_LAP] += (double)eq * (double)lap;
-      acc[ADJ_ETA_LAM] += el_;
-      acc[ADJ_ETA3_LAM] += (double)e2 * el_;
-      acc[ADJ_S2_ETA_LAM] += (double)S * (double)S * el_;
-      acc[ADJ_AC_LAM] += 2.0 * ((double)S - (double)e2) * el_;
-      acc[ADJ_S_LAM] += (2.0 * (double)mc.el * (double)Rv + (double)linq) * el_;
+      S[j] = s2;
+      ed[j] = sd;
     }
-    stv<CW>(a.lam_out + (long long)q * N + cell, out);
+#pragma unroll
+    for (int q = 0; q < VM; ++q) {
+      if (q >= Vn) break;
+      const T* lq_ = a.lam_in + (long long)q * N + cell;
+      T vxp[CW], vxm[CW], vyp[CW], vym[CW], Rq[CW];
+      ldv<CW>(lq_ + oxp, vxp);
+      ldv<CW>(lq_ + oxm, vxm);
+      ldv<CW>(lq_ + oyp, vyp);
+      ldv<CW>(lq_ + oym, vym);
+      ldv<CW>(a.R + (long long)q * N + cell, Rq);
+      const T zl_ = lq_[ozl], zr_ = lq_[ozr];
+      const T* Qq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
+      const T linq = mc.lin[q];
+      T out[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        const T eq = e[q][j], lq = l[q][j];
+        const T zlv = j == 0 ? zl_ : l[q][j - 1];
+        const T zrv = j == CW - 1 ? zr_ : l[q][j + 1];
+        const T d0 = vxp[j] + vxm[j] - 2 * lq, d1 = vyp[j] + vym[j] - 2 * lq, d2 = zlv + zrv - 2 * lq;
+        const T gl = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;  // L kappa lap lam
+        const T lap = mc.gcoef[0] * d0 + mc.gcoef[1] * d1 + mc.gcoef[2] * d2;
+        const T e2 = eq * eq;
+        const T off = ed[j] - eq * lq;
+        const T Hl = (mc.A2 - 3 * mc.A4 * e2 + mc.A6 * S[j] * S[j] + 2 * mc.Ac * (S[j] - e2)) * lq +
+                     4 * eq * (mc.A6 * S[j] * ed[j] + mc.Ac * off);
+        const T Rv = Rq[j], Qv = Qq[j];
+        out[j] = lq + mc.dt * (gl - mc.L * Hl + mc.el * (Rv * lq + 2 * eq * Qv) + linq * lq);
+        const double el_ = (double)eq * (double)lq;
+        acc[ADJ_ETA_LAP] += (double)eq * (double)lap;
+        acc[ADJ_ETA_LAM] += el_;
+        acc[ADJ_ETA3_LAM] += (double)e2 * el_;
+        acc[ADJ_S2_ETA_LAM] += (double)S[j] * (double)S[j] * el_;
+        acc[ADJ_AC_LAM] += 2.0 * ((double)S[j] - (double)e2) * el_;
+        acc[ADJ_S_LAM] += (2.0 * (double)mc.el * (double)Rv + (double)linq) * el_;
+      }
+      stv<CW>(a.lam_out + (long long)q * N + cell, out);
+    }
   }
   Neu nacc[ADJ_N];
 #pragma unroll

@@ -1754,13 +1754,28 @@ struct gs_adjoint {
   void* RT = nullptr;
   double* gsum = nullptr;  // [nsteps][ADJ_N]
   int seg_valid = -1;      // segment held in seg_eta / seg_R
+  const void* z_ready = nullptr;  // field whose z spectra the last update left in spec
+  // the forward steps and the reverse sweep replayed as CUDA graphs after a
+  // first direct run (gs_adjoint_use_graph)
+  bool use_graph = true, warm = false;
+  cudaGraphExec_t gfwd = nullptr, gbwd = nullptr;
+  cudaStream_t gstream = nullptr;
+  int64_t nl_fwd = 0, nl_bwd = 0;  // kernel launches inside each graph
+  int ret_fwd = 0, ret_bwd = 0;     // what each body returned (kept for replays)
   bool forward_done = false, have_target = false;
   double lam_el = 0, e_target = 0, e_el_T = 0;
   size_t bytes = 0;
 };
 
+static void adj_graph_reset(gs_adjoint* a) {
+  if (a->gfwd) cudaGraphExecDestroy(a->gfwd);
+  if (a->gbwd) cudaGraphExecDestroy(a->gbwd);
+  a->gfwd = a->gbwd = nullptr;
+}
+
 static void free_adjoint(gs_adjoint* a) {
   if (!a) return;
+  adj_graph_reset(a);
   auto f = [](void* p) {
     if (p) cudaFree(p);
   };
@@ -1848,6 +1863,7 @@ extern "C" int gs_adjoint_set_params(gs_adjoint* a, const gs_params* p) {
     return gs_set_error(GS_EINVAL, "adjoint: grid, variant count and dtype are fixed at creation");
   a->s->p = *p;
   a->forward_done = false;
+  adj_graph_reset(a);  // the captured launches hold the old constants
   a->s->btab_state = 0;
   return ensure_btab(a->s, a->s->own_stream);
 }
@@ -1876,28 +1892,139 @@ static void* adj_eta(gs_adjoint* a, int n) {
   return a->s->eta[n & 1];
 }
 
+// one forward step in -> out; the update also leaves the z spectra of out^2
+// in the spectrum buffer, which the next step from out takes as its z forward
 template <typename T>
 static int adj_fwd_step(gs_adjoint* a, const void* in, void* out, void* r_out, int n, cudaStream_t st) {
   gs_sim* s = a->s;
   s->step = n;
-  GS_TRY(elastic_chain<T>(s, reinterpret_cast<const T*>(in), st));
+  GS_TRY(elastic_chain<T>(s, reinterpret_cast<const T*>(in), st, a->z_ready == in));
   MartArgs<T> ma;
   fill_mart_args<T>(s, ma, reinterpret_cast<const T*>(in), reinterpret_cast<T*>(out));
   ma.r_out = reinterpret_cast<T*>(r_out);
+  ma.spec_next = reinterpret_cast<cplx<T>*>(s->spec);
   GS_CU(launch_mart_update<T>(ma, s->h, false, st, nullptr), "update pass");
   s->launches += 1;
+  a->z_ready = out;
+  return GS_OK;
+}
+
+// The reverse sweep from lam[0] (the seed) to dJ/deta_0, segment by segment;
+// returns the index of the lam buffer that holds dJ/deta_0.  Its launches
+// depend only on the handle's sizes and parameters, so it can be captured.
+template <typename T> static int adj_sweep(gs_adjoint* a, cudaStream_t st) {
+  gs_sim* s = a->s;
+  const int V = s->p.nvariants;
+  const long long N = s->N;
+  int c = 0;
+  const T* src[GS_MAXF];
+  const T* mul[GS_MAXF];
+  int sq[GS_MAXF];
+  for (int j = a->nseg - 1; j >= 0; --j) {
+    const int n0 = j * a->K, len = (j == a->nseg - 1) ? a->nsteps - n0 : a->K;
+    if (a->seg_valid != j) {  // recompute eta_n and R_n of the segment
+      a->seg_valid = j;
+      a->z_ready = nullptr;  // the backward chains used the spectrum buffer
+      for (int i = 0; i < len; ++i) {
+        void* in = i == 0 ? a->ckpt[j] : a->seg_eta[i];
+        void* out = i + 1 < len ? a->seg_eta[i + 1] : s->eta[0];
+        GS_TRY(adj_fwd_step<T>(a, in, out, a->seg_R[i], n0 + i, st));
+      }
+    }
+    for (int i = len - 1; i >= 0; --i) {
+      const int n = n0 + i;
+      const T* eta = reinterpret_cast<const T*>(i == 0 ? a->ckpt[j] : a->seg_eta[i]);
+      const T* lin = reinterpret_cast<const T*>(a->lam[c]);
+      for (int f = 0; f < V; ++f) {
+        src[f] = eta + (long long)f * N;
+        mul[f] = lin + (long long)f * N;
+        sq[f] = 0;
+      }
+      GS_TRY(elastic_chain_g<T>(s, src, sq, V, 0, 1.0 / (double)N, s->spec, V, st, mul));
+      AdjArgs<T> aa;
+      memset(&aa, 0, sizeof(aa));
+      aa.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+      aa.eta = eta;
+      aa.lam_in = lin;
+      aa.lam_out = reinterpret_cast<T*>(a->lam[c ^ 1]);
+      aa.R = reinterpret_cast<const T*>(a->seg_R[i]);
+      aa.n0 = s->n0;
+      aa.n1 = s->n1;
+      aa.n2 = s->n2;
+      aa.nrows = (long long)s->n0 * s->n1;
+      aa.tw_h = twp<T>(s, 1);
+      aa.tw_n2 = twp<T>(s, 0);
+      s->step = n;
+      build_mart<T>(s, aa.mc);
+      aa.partials = s->partials;
+      aa.fd_n1 = FastDiv((uint32_t)s->n1);
+      aa.fd_upr = FastDiv((uint32_t)(s->n2 % 4 == 0 ? s->n2 / 4 : s->n2 / 2));
+      aa.fd_v = FastDiv((uint32_t)V);
+      int nbk = 0;
+      GS_CU(launch_adj_update<T>(aa, s->h, st, &nbk), "adjoint update");
+      GS_CU(launch_reduce(s->partials, nbk, ADJ_N, a->gsum + (size_t)n * ADJ_N, st), "adjoint reduce");
+      s->launches += 2;
+      c ^= 1;
+    }
+  }
+  return c;
+}
+
+// The forward steps eta_0 -> eta_T of the run (checkpoints, last segment).
+template <typename T> static int adj_steps(gs_adjoint* a, cudaStream_t st) {
+  a->seg_valid = a->nseg - 1;
+  a->z_ready = nullptr;
+  for (int n = 0; n < a->nsteps; ++n) {
+    void* r_out = n / a->K == a->nseg - 1 ? a->seg_R[n % a->K] : nullptr;
+    GS_TRY(adj_fwd_step<T>(a, adj_eta(a, n), adj_eta(a, n + 1), r_out, n, st));
+  }
+  return GS_OK;
+}
+
+// Run body directly the first time (kernel attributes are set outside any
+// capture), then capture it once as a CUDA graph and replay that graph.
+// body's host-side effects are the same on every run, so replaying leaves
+// the handle as a direct run would; *ret holds body's result from the last
+// direct run or capture, which a replay repeats.
+template <class F>
+static int adj_graph(gs_adjoint* a, cudaGraphExec_t* ex, int* ret, int64_t* nlaunch, cudaStream_t st, F body,
+                     bool allowed = true) {
+  if (!a->use_graph || !a->warm || !allowed) {
+    const int r = body();
+    if (r < 0) return r;
+    *ret = r;
+    return GS_OK;
+  }
+  if (!*ex || a->gstream != st) {
+    if (*ex) cudaGraphExecDestroy(*ex);
+    *ex = nullptr;
+    cudaGraph_t g;
+    const int64_t l0 = a->s->launches;
+    GS_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const int r = body();
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (r < 0) return r;
+    GS_CU(e, "end capture");
+    GS_CU(cudaGraphInstantiate(ex, g, 0), "instantiate graph");
+    cudaGraphDestroy(g);
+    a->gstream = st;
+    *ret = r;
+    *nlaunch = a->s->launches - l0;
+    a->s->launches = l0;
+  }
+  GS_CU(cudaGraphLaunch(*ex, st), "graph launch");
+  a->s->launches += *nlaunch;
   return GS_OK;
 }
 
 template <typename T> static int adj_forward(gs_adjoint* a, cudaStream_t st) {
   gs_sim* s = a->s;
+  GS_TRY(adj_graph(a, &a->gfwd, &a->ret_fwd, &a->nl_fwd, st, [&]() { return adj_steps<T>(a, st); }));
   a->seg_valid = a->nseg - 1;
-  for (int n = 0; n < a->nsteps; ++n) {
-    void* r_out = n / a->K == a->nseg - 1 ? a->seg_R[n % a->K] : nullptr;
-    GS_TRY(adj_fwd_step<T>(a, adj_eta(a, n), adj_eta(a, n + 1), r_out, n, st));
-  }
+  a->z_ready = a->etaT;
   // E_el and R at the final state
-  GS_TRY(elastic_chain<T>(s, reinterpret_cast<const T*>(a->etaT), st));
+  GS_TRY(elastic_chain<T>(s, reinterpret_cast<const T*>(a->etaT), st, a->z_ready == a->etaT));
+  a->z_ready = nullptr;
   MartArgs<T> ma;
   fill_mart_args<T>(s, ma, reinterpret_cast<const T*>(a->etaT), nullptr);
   ma.r_out = reinterpret_cast<T*>(a->RT);
@@ -1952,56 +2079,11 @@ static int adj_backward(gs_adjoint* a, const void* seed_dev, double seed_e, doub
   GS_CU(launch_reduce(s->partials, nb, 1, s->red, st), "reduce");
   double field = 0;
   GS_CU(cudaMemcpyAsync(&field, s->red, sizeof(double), cudaMemcpyDeviceToHost, st), "loss D2H");
-  int c = 0;
-  const T* src[GS_MAXF];
-  const T* mul[GS_MAXF];
-  int sq[GS_MAXF];
-  for (int j = a->nseg - 1; j >= 0; --j) {
-    const int n0 = j * a->K, len = (j == a->nseg - 1) ? a->nsteps - n0 : a->K;
-    if (a->seg_valid != j) {  // recompute eta_n and R_n of the segment
-      a->seg_valid = j;
-      for (int i = 0; i < len; ++i) {
-        void* in = i == 0 ? a->ckpt[j] : a->seg_eta[i];
-        void* out = i + 1 < len ? a->seg_eta[i + 1] : s->eta[0];
-        GS_TRY(adj_fwd_step<T>(a, in, out, a->seg_R[i], n0 + i, st));
-      }
-    }
-    for (int i = len - 1; i >= 0; --i) {
-      const int n = n0 + i;
-      const T* eta = reinterpret_cast<const T*>(i == 0 ? a->ckpt[j] : a->seg_eta[i]);
-      const T* lin = reinterpret_cast<const T*>(a->lam[c]);
-      for (int f = 0; f < V; ++f) {
-        src[f] = eta + (long long)f * N;
-        mul[f] = lin + (long long)f * N;
-        sq[f] = 0;
-      }
-      GS_TRY(elastic_chain_g<T>(s, src, sq, V, 0, 1.0 / (double)N, s->spec, V, st, mul));
-      AdjArgs<T> aa;
-      memset(&aa, 0, sizeof(aa));
-      aa.spec = reinterpret_cast<const cplx<T>*>(s->spec);
-      aa.eta = eta;
-      aa.lam_in = lin;
-      aa.lam_out = reinterpret_cast<T*>(a->lam[c ^ 1]);
-      aa.R = reinterpret_cast<const T*>(a->seg_R[i]);
-      aa.n0 = s->n0;
-      aa.n1 = s->n1;
-      aa.n2 = s->n2;
-      aa.nrows = (long long)s->n0 * s->n1;
-      aa.tw_h = twp<T>(s, 1);
-      aa.tw_n2 = twp<T>(s, 0);
-      s->step = n;
-      build_mart<T>(s, aa.mc);
-      aa.partials = s->partials;
-      aa.fd_n1 = FastDiv((uint32_t)s->n1);
-      aa.fd_upr = FastDiv((uint32_t)(s->n2 % 4 == 0 ? s->n2 / 4 : s->n2 / 2));
-      aa.fd_v = FastDiv((uint32_t)V);
-      int nbk = 0;
-      GS_CU(launch_adj_update<T>(aa, s->h, st, &nbk), "adjoint update");
-      GS_CU(launch_reduce(s->partials, nbk, ADJ_N, a->gsum + (size_t)n * ADJ_N, st), "adjoint reduce");
-      s->launches += 2;
-      c ^= 1;
-    }
-  }
+  // the captured sweep starts with the last segment held (as after a forward run)
+  const bool from_forward = a->seg_valid == a->nseg - 1;
+  GS_TRY(adj_graph(a, &a->gbwd, &a->ret_bwd, &a->nl_bwd, st, [&]() { return adj_sweep<T>(a, st); }, from_forward));
+  const int c = a->ret_bwd;
+  a->seg_valid = 0;  // as the sweep leaves it
   std::vector<double> h((size_t)a->nsteps * ADJ_N);
   GS_CU(cudaMemcpyAsync(h.data(), a->gsum, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "sums D2H");
   GS_CU(cudaStreamSynchronize(st), "adjoint sync");
@@ -2049,7 +2131,15 @@ extern "C" int gs_adjoint_backward(gs_adjoint* a, const void* seed, int seed_dty
   const int c = s->p.dtype == GS_DTYPE_F64 ? adj_backward<double>(a, sd, seed_e, loss, grads, st)
                                            : adj_backward<float>(a, sd, seed_e, loss, grads, st);
   if (c < 0) return c;
+  a->warm = true;  // both sweeps have run directly: kernel attributes are set
   if (grad_eta0) GS_TRY(download(s, a->lam[c], grad_eta0, count, grad_dtype));
+  return GS_OK;
+}
+
+extern "C" int gs_adjoint_use_graph(gs_adjoint* a, int on) {
+  if (!a) return gs_set_error(GS_EINVAL, "gs_adjoint_use_graph: null handle");
+  a->use_graph = on != 0;
+  if (!on) adj_graph_reset(a);
   return GS_OK;
 }
 

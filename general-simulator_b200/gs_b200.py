@@ -163,6 +163,7 @@ def lib() -> C.CDLL:
         "gs_adjoint_backward": (C.c_int, [vp, vp, C.c_int, C.c_double, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double), vp, C.c_int, vp]),
         "gs_adjoint_device_bytes": (C.c_size_t, [vp]),
+        "gs_adjoint_use_graph": (C.c_int, [vp, C.c_int]),
         "gs_adjoint_launch_count": (C.c_int64, [vp]),
         "gs_sim_set_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_get_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
@@ -265,6 +266,9 @@ class Adjoint:
 
     def device_bytes(self) -> int:
         return int(lib().gs_adjoint_device_bytes(self.h))
+
+    def use_graph(self, on: bool) -> None:
+        check(lib().gs_adjoint_use_graph(self.h, int(bool(on))), "gs_adjoint_use_graph")
 
     def launch_count(self) -> int:
         return int(lib().gs_adjoint_launch_count(self.h))

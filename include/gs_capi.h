@@ -245,6 +245,10 @@ int gs_adjoint_forward(gs_adjoint* a, const void* eta0, int dtype, void* eta_fin
                        void* stream);
 int gs_adjoint_backward(gs_adjoint* a, const void* seed, int seed_dtype, double seed_e, double* loss,
                         double* grads, void* grad_eta0, int grad_dtype, void* stream);
+/* Replay the forward steps and the reverse sweep as CUDA graphs captured
+ * after a first direct run (1, default) or always launch directly (0).
+ * Results are the same either way; new parameters drop the graphs. */
+int gs_adjoint_use_graph(gs_adjoint* a, int on);
 /* Device bytes held by the handle (checkpoints, segment, adjoint fields). */
 size_t gs_adjoint_device_bytes(const gs_adjoint* a);
 /* Kernel launches issued by the last forward or backward call. */

@@ -148,3 +148,36 @@ def test_adjoint_rejects_refcompat_and_bad_use(gb):
         assert a.device_bytes() > 0
     finally:
         a.close()
+
+
+@pytest.mark.parametrize("dtype", [F64, F32])
+def test_graph_replay_equals_direct_launches(gb, dtype):
+    """Forward and backward replayed as captured graphs (after the first
+    direct run) give the same bits as direct launches, across repeated
+    runs, a second backward without a forward and new parameters."""
+    p, eta0, tgt = setup(gb, (8, 8, 12), 3, dtype, 1e-3)
+    eta1 = gb.initial_eta(p, 9, 0.3)
+
+    def run(graph):
+        a = gb.Adjoint(p, 7, 3)
+        out = []
+        try:
+            a.use_graph(graph)
+            a.set_loss(tgt, 0.1, 0.0)
+            for e in (eta0, eta1, eta0):
+                a.forward(e)
+                out.append(a.backward())
+            out.append(a.backward())  # no forward in between
+            q = p.copy()
+            q.kappa = 0.7
+            a.set_params(q)
+            for _ in range(2):
+                a.forward(eta1)
+                out.append(a.backward())
+        finally:
+            a.close()
+        return out
+
+    direct, graph = run(False), run(True)
+    for (l0, g0, e0), (l1, g1, e1) in zip(direct, graph):
+        assert np.array_equal(l0, l1) and np.array_equal(g0, g1) and np.array_equal(e0, e1)
