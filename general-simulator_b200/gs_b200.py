@@ -170,6 +170,8 @@ def lib() -> C.CDLL:
         "gs_sim_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(GsSchedule)]),
         "gs_batch_autotune": (C.c_int, [vp, C.c_int, vp]),
         "gs_batch_get_schedule": (C.c_int, [vp, C.c_int, C.POINTER(GsSchedule)]),
+        "gs_cores_paint": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, C.c_double, C.c_double,
+                                     C.c_double, vp, vp]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
         "gs_mart_step_noalloc_max_bytes": (C.c_size_t, []),
     }

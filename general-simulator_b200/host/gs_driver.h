@@ -36,7 +36,7 @@ class Dynamics {
   virtual void WillReport(bool) {}
 };
 
-// factory of the registered plugins: mart, precipitate, stress, pow
+// factory of the registered plugins: mart, precipitate, stress, cores, pow
 std::unique_ptr<Dynamics> make_dynamics(const std::string& name);
 
 class Driver {

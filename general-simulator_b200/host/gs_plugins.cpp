@@ -7,8 +7,10 @@
 // (include/gs_capi.h).  `set model baseline` selects the project's
 // discretisation with the extra keys landau / kappa / mobility / noise /
 // appliedstress; the default is the reference's formulas.  Dynamics_pow is
-// the reference's host-only demo (src/dynamics_pow.cu:18-47).
+// the reference's host-only demo (src/dynamics_pow.cu:18-47); Dynamics_cores
+// makes the nuclei that start the precipitate chain.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -410,9 +412,105 @@ class Pow : public Dynamics {
   }
 };
 
+// Dynamics_cores (src/dynamics_cores.cu:14-186): nuclei for the precipitate
+// chain.  The placement makes the reference's draws from the C library's
+// random() in the reference's order (random: a centre, redrawn while it lies
+// in an earlier nucleus, then the variant; regular: one draw, then variant
+// cn % V); the painting of the grid runs on the device (gs_cores_paint).
+// regular2d / regular3d take the variant as random() % V: the reference's
+// floor(random() * VariantN) overflows int and indexes eta out of range.
+class Cores : public Dynamics {
+ public:
+  int V = 4, ncores = 5;
+  float radius = 5.0f, c1 = 0.2f, c2 = 0.44f;
+  std::string method = "random";
+  Field* eta = nullptr;
+  Field* conc = nullptr;
+
+  int Initialize() override {
+    nx = ny = nz = 16;
+    dx = dy = dz = 0.1f;
+    std::string s = (*Vars)["gridsize"];
+    if (!s.empty()) s >> nx >> ny >> nz >> dx >> dy >> dz;
+    (void)((*Vars)["variantn"] >>= V);
+    (void)((*Vars)["coresn"] >>= ncores);
+    (void)((*Vars)["radius"] >>= radius);
+    s = (*Vars)["concentration"];
+    if (!s.empty()) s >> c1 >> c2;
+    s = (*Vars)["method"];
+    if (!s.empty()) method = take_word(s);
+    eta = &(*Datas)["eta"];
+    eta->init({V, nx, ny, nz}, 0.0f);
+    conc = &(*Datas)["concentration"];
+    conc->init({nx, ny, nz}, c1);
+    return kNormal;
+  }
+
+  bool marked(const std::vector<int>& cen, int i, int j, int k) const {
+    const double r = (double)radius, r2 = r * r;
+    for (size_t q = 0; q + 2 < cen.size(); q += 3) {
+      const double x = i - cen[q], y = j - cen[q + 1], z = k - cen[q + 2];
+      auto in = [r2](double a, double b, double c) { return a * a + b * b + c * c <= r2; };
+      if (in(x, y, z) || in(x + nx, y, z) || in(x - nx, y, z) || in(x, y + ny, z) || in(x, y - ny, z) ||
+          in(x, y, z + nz) || in(x, y, z - nz))
+        return true;
+    }
+    return false;
+  }
+
+  int Calculate() override {
+    std::vector<int> cen, var;
+    if (method == "random") {
+      for (int cn = 0; cn < ncores; ++cn) {
+        int ox = 0, oy = 0, oz = 0;
+        for (int j = 0; j < 100000; ++j) {
+          ox = (int)(random() % nx);
+          oy = (int)(random() % ny);
+          oz = (int)(random() % nz);
+          if (!marked(cen, ox, oy, oz)) break;
+        }
+        cen.insert(cen.end(), {ox, oy, oz});
+        var.push_back((int)(random() % V));
+      }
+    } else if (method == "regular") {
+      for (int cn = 0; cn < ncores; ++cn) {
+        (void)random();
+        cen.insert(cen.end(), {nx / 2, ny / 2, nz / ncores / 2 + nx / ncores * cn});
+        var.push_back(cn % V);
+      }
+    } else if (method == "regular2d") {
+      for (int c1i = 0; c1i < ncores; ++c1i)
+        for (int c2i = 0; c2i < ncores; ++c2i) {
+          cen.insert(cen.end(), {nx / 2, ny / ncores / 2 + ny / ncores * c2i, nz / ncores / 2 + nx / ncores * c1i});
+          var.push_back((int)(random() % V));
+        }
+    } else if (method == "regular3d") {
+      for (int c1i = 0; c1i < ncores; ++c1i)
+        for (int c2i = 0; c2i < ncores; ++c2i)
+          for (int c3i = 0; c3i < ncores; ++c3i) {
+            cen.insert(cen.end(), {nx / ncores / 2 + nx / ncores * c3i, ny / ncores / 2 + ny / ncores * c2i,
+                                   nz / ncores / 2 + nx / ncores * c1i});
+            var.push_back((int)(random() % V));
+          }
+    } else {
+      return kNormal;  // the reference paints nothing for another method
+    }
+    if (gs_cores_paint(nx, ny, nz, V, (int)var.size(), cen.data(), var.data(), radius, c1, c2, eta->v.data(),
+                       conc->v.data()) != GS_OK) {
+      log() << "Error: " << capi_error() << "\n";
+      return kErr;
+    }
+    return kNormal;
+  }
+  int RunFunc(std::string) override { return kNormal; }
+  int Fix(float) override { return kNormal; }
+  std::string Get(std::string) override { return "nan"; }
+};
+
 }  // namespace
 
 std::unique_ptr<Dynamics> make_dynamics(const std::string& name) {
+  if (name == "cores") return std::make_unique<Cores>();
   if (name == "mart") return std::make_unique<Mart>();
   if (name == "precipitate") return std::make_unique<Precipitate>();
   if (name == "stress") return std::make_unique<Stress>();

@@ -185,6 +185,17 @@ int64_t gs_sim_launch_count(const gs_sim* s);
  * bit.  Setting a field, a schedule or autotuning drops the captured graph. */
 int gs_sim_use_graph(gs_sim* s, int on);
 
+/* ---- nuclei for the precipitate chain ----------------------------------- */
+/* Dynamics_cores::Calculate painting step (src/dynamics_cores.cu:55-186) on the
+ * device: ncores nuclei at centers[3q..3q+2] of variant[q], radius `radius`
+ * (used as a float, as the reference's Real), with the reference's periodic
+ * rule (the offset and its shifts by +-n along one axis at a time).  Writes
+ * eta [V][nx][ny][nz] (1 in a nucleus of that variant, else 0) and the
+ * concentration [nx][ny][nz] (c_core in any nucleus, else c_matrix) to host
+ * buffers.  The placement (random draws, marks) stays with the caller. */
+int gs_cores_paint(int nx, int ny, int nz, int nvariants, int ncores, const int* centers, const int* variant,
+                   double radius, double c_matrix, double c_core, float* eta_host, float* conc_host);
+
 /* ---- tile schedule and autotuner ---------------------------------------- */
 /* Tile sizes of the martensite passes: z lines per block, y and x columns
  * per block, update rows per block (0 = the launcher's default; sizes a

@@ -879,3 +879,45 @@ int or_mart_adjoint(const gs_params* p, const double* eta0, int nsteps, const do
   free(lnew);
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* nuclei of the precipitate chain (src/dynamics_cores.cu:55-186)      */
+/* ------------------------------------------------------------------ */
+/* The reference's test, point by point: pow(0.0f + i - ox, 2) + ... <=
+ * pow(0.0f + Radius, 2) in double, for the offset and its shifts by +-n
+ * along one axis at a time (the seven || terms of RandomCores). */
+static int core_hit(int i, int j, int k, int ox, int oy, int oz, int nx, int ny, int nz, double r2) {
+  const double dx = i - ox, dy = j - oy, dz = k - oz;
+#define SQ(a) ((a) * (a))
+  return SQ(dx) + SQ(dy) + SQ(dz) <= r2 || SQ(dx + nx) + SQ(dy) + SQ(dz) <= r2 ||
+         SQ(dx - nx) + SQ(dy) + SQ(dz) <= r2 || SQ(dx) + SQ(dy + ny) + SQ(dz) <= r2 ||
+         SQ(dx) + SQ(dy - ny) + SQ(dz) <= r2 || SQ(dx) + SQ(dy) + SQ(dz + nz) <= r2 ||
+         SQ(dx) + SQ(dy) + SQ(dz - nz) <= r2;
+#undef SQ
+}
+
+int or_cores_paint(int nx, int ny, int nz, int V, int ncores, const int* centers, const int* variant, double radius,
+                   double c_matrix, double c_core, float* eta, float* conc) {
+  const long long N = (long long)nx * ny * nz;
+  const double r = (double)(float)radius;
+  const double r2 = r * r;
+  for (long long c = 0; c < N; ++c) conc[c] = (float)c_matrix;
+  for (long long c = 0; c < N * V; ++c) eta[c] = 0.0f;
+  for (int q = 0; q < ncores; ++q)
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k)
+          if (core_hit(i, j, k, centers[3 * q], centers[3 * q + 1], centers[3 * q + 2], nx, ny, nz, r2)) {
+            const long long c = ((long long)i * ny + j) * nz + k;
+            conc[c] = (float)c_core;
+            eta[(long long)variant[q] * N + c] = 1.0f;
+          }
+  return 0;
+}
+
+int or_cores_marked(int nx, int ny, int nz, int ncores, const int* centers, double radius, int i, int j, int k) {
+  const double r = (double)(float)radius;
+  for (int q = 0; q < ncores; ++q)
+    if (core_hit(i, j, k, centers[3 * q], centers[3 * q + 1], centers[3 * q + 2], nx, ny, nz, r * r)) return 1;
+  return 0;
+}

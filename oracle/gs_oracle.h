@@ -62,6 +62,13 @@ int or_precip_stats(const gs_params* p, const double* c, const double* eta, gs_s
 /* Stress: stress [6][N] and defect [N] of an eta configuration. */
 int or_stress(const gs_params* p, const double* eta, double* stress, double* defect);
 
+/* Nuclei of the precipitate chain (src/dynamics_cores.cu:55-186): paint
+ * eta [V][N] and the concentration [N] (float, as the reference's Real);
+ * or_cores_marked says whether (i, j, k) lies in one of the first ncores. */
+int or_cores_paint(int nx, int ny, int nz, int V, int ncores, const int* centers, const int* variant, double radius,
+                   double c_matrix, double c_core, float* eta, float* conc);
+int or_cores_marked(int nx, int ny, int nz, int ncores, const int* centers, double radius, int i, int j, int k);
+
 /* Set the number of OpenMP threads used by the oracle (0 = default). */
 void or_set_threads(int n);
 int or_get_threads(void);

@@ -40,6 +40,11 @@ def lib() -> C.CDLL:
         L.or_precip_stats.argtypes = [P, dp, dp, S]
         L.or_stress.argtypes = [P, dp, dp, dp]
         L.or_mart_adjoint.argtypes = [P, dp, C.c_int, dp, C.c_double, C.c_double, dp, C.c_double, dp, dp, dp]
+        ip = C.POINTER(C.c_int)
+        fp = C.POINTER(C.c_float)
+        L.or_cores_paint.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, C.c_double, C.c_double,
+                                     C.c_double, fp, fp]
+        L.or_cores_marked.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, C.c_double, C.c_int, C.c_int, C.c_int]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         _lib = L
@@ -154,3 +159,41 @@ def mart_loss(p, eta0, nsteps, target, lam_el, e_target):
     eT = mart_run(p, eta0, nsteps)
     st = mart_stats(p, eT)
     return ((eT - target) ** 2).sum() + lam_el * (st["e_el"] - e_target) ** 2
+
+
+def cores_paint(shape, V, centers, variants, radius, c_matrix, c_core):
+    """(eta [V][nx][ny][nz], concentration [nx][ny][nz]) as float32."""
+    nx, ny, nz = shape
+    n = len(variants)
+    cen = np.ascontiguousarray(np.asarray(centers, dtype=np.int32).reshape(n * 3) if n else np.zeros(3, np.int32))
+    var = np.ascontiguousarray(np.asarray(variants, dtype=np.int32) if n else np.zeros(1, np.int32))
+    eta = np.zeros((V, nx, ny, nz), dtype=np.float32)
+    conc = np.zeros((nx, ny, nz), dtype=np.float32)
+    ip = C.POINTER(C.c_int)
+    fp = C.POINTER(C.c_float)
+    lib().or_cores_paint(nx, ny, nz, V, n, cen.ctypes.data_as(ip), var.ctypes.data_as(ip), radius, c_matrix, c_core,
+                         eta.ctypes.data_as(fp), conc.ctypes.data_as(fp))
+    return eta, conc
+
+
+def cores_place(shape, V, ncores, radius, method, rand):
+    """Nucleus centres and variants in the order the reference draws them;
+    rand() returns the next value of the C library's random()."""
+    nx, ny, nz = shape
+    centers, variants = [], []
+    ip = C.POINTER(C.c_int)
+    if method == "random":
+        for _ in range(ncores):
+            cen = np.ascontiguousarray(np.asarray(centers, dtype=np.int32).reshape(-1) if centers else np.zeros(3, np.int32))
+            for _ in range(100000):
+                o = (rand() % nx, rand() % ny, rand() % nz)
+                if not lib().or_cores_marked(nx, ny, nz, len(centers), cen.ctypes.data_as(ip), radius, *o):
+                    break
+            centers.append(o)
+            variants.append(rand() % V)
+    elif method == "regular":
+        for cn in range(ncores):
+            rand()
+            centers.append((nx // 2, ny // 2, nz // ncores // 2 + nx // ncores * cn))
+            variants.append(cn % V)
+    return centers, variants

@@ -5,8 +5,9 @@ reference's kernels are device-only); the front-end cases run anywhere.
 
   python tests/golden/make_ref_fixtures.py --out DIR [--physics] [--frontend]
 
-Writes DIR/ref_<case>.npz (inputs, dumps, the info lines) and
-DIR/frontend_<script>.txt.  The committed copies under tests/golden/ are
+Writes DIR/ref_<case>.npz (inputs, dumps, the info lines),
+DIR/frontend_<script>.txt and DIR/ref_cores.npz (the nuclei generator, which
+runs on the host in the reference).  The committed copies under tests/golden/ are
 the outputs of this script; the tests never run the reference.
 """
 from __future__ import annotations
@@ -203,6 +204,41 @@ def case_frontend(out: str) -> None:
             f.write(r.stdout)
 
 
+CORES_CASES = [  # (name, grid, variants, nuclei, radius, method)
+    ("random", (32, 24, 16), 4, 3, 4.5, "random"),
+    ("random_dense", (16, 16, 16), 3, 8, 5.0, "random"),
+    ("regular", (24, 20, 32), 4, 2, 3.0, "regular"),
+]
+
+
+def cores_script(grid, V, n, r, method) -> str:
+    nx, ny, nz = grid
+    return f"""sys cores
+set gridsize {nx} {ny} {nz} 0.2 0.2 0.2
+set variantn {V}
+set coresn {n}
+set radius {r}
+set concentration 0.2 0.44
+set method {method}
+set binary on
+dump dd 1 eta concentration
+run
+"""
+
+
+def case_cores(out: str) -> None:
+    """Dynamics_cores runs on the host in the reference: no device needed."""
+    arrays = {}
+    for name, grid, V, n, r, method in CORES_CASES:
+        with tempfile.TemporaryDirectory() as d:
+            with open(os.path.join(d, "in.cores"), "w") as f:
+                f.write(cores_script(grid, V, n, r, method))
+            subprocess.run([GSI, "in.cores"], cwd=d, capture_output=True, text=True, timeout=120)
+            arrays[f"{name}_eta"] = read_binary_field(os.path.join(d, "dd", "eta.1.data"))
+            arrays[f"{name}_concentration"] = read_binary_field(os.path.join(d, "dd", "concentration.1.data"))
+    np.savez_compressed(os.path.join(out, "ref_cores.npz"), **arrays)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
@@ -212,6 +248,7 @@ def main() -> None:
     os.makedirs(a.out, exist_ok=True)
     if a.frontend:
         case_frontend(a.out)
+        case_cores(a.out)
     if a.physics:
         case_mart(a.out)
         case_precipitate(a.out)

@@ -151,3 +151,39 @@ def test_stress_script_matches_reference(gsi, tmp_path):
     d = mf.read_binary_field(str(tmp_path / "dumpdir" / "defect.1.data"))
     assert rel_l2(s, ref["stress"]) < 2e-6
     assert np.array_equal(d, ref["defect"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", mf.CORES_CASES, ids=[c[0] for c in mf.CORES_CASES])
+def test_cores_script_identical_to_reference(gsi, tmp_path, case):
+    """`sys cores`: the same draws and the device painting give the
+    reference binary's eta and concentration dumps exactly."""
+    name, grid, V, n, r, method = case
+    run_script(gsi, tmp_path, "in.cores", mf.cores_script(grid, V, n, r, method))
+    ref = rc.load("cores")
+    eta = mf.read_binary_field(str(tmp_path / "dd" / "eta.1.data"))
+    conc = mf.read_binary_field(str(tmp_path / "dd" / "concentration.1.data"))
+    assert np.array_equal(eta, ref[f"{name}_eta"])
+    assert np.array_equal(conc, ref[f"{name}_concentration"])
+
+
+@pytest.mark.gpu
+def test_cores_paint_matches_oracle_large(gb, orc):
+    """gs_cores_paint through the C ABI against the oracle on a larger grid
+    with overlapping nuclei of several variants."""
+    import ctypes as C
+
+    rng = np.random.default_rng(5)
+    grid, V, n, r = (64, 48, 40), 4, 25, 7.5
+    centers = rng.integers(0, [64, 48, 40], size=(n, 3)).astype(np.int32)
+    variants = rng.integers(0, V, size=n).astype(np.int32)
+    eta = np.zeros((V,) + grid, np.float32)
+    conc = np.zeros(grid, np.float32)
+    L = gb.lib()
+    rc_ = L.gs_cores_paint(*grid, V, n, centers.ctypes.data_as(C.c_void_p), variants.ctypes.data_as(C.c_void_p),
+                           C.c_double(r), C.c_double(0.2), C.c_double(0.44), eta.ctypes.data_as(C.c_void_p),
+                           conc.ctypes.data_as(C.c_void_p))
+    assert rc_ == gb.GS_OK, gb.last_error()
+    oe, oc = orc.cores_paint(grid, V, centers.tolist(), variants.tolist(), r, 0.2, 0.44)
+    assert np.array_equal(eta, oe) and np.array_equal(conc, oc)
+    assert (eta.sum(axis=0) > 1).any()  # overlaps of different variants are exercised

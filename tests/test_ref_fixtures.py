@@ -79,3 +79,30 @@ def test_gpu_mart_refcompat_matches_reference(gb):
         assert abs(st["elastic_mean"] - el) <= 5e-5 * abs(el)
         assert abs(st["dislocation_mean"] - disl) <= 5e-5 * abs(disl)
     s.close()
+
+
+# ---- nuclei of the precipitate chain (Dynamics_cores) ----------------------
+CORES_CASES = [("random", (32, 24, 16), 4, 3, 4.5, "random"),
+               ("random_dense", (16, 16, 16), 3, 8, 5.0, "random"),
+               ("regular", (24, 20, 32), 4, 2, 3.0, "regular")]
+
+
+def _libc_random():
+    import ctypes
+
+    libc = ctypes.CDLL(None)
+    libc.random.restype = ctypes.c_long
+    libc.srandom(1)  # the state of a fresh process
+    return lambda: int(libc.random())
+
+
+@pytest.mark.parametrize("case", CORES_CASES, ids=[c[0] for c in CORES_CASES])
+def test_oracle_cores_match_reference(orc, case):
+    """The oracle's placement (the reference's random() draws and marks) and
+    painting reproduce the reference binary's eta and concentration."""
+    name, grid, V, n, r, method = case
+    ref = rc.load("cores")
+    centers, variants = orc.cores_place(grid, V, n, r, method, _libc_random())
+    eta, conc = orc.cores_paint(grid, V, centers, variants, r, 0.2, 0.44)
+    assert np.array_equal(eta, ref[f"{name}_eta"])
+    assert np.array_equal(conc, ref[f"{name}_concentration"])
