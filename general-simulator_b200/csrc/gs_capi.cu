@@ -1020,6 +1020,66 @@ static int download(gs_sim* s, const void* src, void* host, size_t count, int dt
   return GS_OK;
 }
 
+// K_p(x) = sigma(x):eps_p from the 6-component form xx xy xz yy yz zz (the
+// 3x3 remap of src/dynamics_mart.cu:128-150 and the contraction of
+// DislocationForceInit, :305-321, which the reference runs on the host),
+// in double with separately rounded products and sums, rounded to T at the end.
+struct KCoef {
+  double c[GS_MAX_V][6];  // multipliers of xx xy xz yy yz zz per variant
+};
+template <typename S, typename T>
+__global__ void k_stress_to_K(const S* __restrict__ sig, long long N, int V, KCoef kc, T* __restrict__ K) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    double s6[6];
+#pragma unroll
+    for (int b = 0; b < 6; ++b) s6[b] = (double)sig[(long long)b * N + i];
+    for (int v = 0; v < V; ++v) {
+      double acc = __dmul_rn(s6[0], kc.c[v][0]);
+#pragma unroll
+      for (int b = 1; b < 6; ++b) acc = __dadd_rn(acc, __dmul_rn(s6[b], kc.c[v][b]));
+      K[(long long)v * N + i] = (T)acc;
+    }
+  }
+}
+
+// sig: device stress [6][N] of type sig_dtype
+static int stress_to_K(gs_sim* s, const void* sig, int sig_dtype, cudaStream_t st) {
+  const int V = s->p.nvariants;
+  const long long N = s->N;
+  KCoef kc;
+  for (int v = 0; v < V; ++v) {
+    const double(*e)[3] = s->p.eigenstrain[v];
+    kc.c[v][0] = e[0][0];
+    kc.c[v][1] = e[0][1] + e[1][0];
+    kc.c[v][2] = e[0][2] + e[2][0];
+    kc.c[v][3] = e[1][1];
+    kc.c[v][4] = e[1][2] + e[2][1];
+    kc.c[v][5] = e[2][2];
+  }
+  if (!s->K) GS_CU(cudaMalloc(&s->K, (size_t)N * V * elt(s)), "cudaMalloc K");
+  long long nb = (N + 255) / 256;
+  if (nb > 148 * 16) nb = 148 * 16;
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  if (sig_dtype == GS_DTYPE_F64) {
+    if (f64)
+      k_stress_to_K<double, double><<<(unsigned)nb, 256, 0, st>>>(static_cast<const double*>(sig), N, V, kc,
+                                                                   static_cast<double*>(s->K));
+    else
+      k_stress_to_K<double, float><<<(unsigned)nb, 256, 0, st>>>(static_cast<const double*>(sig), N, V, kc,
+                                                                  static_cast<float*>(s->K));
+  } else {
+    if (f64)
+      k_stress_to_K<float, double><<<(unsigned)nb, 256, 0, st>>>(static_cast<const float*>(sig), N, V, kc,
+                                                                  static_cast<double*>(s->K));
+    else
+      k_stress_to_K<float, float><<<(unsigned)nb, 256, 0, st>>>(static_cast<const float*>(sig), N, V, kc,
+                                                                 static_cast<float*>(s->K));
+  }
+  GS_CU(cudaGetLastError(), "stress to K");
+  GS_CU(cudaStreamSynchronize(st), "stress to K sync");
+  return GS_OK;
+}
+
 // drop a captured step (its launches hold pointers and tile sizes)
 static void sim_graph_reset(gs_sim* s) {
   if (s->gexec) {
@@ -1063,27 +1123,15 @@ extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, s
     return upload(s, s->defect, host, count, dtype);
   }
   if (nm == "dislocationstress") {
-    // K_p(x) = sigma(x):eps_p from the 6-component form xx xy xz yy yz zz
-    // (the 3x3 remap of src/dynamics_mart.cu:128-150 and the contraction of
-    // DislocationForceInit, :305-321)
     if (count != 6 * N) return gs_set_error(GS_EINVAL, "dislocationstress: %zu values, expected %zu", count, 6 * N);
-    std::vector<double> sig(6 * N);
-    if (dtype == GS_DTYPE_F64)
-      memcpy(sig.data(), host, 6 * N * 8);
-    else
-      for (size_t i = 0; i < 6 * N; ++i) sig[i] = static_cast<const float*>(host)[i];
-    std::vector<double> K(N * V);
-    for (int v = 0; v < V; ++v) {
-      const double(*e)[3] = s->p.eigenstrain[v];
-      for (size_t i = 0; i < N; ++i) {
-        const double xx = sig[0 * N + i], xy = sig[1 * N + i], xz = sig[2 * N + i];
-        const double yy = sig[3 * N + i], yz = sig[4 * N + i], zz = sig[5 * N + i];
-        K[v * N + i] = xx * e[0][0] + xy * (e[0][1] + e[1][0]) + xz * (e[0][2] + e[2][0]) + yy * e[1][1] +
-                       yz * (e[1][2] + e[2][1]) + zz * e[2][2];
-      }
-    }
-    if (!s->K) GS_CU(cudaMalloc(&s->K, N * V * elt(s)), "cudaMalloc K");
-    return upload(s, s->K, K.data(), N * V, GS_DTYPE_F64);
+    const size_t eb = dtype == GS_DTYPE_F64 ? 8 : 4;
+    void* sig = nullptr;
+    GS_CU(cudaMalloc(&sig, 6 * N * eb), "cudaMalloc stress upload");
+    int rc = gs_cuda_check(cudaMemcpy(sig, host, 6 * N * eb, cudaMemcpyHostToDevice), "upload stress");
+    if (rc == GS_OK) rc = gs_cuda_check(cudaDeviceSynchronize(), "upload stress sync");
+    if (rc == GS_OK) rc = stress_to_K(s, sig, dtype, s->own_stream);
+    cudaFree(sig);
+    return rc;
   }
   return gs_set_error(GS_EINVAL, "unknown field '%s'", name);
 }
@@ -2251,4 +2299,52 @@ extern "C" int gs_batch_get_schedule(const gs_batch* b, int group, gs_schedule* 
     return gs_set_error(GS_EINVAL, "gs_batch_get_schedule: bad arguments");
   *sc = b->groups[group]->sched;
   return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device-to-device hand-off between simulations
+// ---------------------------------------------------------------------------
+// The reference passes the stress stage's results to the martensite stage
+// through files (dump stress / defect, then read dislocationstress / defect:
+// scripts/in.precipitate.sh) and remaps them on the host
+// (src/dynamics_mart.cu:128-154, :305-321).  Here they stay on the device.
+extern "C" int gs_sim_take_field(gs_sim* dst, const char* dst_name, gs_sim* src, const char* src_name) {
+  if (!dst || !src || !dst_name || !src_name) return gs_set_error(GS_EINVAL, "gs_sim_take_field: null argument");
+  if (dst->p.nx != src->p.nx || dst->p.ny != src->p.ny || dst->p.nz != src->p.nz)
+    return gs_set_error(GS_EINVAL, "gs_sim_take_field: grids differ");
+  const std::string dn(dst_name), sn(src_name);
+  GS_CU(cudaStreamSynchronize(src->own_stream), "sync source");
+  GS_CU(cudaStreamSynchronize(dst->own_stream), "sync destination");
+  sim_graph_reset(dst);
+  dst->spec_ready = false;
+  const size_t N = (size_t)dst->N;
+  if (dn == "dislocationstress" && sn == "stress") {
+    if (dst->p.model != GS_MODEL_MART || !src->stressbuf)
+      return gs_set_error(GS_EINVAL, "gs_sim_take_field: stress of a stress model into a martensite model");
+    return stress_to_K(dst, src->stressbuf, src->p.dtype, dst->own_stream);
+  }
+  if (dn == "defect" && sn == "defect") {
+    if (dst->p.model != GS_MODEL_MART || !src->defect)
+      return gs_set_error(GS_EINVAL, "gs_sim_take_field: defect of a stress model into a martensite model");
+    if (!dst->defect) GS_CU(cudaMalloc(&dst->defect, N * elt(dst)), "cudaMalloc defect");
+    if (dst->p.dtype == src->p.dtype) {
+      GS_CU(cudaMemcpy(dst->defect, src->defect, N * elt(dst), cudaMemcpyDeviceToDevice), "copy defect");
+    } else {
+      std::vector<char> tmp(N * elt(src));
+      GS_TRY(download(src, src->defect, tmp.data(), N, src->p.dtype));
+      GS_TRY(upload(dst, dst->defect, tmp.data(), N, src->p.dtype));
+    }
+    GS_CU(cudaDeviceSynchronize(), "copy defect sync");
+    return GS_OK;
+  }
+  if (dn == "eta" && sn == "eta") {
+    if (dst->p.nvariants != src->p.nvariants || dst->p.dtype != src->p.dtype)
+      return gs_set_error(GS_EINVAL, "gs_sim_take_field: eta needs the same variants and dtype");
+    GS_CU(cudaMemcpy(dst->eta[dst->cur], src->eta[src->cur], N * elt(dst) * dst->p.nvariants,
+                     cudaMemcpyDeviceToDevice),
+          "copy eta");
+    GS_CU(cudaDeviceSynchronize(), "copy eta sync");
+    return GS_OK;
+  }
+  return gs_set_error(GS_EINVAL, "gs_sim_take_field: cannot take '%s' from '%s'", dst_name, src_name);
 }

@@ -170,6 +170,7 @@ def lib() -> C.CDLL:
         "gs_sim_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(GsSchedule)]),
         "gs_batch_autotune": (C.c_int, [vp, C.c_int, vp]),
         "gs_batch_get_schedule": (C.c_int, [vp, C.c_int, C.POINTER(GsSchedule)]),
+        "gs_sim_take_field": (C.c_int, [vp, C.c_char_p, vp, C.c_char_p]),
         "gs_cores_paint": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, C.c_double, C.c_double,
                                      C.c_double, vp, vp]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
@@ -366,6 +367,9 @@ class Sim:
 
     def use_graph(self, on: bool) -> None:
         check(lib().gs_sim_use_graph(self.h, 1 if on else 0), "use_graph")
+
+    def take_field(self, name: str, src: "Sim", src_name: str) -> None:
+        check(lib().gs_sim_take_field(self.h, name.encode(), src.h, src_name.encode()), f"take_field({name})")
 
 
 class Batch:

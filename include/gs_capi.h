@@ -176,6 +176,13 @@ int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes)
  * z forward, y forward, x contraction, y inverse, update for the
  * martensite step; y passes are absent when the middle axis is 1). */
 int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int max_pass, int* npass);
+/* Hand a field from one simulation to another on the device, replacing the
+ * reference's file hand-off between stages (dump stress/defect, then read
+ * dislocationstress/defect: scripts/in.precipitate.sh; remap on the host,
+ * src/dynamics_mart.cu:128-154,305-321).  Pairs (dst <- src):
+ * "dislocationstress" <- "stress" (stress model into martensite: K_p = sigma:eps_p
+ * formed on the device), "defect" <- "defect", "eta" <- "eta".  Same grid. */
+int gs_sim_take_field(gs_sim* dst, const char* dst_name, gs_sim* src, const char* src_name);
 /* Number of kernel launches issued by the last gs_sim_step call. */
 int64_t gs_sim_launch_count(const gs_sim* s);
 /* Make gs_sim_step replay a captured CUDA graph of two steps (1) or launch

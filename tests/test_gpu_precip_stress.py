@@ -150,3 +150,52 @@ def test_stress_fp32_matches_reference_fixture(gb):
     sg, dg = run_stress(gb, p, d["eta0"])
     assert rel_l2(sg, d["stress"]) < 2e-6
     assert np.array_equal(dg, d["defect"])
+
+
+@pytest.mark.parametrize("dtype", [F64, F32])
+def test_stress_to_mart_handoff_on_device(gb, dtype):
+    """gs_sim_take_field: the stress stage's stress and defect handed to a
+    martensite simulation on the device step it exactly as the same fields
+    downloaded and uploaded through the host."""
+    shape = (16, 12, 8)
+    ps = gb.default_params(gb.GS_MODEL_STRESS, gb.GS_MODE_REFCOMPAT)
+    ps.dtype = dtype
+    ps.nx, ps.ny, ps.nz = shape
+    ps.nvariants = 4
+    t = 0.0063
+    eps = np.array([[[0.01, t, t], [t, -0.004, t], [t, t, 0.002]],
+                    [[0.0, t, -t], [t, 0.01, -t], [-t, -t, 0.0]],
+                    [[0.0, -t, t], [-t, 0.0, -t], [t, -t, 0.01]],
+                    [[-0.01, -t, -t], [-t, 0.0, t], [-t, t, 0.0]]])
+    ps.set_eigenstrain(eps)
+    rng = np.random.default_rng(3)
+    eta_s = rng.uniform(0.0, 1.0, (4,) + shape)
+    st = gb.Sim(ps)
+    pm = gb.default_params(gb.GS_MODEL_MART, gb.GS_MODE_REFCOMPAT)
+    pm.dtype = dtype
+    pm.nx, pm.ny, pm.nz = shape
+    pm.nvariants = 4
+    pm.set_eigenstrain(eps)
+    pm.weight_dislocation = 0.1
+    eta0 = rng.uniform(0.0, 0.1, (4,) + shape)
+    a, b = gb.Sim(pm), gb.Sim(pm)
+    try:
+        st.set_field("eta", eta_s)
+        st.step(1)
+        N = int(np.prod(shape))
+        stress = st.get_field("stress", 6 * N, np.float64 if dtype == F64 else np.float32)
+        defect = st.get_field("defect", N, np.float64 if dtype == F64 else np.float32)
+        a.set_field("eta", eta0)
+        a.set_field("dislocationstress", stress)
+        a.set_field("defect", defect)
+        b.set_field("eta", eta0)
+        b.take_field("dislocationstress", st, "stress")
+        b.take_field("defect", st, "defect")
+        a.step(3)
+        b.step(3)
+        assert np.array_equal(a.eta(), b.eta())
+        assert defect.sum() > 0 and np.abs(stress).max() > 0
+    finally:
+        a.close()
+        b.close()
+        st.close()
