@@ -419,9 +419,16 @@ template <typename T> static const cplx<T>* twp(const gs_sim* s, int which) {
 // itself: the stresses sigma = C:eps have no shear component coupling c with
 // another axis, and the quadratic form Omega^-1(n) keeps its parity.  Axes of
 // extent 1 carry k = 0 only and need no check.
+// the contraction a model's step runs through the table: martensite the
+// variants x variants set, precipitate the (eta_p^2, c) set; -1: none
+static int btab_which(const gs_sim* s) {
+  return s->p.model == GS_MODEL_MART ? 0 : (s->p.model == GS_MODEL_PRECIPITATE ? 2 : -1);
+}
+
 static bool btab_symmetric(const gs_sim* s) {
   ElasticConst<double> ec;
-  build_elastic<double>(s, 0, 1.0, ec);
+  build_elastic<double>(s, btab_which(s), 1.0, ec);
+  if (ec.na != ec.nb) return false;  // square sets only
   const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
   const int nc[3] = {s->n0, s->n1, s->n2};
   for (int c = 0; c < 3; ++c) {
@@ -441,13 +448,17 @@ static bool btab_symmetric(const gs_sim* s) {
 
 // (Re)build the table of the handle's current parameters (martensite only).
 template <typename T> static int build_btab(gs_sim* s, cudaStream_t st) {
-  if (s->p.model != GS_MODEL_MART || s->btab_state == -1) return GS_OK;
+  const int which = btab_which(s);
+  if (which < 0 || s->btab_state == -1) return GS_OK;
   if (!btab_symmetric(s)) {
     s->btab_state = -2;
     return GS_OK;
   }
+  ElasticConst<T> ec;
+  build_elastic<T>(s, which, 1.0 / (double)s->N, ec);
+  s->btab_fields = ec.nb;
   const size_t npt = (size_t)(s->n0 / 2 + 1) * (s->n1 / 2 + 1) * (s->n2 / 2 + 1);
-  const size_t bytes = npt * btab_stride(s->p.nvariants) * sizeof(T);
+  const size_t bytes = npt * btab_stride(ec.nb) * sizeof(T);
   if (s->btab && s->btab_bytes != bytes) {
     cudaFree(s->btab);
     s->btab = nullptr;
@@ -456,8 +467,6 @@ template <typename T> static int build_btab(gs_sim* s, cudaStream_t st) {
     GS_CU(cudaMalloc(&s->btab, bytes), "cudaMalloc B table");
     s->btab_bytes = bytes;
   }
-  ElasticConst<T> ec;
-  build_elastic<T>(s, 0, 1.0 / (double)s->N, ec);
   GS_CU(launch_btab_fill<T>(ec, s->n0, s->n1, s->n2, reinterpret_cast<T*>(s->btab), st), "B table fill");
   GS_CU(cudaStreamSynchronize(st), "B table sync");
   s->btab_state = 1;
@@ -472,7 +481,7 @@ template <typename T> static void set_btab(const gs_sim* s, XArgs<T>& xa) {
   xa.btab = reinterpret_cast<const T*>(s->btab);
   xa.bt_d1 = s->n1 / 2 + 1;
   xa.bt_d2 = s->n2 / 2 + 1;
-  xa.bt_stride = btab_stride(s->p.nvariants);
+  xa.bt_stride = btab_stride(s->btab_fields);
 }
 
 // ---------------------------------------------------------------------------
@@ -523,7 +532,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   xa.G = G;
   xa.tw = twp<T>(s, 3);
   build_elastic<T>(s, which, scale, xa.ec);
-  if (which == 0 && s->btab_state == 1) set_btab<T>(s, xa);
+  if (s->btab_state == 1 && which == btab_which(s) && F == s->btab_fields && G == F) set_btab<T>(s, xa);
   xa.tz_req = s->sched.x_cols;
   GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
   gs_mark(s, st);

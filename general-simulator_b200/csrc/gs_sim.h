@@ -54,6 +54,7 @@ struct gs_sim {
   void* btab = nullptr;
   size_t btab_bytes = 0;
   int btab_state = 0;
+  int btab_fields = 0;  // square size of the tabled contraction
   // batched group: nb simulations of one shape with their own coefficients,
   // fields stored sim after sim; per-sim constants live on the device
   int nb = 1;
