@@ -699,7 +699,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   const int V = p.nvariants;
   const long long N = s->N;
   const bool ref = p.mode == GS_MODE_REFCOMPAT;
-  GS_TRY(precip_potential<T>(s, st));
+  const int F1 = precip_nfields(s);
   T* eta = reinterpret_cast<T*>(s->eta[0]);
   T* c = reinterpret_cast<T*>(s->conc);
   T* mu = reinterpret_cast<T*>(s->mubuf);
@@ -723,11 +723,62 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   la.k1 = (uint32_t)(p.seed >> 32);
   la.sim = p.sim_id;
   la.step = (uint32_t)s->step;
-  GS_CU(launch_precip_local<T>(la, st), "precipitate local terms");
-  gs_mark(s, st);
-  // chain 2: [c, mu, eta_0, g_0, eta_1, g_1, ...] -> k-space update -> [c', eta']
   const int F2 = 2 * V + 2, G2 = V + 1;
   const long long rows = (long long)s->n0 * s->n1;
+  // chain 1 to its y inverse, then one sweep: z C2R of R, local terms, z R2C
+  // of the update fields (k_precip_mid); rows too wide for one block take the
+  // separate passes
+  bool fused = false;
+  {
+    const T* src[GS_MAXF + 1];
+    int sq[GS_MAXF + 1];
+    for (int f = 0; f < V; ++f) {
+      src[f] = eta + (long long)f * N;
+      sq[f] = 1;
+    }
+    if (F1 > V) {
+      src[V] = c;
+      sq[V] = 0;
+    }
+    GS_TRY(elastic_chain_g<T>(s, src, sq, F1, 2, 1.0 / (double)N, s->spec, F1, st));
+    PrecipMidArgs<T> pm;
+    memset(&pm, 0, sizeof(pm));
+    pm.rspec = reinterpret_cast<const cplx<T>*>(s->spec);
+    pm.c = c;
+    pm.eta = eta;
+    pm.dst = reinterpret_cast<cplx<T>*>(s->spec2);
+    pm.nrows = rows;
+    pm.n2 = s->n2;
+    pm.F1 = F1;
+    pm.tw_h = twp<T>(s, 1);
+    pm.tw_n2 = twp<T>(s, 0);
+    pm.loc = la;
+    const cudaError_t e = launch_precip_mid<T>(pm, s->h, st);
+    if (e == cudaSuccess) {
+      fused = true;
+      gs_mark(s, st);
+      s->launches += 1;
+    } else if (e != cudaErrorInvalidConfiguration) {
+      GS_CU(e, "precipitate middle sweep");
+    }
+  }
+  if (!fused) {
+    ZinvArgs<T> zr;
+    memset(&zr, 0, sizeof(zr));
+    zr.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+    for (int f = 0; f < F1; ++f) zr.dst[f] = reinterpret_cast<T*>(s->rbuf) + (long long)f * N;
+    zr.rows_per_field = rows;
+    zr.nrows = rows * F1;
+    zr.tw_h = twp<T>(s, 1);
+    zr.tw_n2 = twp<T>(s, 0);
+    zr.offset_field = -1;
+    GS_CU(launch_zinv<T>(zr, s->h, st), "z inverse (elastic potential)");
+    gs_mark(s, st);
+    GS_CU(launch_precip_local<T>(la, st), "precipitate local terms");
+    gs_mark(s, st);
+    s->launches += 2;
+  }
+  // chain 2: [c, mu, eta_0, g_0, eta_1, g_1, ...] -> k-space update -> [c', eta']
   ZfwdArgs<T> za;
   memset(&za, 0, sizeof(za));
   za.src[0] = c;
@@ -741,8 +792,11 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   za.nrows = rows * F2;
   za.tw_h = twp<T>(s, 1);
   za.tw_n2 = twp<T>(s, 0);
-  GS_CU(launch_zfwd<T>(za, s->h, st), "z forward (update fields)");
-  gs_mark(s, st);
+  if (!fused) {
+    GS_CU(launch_zfwd<T>(za, s->h, st), "z forward (update fields)");
+    gs_mark(s, st);
+    s->launches += 1;
+  }
   YArgs<T> ya;
   ya.spec = reinterpret_cast<cplx<T>*>(s->spec2);
   ya.n0 = s->n0;
@@ -787,7 +841,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   zi.offset = s->mass0 / (double)N;
   GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (c, eta)");
   gs_mark(s, st);
-  s->launches += 3 + (s->n1 > 1 ? 2 : 0);
+  s->launches += 2 + (s->n1 > 1 ? 2 : 0);
   s->step += 1;
   return GS_OK;
 }

@@ -37,6 +37,9 @@ template <typename T>
 cudaError_t launch_btab_fill(const ElasticConst<T>& ec, int n0, int n1, int n2, T* tab, cudaStream_t s);
 template <typename T> cudaError_t launch_zinv(ZinvArgs<T>& a, int H, cudaStream_t s);
 template <typename T> cudaError_t launch_precip_local(PrecipLocalArgs<T>& a, cudaStream_t s);
+template <typename T> struct PrecipMidArgs;
+// returns cudaErrorInvalidConfiguration when a row's lines exceed one block
+template <typename T> cudaError_t launch_precip_mid(PrecipMidArgs<T>& a, int H, cudaStream_t s);
 template <typename T> cudaError_t launch_defect(const T* eta, T* defect, long long N, int V, cudaStream_t s);
 template <typename T> cudaError_t launch_precip_stats(PrecipStatsArgs<T>& a, cudaStream_t s, int* nblocks);
 // returns the number of blocks through nblocks (statistics partial rows)

@@ -23,6 +23,27 @@ template <typename T> struct PrecipLocalArgs {
   uint32_t k0, k1, sim, step;
 };
 
+// mu_c at one cell (s1 = sum_p eta_p^2; rc = R of c when c couples)
+template <typename T>
+__device__ __forceinline__ T precip_mu(const PrecipLocalArgs<T>& a, T c, T s1, T rc, T z) {
+  T mu = a.A[1] * (c - a.c1) + a.A[2] / (T)2 * s1;
+  if (a.c_elastic) mu += a.Es * rc;
+  mu += a.an * z;
+  return mu;
+}
+
+// g_p at one cell (t2, t4: sums of eta_r^2, eta_r^4 over r != p)
+template <typename T>
+__device__ __forceinline__ T precip_g(const PrecipLocalArgs<T>& a, T c, T x, T t2, T t4, T rp, T z) {
+  const T t22 = t2 * t2 - t4;  // sum over ordered pairs i != j, both != p
+  const T x2 = x * x;
+  T gv = (2 * a.A[5] * x + 4 * a.A[6] * x2 * x) * t2 + (2 * a.A[6] * x) * t4 + (2 * a.A[7] * x) * t22 +
+         a.A[2] * x * (c - a.c2) - a.A[3] * x2 * x + a.A[4] * x2 * x2 * x;
+  gv += a.Es * (T)2 * x * rp;
+  gv += a.an * z;
+  return gv;
+}
+
 template <typename T>
 __global__ void k_precip_local(PrecipLocalArgs<T> a) {
   const long long nq = (a.N + 3) >> 2;
@@ -39,10 +60,7 @@ __global__ void k_precip_local(PrecipLocalArgs<T> a) {
         s1 += e * e;
         s2 += e * e * e * e;
       }
-      T mu = a.A[1] * (c - a.c1) + a.A[2] / (T)2 * s1;
-      if (a.c_elastic) mu += a.Es * a.R[(long long)a.V * a.N + i];
-      mu += a.an * zc[j];
-      a.mu[i] = mu;
+      a.mu[i] = precip_mu(a, c, s1, a.c_elastic ? a.R[(long long)a.V * a.N + i] : (T)0, zc[j]);
     }
     for (int p = 0; p < a.V; ++p) {
       T zp[4] = {0, 0, 0, 0};
@@ -58,17 +76,136 @@ __global__ void k_precip_local(PrecipLocalArgs<T> a) {
             t2 += e * e;
             t4 += e * e * e * e;
           }
-        const T t22 = t2 * t2 - t4;  // sum over ordered pairs i != j, both != p
-        const T x = a.eta[p * a.N + i];
-        const T x2 = x * x;
-        T gv = (2 * a.A[5] * x + 4 * a.A[6] * x2 * x) * t2 + (2 * a.A[6] * x) * t4 + (2 * a.A[7] * x) * t22 +
-               a.A[2] * x * (c - a.c2) - a.A[3] * x2 * x + a.A[4] * x2 * x2 * x;
-        gv += a.Es * (T)2 * x * a.R[p * a.N + i];
-        gv += a.an * zp[j];
-        a.g[p * a.N + i] = gv;
+        a.g[p * a.N + i] = precip_g(a, c, a.eta[p * a.N + i], t2, t4, a.R[p * a.N + i], zp[j]);
       }
     }
   }
+}
+
+// The middle of the precipitate step in one sweep over rows: the z C2R of
+// the elastic potentials R (chain 1 after its y inverse), the local terms
+// mu_c and g_p, and the z R2C of the update fields [c, mu, eta_0, g_0, ...]
+// (chain 2).  Shared memory holds, per row, one line per update field in
+// chain-2 order: c and eta_p are loaded into their lines, R_c and R_p are
+// transformed into the lines of mu and g_p, each thread overwrites the R of
+// its own cells with mu and g_p, and every line is transformed to the
+// chain-2 spectrum rows.  R, mu and g never go to HBM.
+template <typename T> struct PrecipMidArgs {
+  const cplx<T>* rspec;  // [F1][rows][H]: R_eta_p^2 (p < V), then R_c
+  const T* c;            // [N]
+  const T* eta;          // [V][N]
+  cplx<T>* dst;          // [2V+2][rows][H]
+  long long nrows;
+  int n2, lr, F1;
+  const cplx<T>* tw_h;
+  const cplx<T>* tw_n2;
+  FastDiv fd_upr;
+  PrecipLocalArgs<T> loc;  // coefficients, noise, V, c_elastic (pointers unused)
+};
+
+template <typename T, int H, int VM>
+__global__ void __launch_bounds__(256) k_precip_mid(PrecipMidArgs<T> a) {
+  using L = Line<T, H>;
+  using V = cplx<T>;
+  constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* smb = reinterpret_cast<V*>(smraw);
+  const int Vn = a.loc.V;
+  const int NL = 2 * Vn + 2;  // lines per row
+  const int n2 = a.n2;
+  const long long N = a.nrows * n2;
+  const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
+  const int rr = line / NL, f2 = line - rr * NL;
+  const long long row = (long long)blockIdx.x * a.lr + rr;
+  const bool rok = rr < a.lr && row < a.nrows;
+  V* sl = smb + line * L::PAD;
+  // R field feeding this line: g_p lines take R_p, the mu line R_c
+  int rf = -1;
+  if (f2 >= 3 && (f2 & 1)) rf = (f2 - 3) >> 1;
+  if (f2 == 1 && a.loc.c_elastic && a.F1 > Vn) rf = Vn;
+  {
+    const bool act = rok && rf >= 0;
+    V r[L::R1];
+    zinv_row<T, H>(a.rspec + ((long long)(rf >= 0 ? rf : 0) * a.nrows + (rok ? row : 0)) * H, act, t, sl, a.tw_h,
+                   a.tw_n2, r);
+    __syncthreads();
+    if (rf >= 0) {
+#pragma unroll
+      for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = r[i];
+    } else if (rok && (f2 == 0 || f2 >= 2)) {  // c or eta_p: the row itself
+      const T* src = f2 == 0 ? a.c : a.eta + (long long)((f2 - 2) >> 1) * N;
+      const V* srow = reinterpret_cast<const V*>(src + row * n2);
+#pragma unroll
+      for (int i = 0; i < L::R1; ++i) sl[L::in_pos(t, i)] = srow[L::in_pos(t, i)];
+    } else {
+#pragma unroll
+      for (int i = 0; i < L::R1; ++i) sl[L::in_pos(t, i)] = mk2((T)0, (T)0);
+    }
+    __syncthreads();
+  }
+  // local terms, one thread per run of CW cells, all fields
+  const int upr = n2 / CW;
+  const int nunits = a.lr * upr;
+  const PrecipLocalArgs<T>& lc = a.loc;
+#pragma unroll 1
+  for (int w = threadIdx.x; w < nunits; w += blockDim.x) {
+    const int ur = (int)a.fd_upr.div((uint32_t)w), u = w - ur * upr;
+    const long long urow = (long long)blockIdx.x * a.lr + ur;
+    if (urow >= a.nrows) continue;
+    const int z0 = u * CW;
+    const long long cell = urow * n2 + z0;
+    T* const lbase = reinterpret_cast<T*>(smb + ur * NL * L::PAD) + z0;
+    auto ln = [lbase](int q) { return lbase + q * (2 * L::PAD); };  // line q of this row (reals)
+    T e[VM][CW], cc[CW];
+#pragma unroll
+    for (int j = 0; j < CW; ++j) cc[j] = ln(0)[j];
+#pragma unroll
+    for (int p = 0; p < VM; ++p)
+      if (p < Vn) {
+#pragma unroll
+        for (int j = 0; j < CW; ++j) e[p][j] = ln(2 + 2 * p)[j];
+      }
+    const bool hi_pair = CW == 2 && (cell & 2);
+    {
+      T zc[4] = {0, 0, 0, 0};
+      if (lc.an != (T)0) normal_quad<T>((uint32_t)(cell >> 2), lc.step, lc.sim, (uint32_t)Vn, lc.k0, lc.k1, zc);
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        T s1 = 0;
+#pragma unroll
+        for (int p = 0; p < VM; ++p)
+          if (p < Vn) s1 += e[p][j] * e[p][j];
+        const T rc = (lc.c_elastic && a.F1 > Vn) ? ln(1)[j] : (T)0;
+        const T zj = CW == 2 ? (hi_pair ? zc[j + 2 < 4 ? j + 2 : 3] : zc[j]) : zc[j];
+        ln(1)[j] = precip_mu(lc, cc[j], s1, rc, zj);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < VM; ++p) {
+      if (p >= Vn) break;
+      T zp[4] = {0, 0, 0, 0};
+      if (lc.an != (T)0) normal_quad<T>((uint32_t)(cell >> 2), lc.step, lc.sim, (uint32_t)p, lc.k0, lc.k1, zp);
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        T t2 = 0, t4 = 0;
+#pragma unroll
+        for (int r = 0; r < VM; ++r)
+          if (r < Vn && r != p) {
+            const T x = e[r][j];
+            t2 += x * x;
+            t4 += x * x * x * x;
+          }
+        const T zj = CW == 2 ? (hi_pair ? zp[j + 2 < 4 ? j + 2 : 3] : zp[j]) : zp[j];
+        ln(3 + 2 * p)[j] = precip_g(lc, cc[j], e[p][j], t2, t4, ln(3 + 2 * p)[j], zj);
+      }
+    }
+  }
+  __syncthreads();
+  V x[L::R1];
+#pragma unroll
+  for (int r = 0; r < L::R1; ++r) x[r] = sl[L::in_pos(t, r)];
+  __syncthreads();
+  zfwd_line<T, H>(x, t, sl, rok ? a.dst + ((long long)f2 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
 }
 
 template <typename T>

@@ -52,6 +52,20 @@ def test_precip_baseline_noise_fp64(gb, orc):
     assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
 
 
+@pytest.mark.parametrize("shape,V", [((8, 12, 2), 4), ((8, 8, 16), 6), ((2, 4, 512), 8)])
+def test_precip_fused_and_separate_passes_fp64(gb, orc, shape, V):
+    """Odd runs of two cells (n2 = 2), the wide-variant instances, and rows
+    too wide for one block (512 cells x 18 update fields), which take the
+    separate z-inverse / local / z-forward passes."""
+    p = precip_base(gb, shape, F64, V=V)
+    c0 = gb.initial_c(p, 12)
+    e0 = gb.initial_eta(p, 13, 0.4)
+    p.noise_amp = 1e-3
+    cr, er = orc.precip_run(p, c0, e0, 2)
+    cg, eg = run_precip(gb, p, c0, e0, 2)
+    assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
+
+
 @pytest.mark.parametrize("V", [1, 2, 3])
 def test_precip_variant_counts(gb, orc, V):
     p = precip_base(gb, (8, 8, 8), F64, V=V)
