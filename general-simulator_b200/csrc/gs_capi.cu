@@ -598,6 +598,19 @@ template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {
   return GS_OK;
 }
 
+// R_p of the current state into R ([V][N]): the chain and the statistics
+// sweep with its R output (the state is not advanced)
+template <typename T> static int mart_potential(gs_sim* s, void* R, cudaStream_t st) {
+  T* in = reinterpret_cast<T*>(s->eta[s->cur]);
+  GS_TRY(elastic_chain<T>(s, in, st));
+  MartArgs<T> ma;
+  fill_mart_args<T>(s, ma, in, nullptr);
+  ma.r_out = reinterpret_cast<T*>(R);
+  int nb = 0;
+  GS_CU(launch_mart_update<T>(ma, s->h, true, st, &nb), "potential pass");
+  return GS_OK;
+}
+
 template <typename T> static int mart_stats(gs_sim* s, gs_stats* o, cudaStream_t st) {
   T* in = reinterpret_cast<T*>(s->eta[s->cur]);
   GS_TRY(elastic_chain<T>(s, in, st));
@@ -1225,6 +1238,26 @@ extern "C" int gs_sim_get_field(gs_sim* s, const char* name, void* host, size_t 
     if (!s->stressbuf) return gs_set_error(GS_EINVAL, "stress: not a stress model");
     if (count != 6 * N) return gs_set_error(GS_EINVAL, "stress: %zu values, expected %zu", count, 6 * N);
     return download(s, s->stressbuf, host, count, dtype);
+  }
+  if (nm == "elastic_potential") {
+    const bool f64 = s->p.dtype == GS_DTYPE_F64;
+    if (s->p.model == GS_MODEL_PRECIPITATE) {
+      const size_t F1 = (size_t)precip_nfields(s);
+      if (count != F1 * N) return gs_set_error(GS_EINVAL, "elastic_potential: %zu values, expected %zu", count, F1 * N);
+      GS_TRY(f64 ? precip_potential<double>(s, s->own_stream) : precip_potential<float>(s, s->own_stream));
+      GS_CU(cudaStreamSynchronize(s->own_stream), "sync");
+      return download(s, s->rbuf, host, count, dtype);
+    }
+    if (s->p.model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "elastic_potential: martensite or precipitate");
+    if (count != (size_t)V * N) return gs_set_error(GS_EINVAL, "elastic_potential: %zu values, expected %zu", count,
+                                                    (size_t)V * N);
+    void* R = nullptr;
+    GS_CU(cudaMalloc(&R, (size_t)V * N * elt(s)), "cudaMalloc potential");
+    int rc = f64 ? mart_potential<double>(s, R, s->own_stream) : mart_potential<float>(s, R, s->own_stream);
+    if (rc == GS_OK) rc = gs_cuda_check(cudaStreamSynchronize(s->own_stream), "sync");
+    if (rc == GS_OK) rc = download(s, R, host, count, dtype);
+    cudaFree(R);
+    return rc;
   }
   return gs_set_error(GS_EINVAL, "unknown field '%s'", name);
 }

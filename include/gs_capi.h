@@ -157,7 +157,8 @@ int gs_sim_destroy(gs_sim* s);
  * the host buffer; count is its number of elements. */
 int gs_sim_set_field(gs_sim* s, const char* name, const void* host, size_t count, int dtype);
 /* Download a field: "eta", "concentration", "stress" [6][N], "defect",
- * "elastic_potential" (R_p of the last step, [F][N]). */
+ * "elastic_potential" (R of the current state: [V][N] for the martensite,
+ * [F][N] for the precipitate, R of eta_p^2 then of c). */
 int gs_sim_get_field(gs_sim* s, const char* name, void* host, size_t count, int dtype);
 /* Per-step scalars read by Calculate: "temperature" (refcompat a1). */
 int gs_sim_set_scalar(gs_sim* s, const char* name, double value);

@@ -320,3 +320,22 @@ def test_fused_z_forward_same_bits_as_separate_pass(gb, dtype, shape):
     finally:
         s.close()
     assert np.array_equal(fused, e)
+
+
+@pytest.mark.parametrize("dtype,tol", [(F64, 1e-11), (F32, 2e-6)])
+def test_elastic_potential_field_matches_oracle(gb, orc, dtype, tol):
+    p = base3d(gb, (16, 12, 8), dtype)
+    eta0 = gb.initial_eta(p, 51, 0.5)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    s = gb.Sim(p)
+    try:
+        s.set_field("eta", eta0)
+        s.step(2)
+        eta = s.eta(np.float64)
+        R = s.get_field("elastic_potential", eta.size, np.float64).reshape(eta.shape)
+        # the state is not advanced by reading the potential
+        assert np.array_equal(s.eta(np.float64), eta)
+    finally:
+        s.close()
+    assert rel_l2(R, orc.mart_potential(p, eta)) < tol
