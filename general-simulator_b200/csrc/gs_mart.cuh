@@ -170,7 +170,9 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
   }
   Neu acc[STATS ? ACC_N : 1];
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
-  const long long N = a.nrows * n2;
+  // one simulation's field set holds fewer than 2^31 values (256 x 256 x
+  // 512 x 8 at most), so cell offsets are 32-bit
+  const int N = (int)(a.nrows * n2);
   const int upr = n2 / CW;
   const int nunits = a.lr * upr;
   // unit w -> (row rr, run u); runs of one row are consecutive so
@@ -178,21 +180,20 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
 #pragma unroll 1
   for (int w = threadIdx.x; w < nunits; w += blockDim.x) {
     const int rr = (int)a.fd_upr.div((uint32_t)w), u = w - rr * upr;
-    const long long row = (long long)blockIdx.x * a.lr + rr;
+    const int row = blockIdx.x * a.lr + rr;
     if (row >= a.nrows) continue;
-    const int x = (int)a.fd_n1.div((uint32_t)row), y = (int)(row - (long long)x * n1);
-    const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
-    const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
+    const int x = (int)a.fd_n1.div((uint32_t)row), y = row - x * n1;
     const int z0 = u * CW;
-    const long long rowb = row * n2, cell = rowb + z0;
+    const int cell = row * n2 + z0;
     // neighbour offsets relative to the run, the same for every variant
-    const long long oxp = ((long long)xp * n1 + y) * n2 + z0 - cell, oxm = ((long long)xm * n1 + y) * n2 + z0 - cell;
-    const long long oyp = ((long long)x * n1 + yp) * n2 + z0 - cell, oym = ((long long)x * n1 + ym) * n2 + z0 - cell;
+    const int sx = n1 * n2;
+    const int oxp = x + 1 == n0 ? -(n0 - 1) * sx : sx, oxm = x == 0 ? (n0 - 1) * sx : -sx;
+    const int oyp = y + 1 == n1 ? -(n1 - 1) * n2 : n2, oym = y == 0 ? (n1 - 1) * n2 : -n2;
     const int ozl = (z0 == 0 ? n2 - 1 : z0 - 1) - z0, ozr = (z0 + CW == n2 ? 0 : z0 + CW) - z0;
     T e[VM][CW];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
-      if (p < Vn) ldv<CW>(a.eta_in + (long long)p * N + cell, e[p]);
+      if (p < Vn) ldv<CW>(a.eta_in + p * N + cell, e[p]);
     T s2[CW], s4[CW], pr[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
 #pragma unroll
     for (int q = 0; q < VM; ++q) {
       if (q >= Vn) break;
-      const T* eq = a.eta_in + (long long)q * N + cell;
+      const T* eq = a.eta_in + q * N + cell;
       T vxp[CW], vxm[CW], vyp[CW], vym[CW];
       ldv<CW>(eq + oxp, vxp);
       ldv<CW>(eq + oxm, vxm);
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       T Kq[CW];
 #pragma unroll
       for (int j = 0; j < CW; ++j) Kq[j] = 0;
-      if (mc.has_K) ldv<CW>(a.K + (long long)q * N + cell, Kq);
+      if (mc.has_K) ldv<CW>(a.K + q * N + cell, Kq);
       T xi[4] = {0, 0, 0, 0};
       if (!STATS && mc.noise != (T)0)
         normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
@@ -282,8 +283,8 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
           acc[ACC_FDISL].add((double)lin);
         }
       }
-      if (!STATS) stv<CW>(a.eta_out + (long long)q * N + cell, out);
-      if (!BATCH && a.r_out) stv<CW>(a.r_out + (long long)q * N + cell, rv);
+      if (!STATS) stv<CW>(a.eta_out + q * N + cell, out);
+      if (!BATCH && a.r_out) stv<CW>(a.r_out + q * N + cell, rv);
       if (FUSE) {
         T* sq = const_cast<T*>(Rq);
 #pragma unroll
