@@ -187,3 +187,23 @@ def test_cores_paint_matches_oracle_large(gb, orc):
     oe, oc = orc.cores_paint(grid, V, centers.tolist(), variants.tolist(), r, 0.2, 0.44)
     assert np.array_equal(eta, oe) and np.array_equal(conc, oc)
     assert (eta.sum(axis=0) > 1).any()  # overlaps of different variants are exercised
+
+
+def test_time_calculate_script(gsi, tmp_path):
+    """scripts/in.time_calculate of the reference: backquoted shell output in
+    variables and expressions ({x2-x1} is the seconds slept)."""
+    text = """set log off
+print `date`
+:x1=`date +%s`
+shell sleep 1
+print `date`
+:x2=`date +%s`
+print since time point {x1} to time point {x2}, {x2-x1} seconds have passed.
+"""
+    out = run_script(gsi, tmp_path, "in.time_calculate", text)
+    import re
+
+    m = re.search(r"since time point (\d+) to time point (\d+), (\d+) seconds have passed\.", out)
+    assert m, out
+    x1, x2, d = map(int, m.groups())
+    assert d == x2 - x1 and 1 <= d <= 3
