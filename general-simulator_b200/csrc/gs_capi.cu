@@ -826,8 +826,13 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   xa.n1 = s->n1;
   xa.n2 = s->n2;
   xa.h = s->h;
-  xa.F = F2;
-  xa.G = G2;
+  // one (field, force) pair per grid-z slice, written to the chain-1
+  // spectrum buffer (free by now): a slice's output rows overlap another
+  // slice's input rows, so the update is not done in place
+  xa.out = reinterpret_cast<cplx<T>*>(s->spec);
+  xa.F = 2;
+  xa.G = 1;
+  xa.nsim = G2;
   xa.tw = twp<T>(s, 3);
   xa.pu.V = V;
   xa.pu.mass_proj = p.mass_projection;
@@ -839,11 +844,13 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   for (int c3 = 0; c3 < 3; ++c3) xa.pu.ktab[c3] = reinterpret_cast<const T*>(s->ktab) + s->ktab_off[c3];
   GS_CU(launch_xprecip<T>(xa, st), "x pass (k-space update)");
   gs_mark(s, st);
-  GS_CU(launch_ypass<T>(ya, s->n1, G2, 1, st), "y inverse (update fields)");
+  YArgs<T> yo = ya;
+  yo.spec = reinterpret_cast<cplx<T>*>(s->spec);
+  GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st), "y inverse (update fields)");
   if (s->n1 > 1) gs_mark(s, st);
   ZinvArgs<T> zi;
   memset(&zi, 0, sizeof(zi));
-  zi.spec = reinterpret_cast<const cplx<T>*>(s->spec2);
+  zi.spec = reinterpret_cast<const cplx<T>*>(s->spec);
   zi.dst[0] = c;
   for (int v = 0; v < V; ++v) zi.dst[1 + v] = eta + (long long)v * N;
   zi.rows_per_field = rows;
@@ -1003,7 +1010,8 @@ extern "C" int gs_sim_create(const gs_params* p, gs_sim** out) {
   } else if (p->model == GS_MODEL_PRECIPITATE) {
     const int F1 = precip_nfields(s);
     if ((rc = dalloc(&s->conc, fb, "concentration")) != GS_OK) return fail(rc);
-    if ((rc = dalloc(&s->spec, fb * F1, "spectrum")) != GS_OK) return fail(rc);
+    // chain 1 (F1 fields), then the V + 1 outputs of the k-space update
+    if ((rc = dalloc(&s->spec, fb * (V + 1), "spectrum")) != GS_OK) return fail(rc);
     if ((rc = dalloc(&s->rbuf, fb * F1, "elastic potentials")) != GS_OK) return fail(rc);
     if ((rc = dalloc(&s->mubuf, fb * (V + 1), "local terms")) != GS_OK) return fail(rc);
     if ((rc = dalloc(&s->spec2, fb * (2 * V + 2), "update spectra")) != GS_OK) return fail(rc);

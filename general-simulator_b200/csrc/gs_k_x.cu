@@ -20,6 +20,7 @@ template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s) 
 }
 
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s) {
+  if (a.F == 2 && a.G == 1 && a.nsim > 1) return launch_x_class<T, 2, 1, PrecipPairOp>(a, s);  // pair slices
   if (a.F <= 10 && a.G <= 5) return launch_x_class<T, 10, 5, PrecipOp>(a, s);
   return launch_x_class<T, 18, 9, PrecipOp>(a, s);
 }

@@ -458,6 +458,30 @@ struct PrecipOp {
   }
 };
 
+// The same update, one (field, force) pair per grid-z slice: slice 0 is
+// (c, mu) -> c', slice 1 + p is (eta_p, g_p) -> eta_p' (the chain-2 fields
+// are stored pair after pair, its outputs one after another, so the batched
+// slice offsets of the x pass address them directly).  Lighter blocks than
+// one block over all 2V + 2 fields.
+struct PrecipPairOp {
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    const PrecipUpd<T>& u = a.pu;
+    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+#pragma unroll
+    for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
+    if (blockIdx.z == 0) {
+      const T ic = u.scale / ((T)1 + u.dtM * u.kc * K * K);
+      out[0] = (in[0] - in[1] * (u.dtM * K)) * ic;
+      if (u.mass_proj && ix == 0 && iy == 0 && iz == 0) out[0] = mk2((T)0, (T)0);
+    } else {
+      const T ie = u.scale / ((T)1 + u.dtL * u.ke * K);
+      out[0] = (in[0] - in[1] * u.dtL) * ie;
+    }
+  }
+};
+
 // threads per block of the x pass for a field-count class (FM, GM)
 template <int FM, int GM> struct XBounds {
   static constexpr int G = FM > GM ? FM : GM;
