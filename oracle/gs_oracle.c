@@ -921,3 +921,173 @@ int or_cores_marked(int nx, int ny, int nz, int ncores, const int* centers, doub
     if (core_hit(i, j, k, centers[3 * q], centers[3 * q + 1], centers[3 * q + 2], nx, ny, nz, r * r)) return 1;
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* adjoint of the precipitate run (baseline mode)                      */
+/* ------------------------------------------------------------------ */
+/* u <- Re IFFT(S(k) FFT(u)) / N for a real field, S real and even: the
+ * semi-implicit factors are such symbols, so each is its own transpose. */
+enum { SYM_DC, SYM_KDC, SYM_K2DC, SYM_DE, SYM_KDE };
+static void apply_symbol(const gs_params* p, int sym, const double* u, double* out) {
+  const int n0 = p->nx, n1 = p->ny, n2 = p->nz;
+  const long N = (long)n0 * n1 * n2;
+  const int ref = p->mode == GS_MODE_REFCOMPAT;
+  const double dt = p->dt, M = p->mobility_c, L = p->mobility_eta;
+  cplx* w = (cplx*)malloc(sizeof(cplx) * N);
+  for (long i = 0; i < N; ++i) w[i] = u[i];
+  or_fft3((double*)w, n0, n1, n2, -1);
+#pragma omp parallel for schedule(static)
+  for (long idx = 0; idx < N; ++idx) {
+    int x = (int)(idx / ((long)n1 * n2)), y = (int)((idx / n2) % n1), z = (int)(idx % n2);
+    int mx = ref ? fold_ref(x, n0) : fold_base(x, n0);
+    int my = ref ? fold_ref(y, n1) : fold_base(y, n1);
+    int mz = ref ? fold_ref(z, n2) : fold_base(z, n2);
+    const double K = ksym(p, mx, my, mz);
+    const double Dc = 1.0 / (1.0 + dt * M * p->kappa_c * K * K), De = 1.0 / (1.0 + dt * L * p->kappa_eta * K);
+    double s = sym == SYM_DC ? Dc : sym == SYM_KDC ? K * Dc : sym == SYM_K2DC ? K * K * Dc : sym == SYM_DE ? De : K * De;
+    w[idx] *= s;
+  }
+  or_fft3((double*)w, n0, n1, n2, +1);
+  for (long i = 0; i < N; ++i) out[i] = creal(w[i]) / (double)N;
+  free(w);
+}
+
+/* J = <seed_c, c_T> + <seed_eta, eta_T> of the run from (c0, eta0); the
+ * gradients with respect to c0, eta0 and theta = (kappa_c, kappa_eta,
+ * coef[1..7]).  One step is c' = Dc (c - dt M K mu), eta_p' = De (eta_p -
+ * dt L g_p) in k space, mu = A1 (c - c1) + A2/2 sum eta^2 + Es R_c,
+ * g_p = dh/deta_p + 2 Es eta_p R_p, R = B * (eta^2, c); the additive noise
+ * drops out.  The transposes: Dc, K, De are real even symbols (their own
+ * transposes) and B is symmetric, so R's transpose is the same convolution. */
+int or_precip_adjoint(const gs_params* p, const double* c0, const double* eta0, int nsteps, const double* seed_c,
+                      const double* seed_eta, double* grad_c0, double* grad_eta0, double* grads) {
+  const int V = p->nvariants;
+  const long N = (long)p->nx * p->ny * p->nz;
+  const long S = N * (V + 1);
+  double* st = (double*)malloc(sizeof(double) * S * (nsteps + 1));
+  memcpy(st, c0, sizeof(double) * N);
+  memcpy(st + N, eta0, sizeof(double) * N * V);
+  for (int n = 0; n < nsteps; ++n) {
+    memcpy(st + (n + 1) * S, st + n * S, sizeof(double) * S);
+    or_precip_run(p, st + (n + 1) * S, st + (n + 1) * S + N, 1, n);
+  }
+  const double dt = p->dt, M = p->mobility_c, L = p->mobility_eta, Es = precip_escale(p);
+  const double* A = p->coef;
+  const int ce = p->c_elastic && p->mode != GS_MODE_REFCOMPAT;
+  double* lc = (double*)malloc(sizeof(double) * N);
+  double* le = (double*)malloc(sizeof(double) * N * V);
+  double* ac = (double*)malloc(sizeof(double) * N);
+  double* dmu = (double*)malloc(sizeof(double) * N);
+  double* ae = (double*)malloc(sizeof(double) * N * V);
+  double* dg = (double*)malloc(sizeof(double) * N * V);
+  double* tmp = (double*)malloc(sizeof(double) * N);
+  double* R = (double*)malloc(sizeof(double) * N * (V + 1));
+  double* dR = (double*)malloc(sizeof(double) * N * (V + 1));
+  double* dP = (double*)malloc(sizeof(double) * N * (V + 1));
+  memcpy(lc, seed_c, sizeof(double) * N);
+  memcpy(le, seed_eta, sizeof(double) * N * V);
+  for (int k = 0; k < 9; ++k) grads[k] = 0;
+  for (int n = nsteps - 1; n >= 0; --n) {
+    const double* c = st + n * S;
+    const double* eta = c + N;
+    const double* c1 = st + (n + 1) * S;
+    const double* eta1 = c1 + N;
+    /* kappa gradients: dc'/dkappa_c = -dt M K^2 Dc c', deta'/dkappa_eta = -dt L K De eta' */
+    apply_symbol(p, SYM_K2DC, c1, tmp);
+    for (long i = 0; i < N; ++i) grads[0] += -dt * M * lc[i] * tmp[i];
+    for (int v = 0; v < V; ++v) {
+      apply_symbol(p, SYM_KDE, eta1 + v * N, tmp);
+      for (long i = 0; i < N; ++i) grads[1] += -dt * L * le[v * N + i] * tmp[i];
+    }
+    apply_symbol(p, SYM_DC, lc, ac);
+    apply_symbol(p, SYM_KDC, lc, dmu);
+    for (long i = 0; i < N; ++i) dmu[i] *= -dt * M;
+    for (int v = 0; v < V; ++v) {
+      apply_symbol(p, SYM_DE, le + v * N, ae + v * N);
+      for (long i = 0; i < N; ++i) dg[v * N + i] = -dt * L * ae[v * N + i];
+    }
+    int F;
+    precip_potential(p, c, eta, R, &F);
+    for (int v = 0; v < V; ++v)
+      for (long i = 0; i < N; ++i) dR[v * N + i] = 2.0 * Es * eta[v * N + i] * dg[v * N + i];
+    if (F > V)
+      for (long i = 0; i < N; ++i) dR[(long)V * N + i] = ce ? Es * dmu[i] : 0.0;
+    elastic_potential(p, 2, dR, F, dP, F);
+    double g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0, g6 = 0, g7 = 0;
+    for (long i = 0; i < N; ++i) {
+      double e[GS_MAX_V], s2 = 0;
+      for (int v = 0; v < V; ++v) {
+        e[v] = eta[v * N + i];
+        s2 += e[v] * e[v];
+      }
+      double nlc = ac[i] + A[1] * dmu[i] + (F > V ? dP[(long)V * N + i] : 0.0);
+      g1 += dmu[i] * (c[i] - p->c1);
+      g2 += dmu[i] * s2 / 2.0;
+      for (int pp = 0; pp < V; ++pp) {
+        const double x = e[pp], d = dg[pp * N + i];
+        double t2 = 0, t4 = 0;
+        for (int j = 0; j < V; ++j)
+          if (j != pp) {
+            t2 += e[j] * e[j];
+            t4 += e[j] * e[j] * e[j] * e[j];
+          }
+        const double t22 = t2 * t2 - t4;
+        nlc += A[2] * x * d;
+        g2 += d * x * (c[i] - p->c2);
+        g3 += -d * x * x * x;
+        g4 += d * x * x * x * x * x;
+        g5 += d * 2.0 * x * t2;
+        g6 += d * (4.0 * x * x * x * t2 + 2.0 * x * t4);
+        g7 += d * 2.0 * x * t22;
+      }
+      lc[i] = nlc;
+      for (int q = 0; q < V; ++q) {
+        const double x = e[q];
+        double t2 = 0, t4 = 0;
+        for (int j = 0; j < V; ++j)
+          if (j != q) {
+            t2 += e[j] * e[j];
+            t4 += e[j] * e[j] * e[j] * e[j];
+          }
+        const double t22 = t2 * t2 - t4;
+        double v = ae[q * N + i] + A[2] * x * dmu[i];
+        v += ((2.0 * A[5] + 12.0 * A[6] * x * x) * t2 + 2.0 * A[6] * t4 + 2.0 * A[7] * t22 + A[2] * (c[i] - p->c2) -
+              3.0 * A[3] * x * x + 5.0 * A[4] * x * x * x * x) *
+             dg[q * N + i];
+        for (int pp = 0; pp < V; ++pp)
+          if (pp != q) {
+            const double y = e[pp];
+            double u2 = 0;
+            for (int j = 0; j < V; ++j)
+              if (j != pp) u2 += e[j] * e[j];
+            v += ((2.0 * A[5] * y + 4.0 * A[6] * y * y * y) * 2.0 * x + 2.0 * A[6] * y * 4.0 * x * x * x +
+                  2.0 * A[7] * y * 4.0 * x * (u2 - x * x)) *
+                 dg[pp * N + i];
+          }
+        v += 2.0 * Es * R[q * N + i] * dg[q * N + i] + 2.0 * x * dP[q * N + i];
+        le[q * N + i] = v;
+      }
+    }
+    grads[2] += g1;
+    grads[3] += g2;
+    grads[4] += g3;
+    grads[5] += g4;
+    grads[6] += g5;
+    grads[7] += g6;
+    grads[8] += g7;
+  }
+  if (grad_c0) memcpy(grad_c0, lc, sizeof(double) * N);
+  if (grad_eta0) memcpy(grad_eta0, le, sizeof(double) * N * V);
+  free(st);
+  free(lc);
+  free(le);
+  free(ac);
+  free(dmu);
+  free(ae);
+  free(dg);
+  free(tmp);
+  free(R);
+  free(dR);
+  free(dP);
+  return 0;
+}

@@ -55,6 +55,12 @@ int or_mart_adjoint(const gs_params* p, const double* eta0, int nsteps, const do
                     double e_target, const double* seed, double seed_e, double* grads, double* grad_eta0,
                     double* loss_out);
 
+/* Adjoint of the precipitate run (baseline mode): J = <seed_c, c_T> +
+ * <seed_eta, eta_T>; grad_c0, grad_eta0 (may be NULL) and grads[9] =
+ * dJ/d(kappa_c, kappa_eta, coef[1..7]). */
+int or_precip_adjoint(const gs_params* p, const double* c0, const double* eta0, int nsteps, const double* seed_c,
+                      const double* seed_eta, double* grad_c0, double* grad_eta0, double* grads);
+
 /* Precipitate: advance c (N) and eta ([V][N]) nsteps. */
 int or_precip_run(const gs_params* p, double* c, double* eta, int nsteps, int64_t step0);
 int or_precip_stats(const gs_params* p, const double* c, const double* eta, gs_stats* st);

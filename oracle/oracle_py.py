@@ -45,6 +45,7 @@ def lib() -> C.CDLL:
         L.or_cores_paint.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, C.c_double, C.c_double,
                                      C.c_double, fp, fp]
         L.or_cores_marked.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.or_precip_adjoint.argtypes = [P, dp, dp, C.c_int, dp, dp, dp, dp, dp]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         _lib = L
@@ -197,3 +198,16 @@ def cores_place(shape, V, ncores, radius, method, rand):
             centers.append((nx // 2, ny // 2, nz // ncores // 2 + nx // ncores * cn))
             variants.append(cn % V)
     return centers, variants
+
+
+def precip_adjoint(p, c0, eta0, nsteps, seed_c, seed_eta):
+    """grads[9] (kappa_c, kappa_eta, coef[1..7]), dJ/dc0, dJ/deta0 of
+    J = <seed_c, c_T> + <seed_eta, eta_T> (baseline precipitate run)."""
+    c = _f64(c0)
+    e = _f64(eta0)
+    gc = np.zeros_like(c)
+    ge = np.zeros_like(e)
+    g = np.zeros(9)
+    lib().or_precip_adjoint(C.byref(p), _dp(c), _dp(e), nsteps, _dp(_f64(seed_c)), _dp(_f64(seed_eta)), _dp(gc),
+                            _dp(ge), _dp(g))
+    return g, gc, ge
