@@ -314,6 +314,46 @@ def extra_ensemble(steps: int = 100, total_steps: int = 2000) -> dict:
             "per_shape_ms_per_step": per_shape, "timed_steps": steps}
 
 
+def extra_configs() -> dict:
+    """The other workloads of the step, timed the same way: the 2D FP64
+    martensite (128^2, 2 variants, 1000-step runs) and the 3D precipitate
+    (256^3, concentration + 4 variants, FP32, semi-implicit, FP64 mass
+    projection) with its relative mass drift over the timed steps."""
+    import torch
+
+    import gs_b200 as gb
+
+    out = {}
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        p = gb.mart2d_params(128, dtype=gb.GS_DTYPE_F64)
+        sim = gb.Sim(p)
+        sim.set_field("eta", gb.initial_eta(p, 0, 0.01))
+        sim.use_graph(True)
+        sim.step(10, sh)
+        steps = 1000
+        ms = _timed(stream, lambda: sim.step(steps, sh)) / steps
+        sim.close()
+        out["mart2d_fp64_128"] = {"ms_per_step": ms, "cell_updates_per_s": p.ncells * 1e3 / ms, "steps": steps,
+                                  "note": "graph replay; a 1000-step run of this workload takes 1000 x ms_per_step"}
+        p = gb.precip3d_params(256, dtype=gb.GS_DTYPE_F32)
+        sim = gb.Sim(p)
+        sim.set_field("concentration", gb.initial_c(p, 2))
+        sim.set_field("eta", gb.initial_eta(p, 3, 0.01))
+        sim.step(3, sh)
+        m0 = sim.stats(sh)["mass"]
+        steps = 20
+        ms = _timed(stream, lambda: sim.step(steps, sh)) / steps
+        m1 = sim.stats(sh)["mass"]
+        launches = sim.launch_count()
+        sim.close()
+        out["precipitate_fp32_256"] = {"ms_per_step": ms, "cell_updates_per_s": p.ncells * 1e3 / ms, "steps": steps,
+                                       "launches_per_step": launches / steps,
+                                       "mass_drift_relative": abs(m1 - m0) / abs(m0)}
+    return out
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: the FP64 oracle on the host cores
 # ---------------------------------------------------------------------------
@@ -485,6 +525,7 @@ def run_ours(args, ws, rank, local):
         extras["comparator"] = extra_comparator(n, ms / args.steps)
         extras["adjoint"] = extra_adjoint()
         extras["ensemble"] = extra_ensemble()
+        extras["other_workloads"] = extra_configs()
     cpu = None
     if ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(n, args.cpu_seconds)

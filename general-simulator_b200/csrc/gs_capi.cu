@@ -16,6 +16,7 @@
 
 #include "../../include/gs_capi.h"
 #include "gs_adjoint.cuh"
+#include "gs_padj.cuh"
 #include "gs_launch.h"
 #include "gs_mart.cuh"
 #include "gs_precip.cuh"
@@ -2451,4 +2452,281 @@ extern "C" int gs_sim_take_field(gs_sim* dst, const char* dst_name, gs_sim* src,
     return GS_OK;
   }
   return gs_set_error(GS_EINVAL, "gs_sim_take_field: cannot take '%s' from '%s'", dst_name, src_name);
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the precipitate run (every state kept)
+// ---------------------------------------------------------------------------
+// The reverse sweep per step: one spectral pass over the pairs (lambda',
+// state') gives D lambda', K D lambda' and K^a D state' of every field
+// (PrecipAdjOp), the first pointwise sweep the local-term adjoints and the
+// elastic sources dR, the elastic chain B * dR, the second sweep the new
+// lambda; R of the state comes from its own chain.  gs_padj.cuh has the
+// formulas; the oracle's or_precip_adjoint states the same in FP64.
+struct gs_padjoint {
+  gs_sim* s = nullptr;
+  int nsteps = 0, F1 = 0;
+  void* states = nullptr;  // [nsteps + 1][V + 1][N] (c, then eta)
+  void* lam[2] = {nullptr, nullptr};
+  void* Y = nullptr;   // [3 (V + 1)] spectra
+  void* Zr = nullptr;  // [3 (V + 1)][N]
+  void* dP = nullptr;  // [F1][N]
+  double* gsum = nullptr;  // [nsteps][PADJ_N]
+  bool forward_done = false;
+  size_t bytes = 0;
+};
+
+static void free_padjoint(gs_padjoint* a) {
+  if (!a) return;
+  cudaDeviceSynchronize();
+  for (void* q : {a->states, a->lam[0], a->lam[1], a->Y, a->Zr, a->dP, (void*)a->gsum})
+    if (q) cudaFree(q);
+  if (a->s) free_sim(a->s);
+  delete a;
+}
+
+extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjoint** out) {
+  if (!p || !out) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_create: null argument");
+  *out = nullptr;
+  if (p->model != GS_MODEL_PRECIPITATE) return gs_set_error(GS_EINVAL, "precipitate adjoint: precipitate model only");
+  if (p->mode != GS_MODE_BASELINE) return gs_set_error(GS_ENOTSUP, "precipitate adjoint: baseline mode only");
+  if (nsteps < 1) return gs_set_error(GS_EINVAL, "precipitate adjoint: nsteps %d", nsteps);
+  gs_padjoint* a = new gs_padjoint();
+  int rc = gs_sim_create(p, &a->s);
+  if (rc != GS_OK) {
+    delete a;
+    return rc;
+  }
+  a->nsteps = nsteps;
+  a->F1 = precip_nfields(a->s);
+  const int V = p->nvariants;
+  const size_t fb = (size_t)a->s->N * elt(a->s);
+  auto get = [&](void** q, size_t b, const char* what) {
+    const int r = dalloc(q, b, what);
+    if (r == GS_OK) a->bytes += b;
+    return r;
+  };
+  if ((rc = get(&a->states, fb * (V + 1) * (nsteps + 1), "adjoint states")) != GS_OK ||
+      (rc = get(&a->lam[0], fb * (V + 1), "adjoint lambda")) != GS_OK ||
+      (rc = get(&a->lam[1], fb * (V + 1), "adjoint lambda")) != GS_OK ||
+      (rc = get(&a->Y, fb * 3 * (V + 1), "adjoint spectra")) != GS_OK ||
+      (rc = get(&a->Zr, fb * 3 * (V + 1), "adjoint fields")) != GS_OK ||
+      (rc = get(&a->dP, fb * a->F1, "adjoint elastic sources")) != GS_OK ||
+      (rc = get(reinterpret_cast<void**>(&a->gsum), (size_t)nsteps * PADJ_N * sizeof(double), "adjoint sums")) !=
+          GS_OK) {
+    free_padjoint(a);
+    return rc;
+  }
+  *out = a;
+  return GS_OK;
+}
+
+extern "C" int gs_precip_adjoint_destroy(gs_padjoint* a) {
+  free_padjoint(a);
+  return GS_OK;
+}
+
+extern "C" size_t gs_precip_adjoint_device_bytes(const gs_padjoint* a) { return a ? a->bytes : 0; }
+
+extern "C" int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
+                                         void* eta_final, void* stream) {
+  if (!a || !c0 || !eta0) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: null argument");
+  gs_sim* s = a->s;
+  const int V = s->p.nvariants;
+  const size_t N = (size_t)s->N, fb = N * elt(s);
+  GS_TRY(gs_sim_set_field(s, "concentration", c0, N, dtype));
+  GS_TRY(gs_sim_set_field(s, "eta", eta0, N * V, dtype));
+  cudaStream_t st = pick_stream(s, stream);
+  s->step = 0;
+  char* S = static_cast<char*>(a->states);
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  for (int n = 0; n <= a->nsteps; ++n) {
+    char* dst = S + (size_t)n * fb * (V + 1);
+    GS_CU(cudaMemcpyAsync(dst, s->conc, fb, cudaMemcpyDeviceToDevice, st), "keep state");
+    GS_CU(cudaMemcpyAsync(dst + fb, s->eta[0], fb * V, cudaMemcpyDeviceToDevice, st), "keep state");
+    if (n < a->nsteps) GS_TRY(f64 ? precip_step<double>(s, st) : precip_step<float>(s, st));
+  }
+  GS_CU(cudaStreamSynchronize(st), "forward sync");
+  a->forward_done = true;
+  if (c_final) GS_TRY(download(s, s->conc, c_final, N, dtype));
+  if (eta_final) GS_TRY(download(s, s->eta[0], eta_final, N * V, dtype));
+  return GS_OK;
+}
+
+template <typename T> static int padj_backward(gs_padjoint* a, cudaStream_t st, int* cur) {
+  gs_sim* s = a->s;
+  const gs_params& p = s->p;
+  const int V = p.nvariants, F1 = a->F1, FV = V + 1;
+  const long long N = s->N, rows = (long long)s->n0 * s->n1;
+  const size_t fstate = (size_t)N * FV;
+  const T* S = reinterpret_cast<const T*>(a->states);
+  T* Zr = reinterpret_cast<T*>(a->Zr);
+  int c = 0;
+  for (int n = a->nsteps - 1; n >= 0; --n) {
+    const T* st0 = S + (size_t)n * fstate;
+    const T* st1 = S + (size_t)(n + 1) * fstate;
+    const T* lin = reinterpret_cast<const T*>(a->lam[c]);
+    T* lout = reinterpret_cast<T*>(a->lam[c ^ 1]);
+    // spectral pass over the pairs (lambda', state')
+    ZfwdArgs<T> za;
+    memset(&za, 0, sizeof(za));
+    for (int f = 0; f < FV; ++f) {
+      za.src[2 * f] = lin + (size_t)f * N;
+      za.src[2 * f + 1] = st1 + (size_t)f * N;
+    }
+    za.dst = reinterpret_cast<cplx<T>*>(s->spec2);
+    za.rows_per_field = rows;
+    za.nrows = rows * 2 * FV;
+    za.tw_h = twp<T>(s, 1);
+    za.tw_n2 = twp<T>(s, 0);
+    GS_CU(launch_zfwd<T>(za, s->h, st), "adjoint z forward");
+    YArgs<T> ya;
+    ya.spec = reinterpret_cast<cplx<T>*>(s->spec2);
+    ya.n0 = s->n0;
+    ya.n1 = s->n1;
+    ya.h = s->h;
+    ya.tw = twp<T>(s, 2);
+    GS_CU(launch_ypass<T>(ya, s->n1, 2 * FV, -1, st), "adjoint y forward");
+    XArgs<T> xa;
+    memset(&xa, 0, sizeof(xa));
+    xa.in = reinterpret_cast<cplx<T>*>(s->spec2);
+    xa.out = reinterpret_cast<cplx<T>*>(a->Y);
+    xa.n0 = s->n0;
+    xa.n1 = s->n1;
+    xa.n2 = s->n2;
+    xa.h = s->h;
+    xa.F = 2;
+    xa.G = 3;
+    xa.nsim = FV;
+    xa.tw = twp<T>(s, 3);
+    xa.pu.V = V;
+    xa.pu.dtM = (T)(p.dt * p.mobility_c);
+    xa.pu.dtL = (T)(p.dt * p.mobility_eta);
+    xa.pu.kc = (T)p.kappa_c;
+    xa.pu.ke = (T)p.kappa_eta;
+    xa.pu.scale = (T)(1.0 / (double)N);
+    for (int c3 = 0; c3 < 3; ++c3) xa.pu.ktab[c3] = reinterpret_cast<const T*>(s->ktab) + s->ktab_off[c3];
+    GS_CU(launch_xprecip_adjoint<T>(xa, st), "adjoint x pass");
+    YArgs<T> yb = ya;
+    yb.spec = reinterpret_cast<cplx<T>*>(a->Y);
+    GS_CU(launch_ypass<T>(yb, s->n1, 3 * FV, 1, st), "adjoint y inverse");
+    for (int f0 = 0; f0 < 3 * FV; f0 += GS_MAXG + 1) {
+      const int nf = 3 * FV - f0 < GS_MAXG + 1 ? 3 * FV - f0 : GS_MAXG + 1;
+      ZinvArgs<T> zi;
+      memset(&zi, 0, sizeof(zi));
+      zi.spec = reinterpret_cast<const cplx<T>*>(a->Y) + (size_t)f0 * rows * s->h;
+      for (int k = 0; k < nf; ++k) zi.dst[k] = Zr + (size_t)(f0 + k) * N;
+      zi.rows_per_field = rows;
+      zi.nrows = rows * nf;
+      zi.tw_h = twp<T>(s, 1);
+      zi.tw_n2 = twp<T>(s, 0);
+      zi.offset_field = -1;
+      GS_CU(launch_zinv<T>(zi, s->h, st), "adjoint z inverse");
+    }
+    // R of state n into rbuf
+    {
+      const T* src[GS_MAXF + 1];
+      int sq[GS_MAXF + 1];
+      for (int f = 0; f < V; ++f) {
+        src[f] = st0 + (size_t)(1 + f) * N;
+        sq[f] = 1;
+      }
+      if (F1 > V) {
+        src[V] = st0;
+        sq[V] = 0;
+      }
+      GS_TRY(elastic_chain_g<T>(s, src, sq, F1, 2, 1.0 / (double)N, s->spec, F1, st));
+      ZinvArgs<T> zr;
+      memset(&zr, 0, sizeof(zr));
+      zr.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+      for (int f = 0; f < F1; ++f) zr.dst[f] = reinterpret_cast<T*>(s->rbuf) + (size_t)f * N;
+      zr.rows_per_field = rows;
+      zr.nrows = rows * F1;
+      zr.tw_h = twp<T>(s, 1);
+      zr.tw_n2 = twp<T>(s, 0);
+      zr.offset_field = -1;
+      GS_CU(launch_zinv<T>(zr, s->h, st), "adjoint potential");
+    }
+    PadjArgs<T> pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.N = N;
+    pa.V = V;
+    pa.F = F1;
+    pa.ce = p.c_elastic ? 1 : 0;
+    for (int i = 0; i < 8; ++i) pa.A[i] = (T)p.coef[i];
+    pa.c1 = (T)p.c1;
+    pa.c2 = (T)p.c2;
+    pa.Es = (T)(p.xi * p.weight_elastic);
+    pa.dtM = (T)(p.dt * p.mobility_c);
+    pa.dtL = (T)(p.dt * p.mobility_eta);
+    pa.lc = lin;
+    pa.le = lin + N;
+    pa.zr = Zr;
+    pa.c = st0;
+    pa.eta = st0 + N;
+    pa.R = reinterpret_cast<const T*>(s->rbuf);
+    pa.dR = reinterpret_cast<T*>(s->mubuf);
+    pa.dP = reinterpret_cast<const T*>(a->dP);
+    pa.lc_out = lout;
+    pa.le_out = lout + N;
+    pa.partials = s->partials;
+    int nb = 0;
+    GS_CU(launch_padj<T>(pa, false, st, &nb), "adjoint local sources");
+    GS_CU(launch_reduce(s->partials, nb, 2, a->gsum + (size_t)n * PADJ_N + PADJ_KC, st), "adjoint reduce");
+    // B * dR
+    {
+      const T* src[GS_MAXF + 1];
+      int sq[GS_MAXF + 1];
+      for (int f = 0; f < F1; ++f) {
+        src[f] = reinterpret_cast<const T*>(s->mubuf) + (size_t)f * N;
+        sq[f] = 0;
+      }
+      GS_TRY(elastic_chain_g<T>(s, src, sq, F1, 2, 1.0 / (double)N, s->spec, F1, st));
+      ZinvArgs<T> zp;
+      memset(&zp, 0, sizeof(zp));
+      zp.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+      for (int f = 0; f < F1; ++f) zp.dst[f] = reinterpret_cast<T*>(a->dP) + (size_t)f * N;
+      zp.rows_per_field = rows;
+      zp.nrows = rows * F1;
+      zp.tw_h = twp<T>(s, 1);
+      zp.tw_n2 = twp<T>(s, 0);
+      zp.offset_field = -1;
+      GS_CU(launch_zinv<T>(zp, s->h, st), "adjoint elastic transpose");
+    }
+    GS_CU(launch_padj<T>(pa, true, st, &nb), "adjoint lambda");
+    GS_CU(launch_reduce(s->partials, nb, 7, a->gsum + (size_t)n * PADJ_N + PADJ_A1, st), "adjoint reduce");
+    c ^= 1;
+  }
+  *cur = c;
+  return GS_OK;
+}
+
+extern "C" int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype,
+                                          double* grads, void* grad_c0, void* grad_eta0, void* stream) {
+  if (!a || !seed_c || !seed_eta || !grads) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: null argument");
+  if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: run the forward first");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  gs_sim* s = a->s;
+  const int V = s->p.nvariants;
+  const size_t N = (size_t)s->N, fb = N * elt(s);
+  GS_TRY(upload(s, a->lam[0], seed_c, N, dtype));
+  GS_TRY(upload(s, static_cast<char*>(a->lam[0]) + fb, seed_eta, N * V, dtype));
+  cudaStream_t st = pick_stream(s, stream);
+  int c = 0;
+  GS_TRY(s->p.dtype == GS_DTYPE_F64 ? padj_backward<double>(a, st, &c) : padj_backward<float>(a, st, &c));
+  std::vector<double> h((size_t)a->nsteps * PADJ_N);
+  GS_CU(cudaMemcpyAsync(h.data(), a->gsum, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "sums D2H");
+  GS_CU(cudaStreamSynchronize(st), "adjoint sync");
+  for (int k = 0; k < PADJ_N; ++k) {
+    double sum = 0, cmp = 0;
+    for (int n = 0; n < a->nsteps; ++n) {
+      const double x = h[(size_t)n * PADJ_N + k], t = sum + x;
+      cmp += std::fabs(sum) >= std::fabs(x) ? (sum - t) + x : (x - t) + sum;
+      sum = t;
+    }
+    grads[k] = sum + cmp;
+  }
+  if (grad_c0) GS_TRY(download(s, a->lam[c], grad_c0, N, dtype));
+  if (grad_eta0) GS_TRY(download(s, static_cast<char*>(a->lam[c]) + fb, grad_eta0, N * V, dtype));
+  return GS_OK;
 }

@@ -3,4 +3,6 @@
 namespace gs {
 template cudaError_t launch_x_class<float, 2, 1, PrecipPairOp>(XArgs<float>&, cudaStream_t);
 template cudaError_t launch_x_class<double, 2, 1, PrecipPairOp>(XArgs<double>&, cudaStream_t);
+template cudaError_t launch_x_class<float, 2, 3, PrecipAdjOp>(XArgs<float>&, cudaStream_t);
+template cudaError_t launch_x_class<double, 2, 3, PrecipAdjOp>(XArgs<double>&, cudaStream_t);
 }  // namespace gs

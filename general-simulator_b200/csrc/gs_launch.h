@@ -26,6 +26,8 @@ template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_
 template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req = 0);
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s);
+// the transposed precipitate update (F = 2, G = 3 per grid-z slice)
+template <typename T> cudaError_t launch_xprecip_adjoint(XArgs<T>& a, cudaStream_t s);
 // field-count class (3, 5 or 9) of the B octant table of V variants
 inline int btab_class(int V) { return V <= 3 ? 3 : (V <= 5 ? 5 : 9); }
 inline int btab_stride(int V) {

@@ -482,6 +482,33 @@ struct PrecipPairOp {
   }
 };
 
+// The transposed precipitate update, one pair per grid-z slice: inputs
+// (lambda', state') of c (slice 0) or eta_p (slice 1 + p); outputs
+// D lambda', K D lambda', K^a D state' with D = 1/(1 + dt M kappa_c K^2),
+// a = 2 for c, D = 1/(1 + dt L kappa_eta K), a = 1 for eta.  The symbols
+// are real and even: each is its own transpose.
+struct PrecipAdjOp {
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    const PrecipUpd<T>& u = a.pu;
+    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+#pragma unroll
+    for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
+    if (blockIdx.z == 0) {
+      const T d = u.scale / ((T)1 + u.dtM * u.kc * K * K);
+      out[0] = in[0] * d;
+      out[1] = in[0] * (K * d);
+      out[2] = in[1] * (K * K * d);
+    } else {
+      const T d = u.scale / ((T)1 + u.dtL * u.ke * K);
+      out[0] = in[0] * d;
+      out[1] = in[0] * (K * d);
+      out[2] = in[1] * (K * d);
+    }
+  }
+};
+
 // threads per block of the x pass for a field-count class (FM, GM)
 template <int FM, int GM> struct XBounds {
   static constexpr int G = FM > GM ? FM : GM;

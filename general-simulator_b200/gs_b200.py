@@ -165,6 +165,11 @@ def lib() -> C.CDLL:
         "gs_adjoint_device_bytes": (C.c_size_t, [vp]),
         "gs_adjoint_use_graph": (C.c_int, [vp, C.c_int]),
         "gs_adjoint_launch_count": (C.c_int64, [vp]),
+        "gs_precip_adjoint_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
+        "gs_precip_adjoint_destroy": (C.c_int, [vp]),
+        "gs_precip_adjoint_forward": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp]),
+        "gs_precip_adjoint_backward": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(C.c_double), vp, vp, vp]),
+        "gs_precip_adjoint_device_bytes": (C.c_size_t, [vp]),
         "gs_sim_set_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_get_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(GsSchedule)]),
@@ -275,6 +280,61 @@ class Adjoint:
 
     def launch_count(self) -> int:
         return int(lib().gs_adjoint_launch_count(self.h))
+
+
+class PrecipAdjoint:
+    """Adjoint of a precipitate run (gs_precip_adjoint*): forward() runs
+    (c0, eta0) -> (c_T, eta_T) keeping every state; backward(seed_c,
+    seed_eta) returns (grads[9], dJ/dc0, dJ/deta0) for J = <seed_c, c_T> +
+    <seed_eta, eta_T>, grads over (kappa_c, kappa_eta, coef[1..7])."""
+
+    PARAM_NAMES = ("kappa_c", "kappa_eta", "A1", "A2", "A3", "A4", "A5", "A6", "A7")
+
+    def __init__(self, params: GsParams, nsteps: int):
+        self.params = params.copy()
+        self.nsteps = nsteps
+        h = C.c_void_p()
+        check(lib().gs_precip_adjoint_create(C.byref(self.params), nsteps, C.byref(h)), "gs_precip_adjoint_create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().gs_precip_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        p = self.params
+        return (p.nx, p.ny, p.nz)
+
+    def forward(self, c0: np.ndarray, eta0: np.ndarray, stream: int = 0):
+        c = np.ascontiguousarray(c0, dtype=np.float64)
+        e = np.ascontiguousarray(eta0, dtype=np.float64)
+        co = np.empty(self.shape, dtype=np.float64)
+        eo = np.empty((self.params.nvariants,) + self.shape, dtype=np.float64)
+        check(lib().gs_precip_adjoint_forward(self.h, c.ctypes.data, e.ctypes.data, GS_DTYPE_F64, co.ctypes.data,
+                                              eo.ctypes.data, C.c_void_p(stream)), "gs_precip_adjoint_forward")
+        return co, eo
+
+    def backward(self, seed_c: np.ndarray, seed_eta: np.ndarray, stream: int = 0):
+        sc = np.ascontiguousarray(seed_c, dtype=np.float64)
+        se = np.ascontiguousarray(seed_eta, dtype=np.float64)
+        g = (C.c_double * 9)()
+        gc = np.empty(self.shape, dtype=np.float64)
+        ge = np.empty((self.params.nvariants,) + self.shape, dtype=np.float64)
+        check(lib().gs_precip_adjoint_backward(self.h, sc.ctypes.data, se.ctypes.data, GS_DTYPE_F64, g,
+                                               gc.ctypes.data, ge.ctypes.data, C.c_void_p(stream)),
+              "gs_precip_adjoint_backward")
+        return np.array(g[:]), gc, ge
+
+    def device_bytes(self) -> int:
+        return int(lib().gs_precip_adjoint_device_bytes(self.h))
 
 
 class Sim:

@@ -273,6 +273,27 @@ size_t gs_adjoint_device_bytes(const gs_adjoint* a);
 /* Kernel launches issued by the last forward or backward call. */
 int64_t gs_adjoint_launch_count(const gs_adjoint* a);
 
+/* ---- adjoint of the precipitate run -------------------------------------- */
+/* The transpose of the semi-implicit precipitate step (Dynamics_precipitate::
+ * Calculate, src/dynamics_precipitate.cu:118-289) in baseline mode: the
+ * Cahn-Hilliard and Allen-Cahn factors 1/(1 + dt M kappa_c K^2), 1/(1 + dt L
+ * kappa_eta K) and the operator K are real even symbols, hence their own
+ * transposes; the local terms' Jacobians are applied pointwise and the
+ * elastic coupling through the same B convolution.  The noise is additive
+ * and drops out; the mass projection only corrects rounding and is not
+ * differentiated.  Every state of the run is kept on the device ((nsteps+1)
+ * (V+1) N values).  gs_precip_adjoint_backward returns, for J = <seed_c, c_T>
+ * + <seed_eta, eta_T>, grads[9] = dJ/d(kappa_c, kappa_eta, coef[1..7]) and
+ * dJ/dc0, dJ/deta0 (host buffers of dtype, NULL to skip). */
+typedef struct gs_padjoint gs_padjoint;
+int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjoint** out);
+int gs_precip_adjoint_destroy(gs_padjoint* a);
+int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
+                              void* eta_final, void* stream);
+int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype, double* grads,
+                               void* grad_c0, void* grad_eta0, void* stream);
+size_t gs_precip_adjoint_device_bytes(const gs_padjoint* a);
+
 /* ---- batched ensembles ------------------------------------------------- */
 /* Many independent martensite simulations advanced together.  Simulations
  * of one grid, variant count, modulus and eigenstrain direction form a group

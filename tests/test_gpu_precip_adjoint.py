@@ -1,0 +1,125 @@
+"""The hand-written adjoint of the precipitate run (gs_precip_adjoint_*,
+through the C ABI) against the FP64 oracle adjoint and central differences.
+
+Tolerances: FP64 gradients agree with the oracle adjoint to 1e-9 relative
+(different FFT algorithms; an entry far below the largest is held to 1e-12 of
+the largest); FP32 gradients to 1e-3 relative; central differences of the
+FP64 GPU forward with h = 1e-6 to 1e-5 relative."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+F64, F32 = 1, 0
+
+
+def setup(gb, shape, V=4, dtype=F64, noise=0.0, c_elastic=1, seed=2):
+    p = gb.precip3d_params(8, dtype=dtype)
+    p.nx, p.ny, p.nz = shape
+    p.nvariants = V
+    p.noise_amp = noise
+    p.c_elastic = c_elastic
+    c0 = gb.initial_c(p, seed)
+    e0 = gb.initial_eta(p, seed + 1, 0.4)
+    rng = np.random.default_rng(seed)
+    return p, c0, e0, rng.standard_normal(c0.shape), rng.standard_normal(e0.shape)
+
+
+def gpu_adjoint(gb, p, c0, e0, ns, sc, se):
+    a = gb.PrecipAdjoint(p, ns)
+    try:
+        cT, eT = a.forward(c0, e0)
+        g, gc, ge = a.backward(sc, se)
+        return g, gc, ge, cT, eT
+    finally:
+        a.close()
+
+
+def close_vec(g, og, rtol):
+    g, og = np.asarray(g), np.asarray(og)
+    return np.all(np.abs(g - og) <= rtol * np.abs(og) + 1e-12 * np.abs(og).max())
+
+
+@pytest.mark.parametrize("shape,V,ns,noise,ce", [
+    ((6, 8, 4), 4, 3, 0.0, 1),
+    ((8, 8, 12), 3, 4, 1e-3, 1),
+    ((8, 12, 2), 2, 5, 0.0, 0),
+    ((1, 16, 24), 2, 4, 1e-3, 1),
+])
+def test_precip_adjoint_f64_matches_oracle(gb, orc, shape, V, ns, noise, ce):
+    p, c0, e0, sc, se = setup(gb, shape, V, F64, noise, ce)
+    g, gc, ge, cT, eT = gpu_adjoint(gb, p, c0, e0, ns, sc, se)
+    og, ogc, oge = orc.precip_adjoint(p, c0, e0, ns, sc, se)
+    oc, oe = orc.precip_run(p, c0, e0, ns)
+    assert rel_l2(cT, oc) < 1e-11 and rel_l2(eT, oe) < 1e-11
+    assert close_vec(g, og, 1e-9), (g, og)
+    assert rel_l2(gc, ogc) < 1e-10
+    assert rel_l2(ge, oge) < 1e-10
+
+
+def test_precip_adjoint_f64_matches_central_differences(gb):
+    """Directional derivatives of the GPU forward run against the GPU
+    adjoint: independent of the oracle."""
+    p, c0, e0, sc, se = setup(gb, (8, 8, 8), 3, F64, 0.0, 1, seed=7)
+    ns, h = 4, 1e-6
+    g, gc, ge, _, _ = gpu_adjoint(gb, p, c0, e0, ns, sc, se)
+
+    def J(q, c=c0, e=e0):
+        a = gb.PrecipAdjoint(q, ns)
+        try:
+            cc, ee = a.forward(c, e)
+        finally:
+            a.close()
+        return (sc * cc).sum() + (se * ee).sum()
+
+    for k in (0, 1, 2, 3, 4):
+        q1, q2 = p.copy(), p.copy()
+        if k == 0:
+            q1.kappa_c += h
+            q2.kappa_c -= h
+        elif k == 1:
+            q1.kappa_eta += h
+            q2.kappa_eta -= h
+        else:
+            q1.coef[k - 1] += h
+            q2.coef[k - 1] -= h
+        fd = (J(q1) - J(q2)) / (2 * h)
+        assert abs(g[k] - fd) <= 1e-5 * abs(fd) + 1e-10, (k, g[k], fd)
+    rng = np.random.default_rng(3)
+    d = rng.standard_normal(c0.shape)
+    fd = (J(p, c0 + h * d) - J(p, c0 - h * d)) / (2 * h)
+    assert abs((gc * d).sum() - fd) <= 1e-6 * abs(fd)
+    d = rng.standard_normal(e0.shape)
+    fd = (J(p, c0, e0 + h * d) - J(p, c0, e0 - h * d)) / (2 * h)
+    assert abs((ge * d).sum() - fd) <= 1e-6 * abs(fd)
+
+
+def test_precip_adjoint_f32(gb, orc):
+    p, c0, e0, sc, se = setup(gb, (16, 16, 16), 4, F32, 0.0, 1, seed=11)
+    g, gc, ge, _, _ = gpu_adjoint(gb, p, c0, e0, 3, sc, se)
+    q = p.copy()
+    q.dtype = F64
+    og, ogc, oge = orc.precip_adjoint(q, c0, e0, 3, sc, se)
+    big = np.abs(og) > 1e-3 * np.abs(og).max()
+    assert np.all(np.abs(g - og)[big] <= 1e-3 * np.abs(og)[big]), (g, og)
+    assert rel_l2(gc, ogc) < 1e-4
+    assert rel_l2(ge, oge) < 1e-4
+
+
+def test_precip_adjoint_rejects(gb):
+    p = gb.mart3d_params(8, dtype=F64)
+    with pytest.raises(RuntimeError):
+        gb.PrecipAdjoint(p, 2)
+    q = gb.precip3d_params(8, dtype=F64)
+    with pytest.raises(RuntimeError):
+        gb.PrecipAdjoint(q, 0)
+    a = gb.PrecipAdjoint(q, 2)
+    try:
+        c0 = np.zeros((8, 8, 8))
+        with pytest.raises(RuntimeError):
+            a.backward(c0, np.zeros((4, 8, 8, 8)))
+        assert a.device_bytes() >= 8 * 512 * 5 * 3
+    finally:
+        a.close()
