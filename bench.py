@@ -354,6 +354,44 @@ def extra_configs() -> dict:
     return out
 
 
+def extra_precip_adjoint(n: int = 128, steps: int = 10) -> dict:
+    """Adjoint of the precipitate run: 128^3, concentration + 4 variants,
+    FP32, 10 steps, noise off.  plain = 10 steps of gs_sim_step; forward =
+    the adjoint's forward run (the same steps, every state kept on the
+    device); backward = gs_precip_adjoint_backward (all ten reverse steps
+    and the nine parameter sums), seeds already on the device.  Device time
+    on one stream."""
+    import torch
+
+    import gs_b200 as gb
+
+    p = gb.precip3d_params(n, dtype=gb.GS_DTYPE_F32)
+    p.noise_amp = 0.0
+    c0 = gb.initial_c(p, 2)
+    e0 = gb.initial_eta(p, 3, 0.3)
+    rng = np.random.default_rng(0)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        sim = gb.Sim(p)
+        sim.set_field("concentration", c0)
+        sim.set_field("eta", e0)
+        sim.step(3, sh)
+        plain = min(_timed(stream, lambda: sim.step(steps, sh)) for _ in range(3))
+        sim.close()
+        a = gb.PrecipAdjoint(p, steps)
+        a.forward(c0, e0, sh, outputs=False)
+        a.set_seed(rng.standard_normal(c0.shape), rng.standard_normal(e0.shape))
+        a.backward(stream=sh, outputs=False)
+        fwd = min(_timed(stream, lambda: a.forward(stream=sh, outputs=False)) for _ in range(3))
+        bwd = min(_timed(stream, lambda: a.backward(stream=sh, outputs=False)) for _ in range(3))
+        mem = a.device_bytes()
+        a.close()
+    return {"workload": f"{n}^3, concentration + 4 variants, FP32, {steps} steps, noise off",
+            "plain_ms": plain, "forward_ms": fwd, "backward_ms": bwd, "adjoint_to_plain": bwd / plain,
+            "device_bytes": mem, "note": "every state of the run is kept; no recomputation"}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: the FP64 oracle on the host cores
 # ---------------------------------------------------------------------------
@@ -526,6 +564,7 @@ def run_ours(args, ws, rank, local):
         extras["adjoint"] = extra_adjoint()
         extras["ensemble"] = extra_ensemble()
         extras["other_workloads"] = extra_configs()
+        extras["precip_adjoint"] = extra_precip_adjoint()
     cpu = None
     if ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(n, args.cpu_seconds)

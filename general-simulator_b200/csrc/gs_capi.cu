@@ -2472,14 +2472,15 @@ struct gs_padjoint {
   void* Zr = nullptr;  // [3 (V + 1)][N]
   void* dP = nullptr;  // [F1][N]
   double* gsum = nullptr;  // [nsteps][PADJ_N]
-  bool forward_done = false;
+  void* seed = nullptr;    // [V + 1][N]: dJ/d(c_T, eta_T)
+  bool forward_done = false, seeded = false;
   size_t bytes = 0;
 };
 
 static void free_padjoint(gs_padjoint* a) {
   if (!a) return;
   cudaDeviceSynchronize();
-  for (void* q : {a->states, a->lam[0], a->lam[1], a->Y, a->Zr, a->dP, (void*)a->gsum})
+  for (void* q : {a->states, a->lam[0], a->lam[1], a->Y, a->Zr, a->dP, (void*)a->gsum, a->seed})
     if (q) cudaFree(q);
   if (a->s) free_sim(a->s);
   delete a;
@@ -2509,6 +2510,7 @@ extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjo
   if ((rc = get(&a->states, fb * (V + 1) * (nsteps + 1), "adjoint states")) != GS_OK ||
       (rc = get(&a->lam[0], fb * (V + 1), "adjoint lambda")) != GS_OK ||
       (rc = get(&a->lam[1], fb * (V + 1), "adjoint lambda")) != GS_OK ||
+      (rc = get(&a->seed, fb * (V + 1), "adjoint seed")) != GS_OK ||
       (rc = get(&a->Y, fb * 3 * (V + 1), "adjoint spectra")) != GS_OK ||
       (rc = get(&a->Zr, fb * 3 * (V + 1), "adjoint fields")) != GS_OK ||
       (rc = get(&a->dP, fb * a->F1, "adjoint elastic sources")) != GS_OK ||
@@ -2530,15 +2532,22 @@ extern "C" size_t gs_precip_adjoint_device_bytes(const gs_padjoint* a) { return 
 
 extern "C" int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
                                          void* eta_final, void* stream) {
-  if (!a || !c0 || !eta0) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: null argument");
+  if (!a) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: null handle");
+  if (!c0 != !eta0) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: give both c0 and eta0, or neither");
   gs_sim* s = a->s;
   const int V = s->p.nvariants;
   const size_t N = (size_t)s->N, fb = N * elt(s);
-  GS_TRY(gs_sim_set_field(s, "concentration", c0, N, dtype));
-  GS_TRY(gs_sim_set_field(s, "eta", eta0, N * V, dtype));
   cudaStream_t st = pick_stream(s, stream);
-  s->step = 0;
   char* S = static_cast<char*>(a->states);
+  if (c0) {
+    GS_TRY(gs_sim_set_field(s, "concentration", c0, N, dtype));
+    GS_TRY(gs_sim_set_field(s, "eta", eta0, N * V, dtype));
+  } else {  // again from the initial state of the previous forward run
+    if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: no initial state yet");
+    GS_CU(cudaMemcpyAsync(s->conc, S, fb, cudaMemcpyDeviceToDevice, st), "initial state");
+    GS_CU(cudaMemcpyAsync(s->eta[0], S + fb, fb * V, cudaMemcpyDeviceToDevice, st), "initial state");
+  }
+  s->step = 0;
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
   for (int n = 0; n <= a->nsteps; ++n) {
     char* dst = S + (size_t)n * fb * (V + 1);
@@ -2701,17 +2710,30 @@ template <typename T> static int padj_backward(gs_padjoint* a, cudaStream_t st, 
   return GS_OK;
 }
 
+extern "C" int gs_precip_adjoint_set_seed(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype) {
+  if (!a || !seed_c || !seed_eta) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_set_seed: null argument");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  gs_sim* s = a->s;
+  const size_t N = (size_t)s->N, fb = N * elt(s);
+  GS_TRY(upload(s, a->seed, seed_c, N, dtype));
+  GS_TRY(upload(s, static_cast<char*>(a->seed) + fb, seed_eta, N * s->p.nvariants, dtype));
+  a->seeded = true;
+  return GS_OK;
+}
+
 extern "C" int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype,
                                           double* grads, void* grad_c0, void* grad_eta0, void* stream) {
-  if (!a || !seed_c || !seed_eta || !grads) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: null argument");
+  if (!a || !grads) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: null argument");
   if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: run the forward first");
   if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  if (!seed_c != !seed_eta) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: give both seeds, or neither");
+  if (seed_c) GS_TRY(gs_precip_adjoint_set_seed(a, seed_c, seed_eta, dtype));
+  if (!a->seeded) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: no seed set");
   gs_sim* s = a->s;
   const int V = s->p.nvariants;
   const size_t N = (size_t)s->N, fb = N * elt(s);
-  GS_TRY(upload(s, a->lam[0], seed_c, N, dtype));
-  GS_TRY(upload(s, static_cast<char*>(a->lam[0]) + fb, seed_eta, N * V, dtype));
   cudaStream_t st = pick_stream(s, stream);
+  GS_CU(cudaMemcpyAsync(a->lam[0], a->seed, fb * (V + 1), cudaMemcpyDeviceToDevice, st), "seed");
   int c = 0;
   GS_TRY(s->p.dtype == GS_DTYPE_F64 ? padj_backward<double>(a, st, &c) : padj_backward<float>(a, st, &c));
   std::vector<double> h((size_t)a->nsteps * PADJ_N);

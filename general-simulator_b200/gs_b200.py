@@ -170,6 +170,7 @@ def lib() -> C.CDLL:
         "gs_precip_adjoint_forward": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp]),
         "gs_precip_adjoint_backward": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(C.c_double), vp, vp, vp]),
         "gs_precip_adjoint_device_bytes": (C.c_size_t, [vp]),
+        "gs_precip_adjoint_set_seed": (C.c_int, [vp, vp, vp, C.c_int]),
         "gs_sim_set_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_get_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(GsSchedule)]),
@@ -313,23 +314,45 @@ class PrecipAdjoint:
         p = self.params
         return (p.nx, p.ny, p.nz)
 
-    def forward(self, c0: np.ndarray, eta0: np.ndarray, stream: int = 0):
-        c = np.ascontiguousarray(c0, dtype=np.float64)
-        e = np.ascontiguousarray(eta0, dtype=np.float64)
-        co = np.empty(self.shape, dtype=np.float64)
-        eo = np.empty((self.params.nvariants,) + self.shape, dtype=np.float64)
-        check(lib().gs_precip_adjoint_forward(self.h, c.ctypes.data, e.ctypes.data, GS_DTYPE_F64, co.ctypes.data,
-                                              eo.ctypes.data, C.c_void_p(stream)), "gs_precip_adjoint_forward")
-        return co, eo
+    def forward(self, c0: Optional[np.ndarray] = None, eta0: Optional[np.ndarray] = None, stream: int = 0,
+                outputs: bool = True):
+        """c0 = eta0 = None: again from the previous initial state (device);
+        outputs=False: keep (c_T, eta_T) on the device and return None."""
+        c = e = None
+        if c0 is not None:
+            c = np.ascontiguousarray(c0, dtype=np.float64)
+            e = np.ascontiguousarray(eta0, dtype=np.float64)
+        co = eo = None
+        if outputs:
+            co = np.empty(self.shape, dtype=np.float64)
+            eo = np.empty((self.params.nvariants,) + self.shape, dtype=np.float64)
+        check(lib().gs_precip_adjoint_forward(self.h, None if c is None else c.ctypes.data,
+                                              None if e is None else e.ctypes.data, GS_DTYPE_F64,
+                                              None if co is None else co.ctypes.data,
+                                              None if eo is None else eo.ctypes.data, C.c_void_p(stream)),
+              "gs_precip_adjoint_forward")
+        return (co, eo) if outputs else None
 
-    def backward(self, seed_c: np.ndarray, seed_eta: np.ndarray, stream: int = 0):
+    def set_seed(self, seed_c: np.ndarray, seed_eta: np.ndarray) -> None:
         sc = np.ascontiguousarray(seed_c, dtype=np.float64)
         se = np.ascontiguousarray(seed_eta, dtype=np.float64)
+        check(lib().gs_precip_adjoint_set_seed(self.h, sc.ctypes.data, se.ctypes.data, GS_DTYPE_F64),
+              "gs_precip_adjoint_set_seed")
+
+    def backward(self, seed_c: Optional[np.ndarray] = None, seed_eta: Optional[np.ndarray] = None, stream: int = 0,
+                 outputs: bool = True):
+        """Seeds None: the last ones given.  Returns (grads[9], dJ/dc0,
+        dJ/deta0); the fields are None with outputs=False."""
+        if seed_c is not None:
+            self.set_seed(seed_c, seed_eta)
         g = (C.c_double * 9)()
-        gc = np.empty(self.shape, dtype=np.float64)
-        ge = np.empty((self.params.nvariants,) + self.shape, dtype=np.float64)
-        check(lib().gs_precip_adjoint_backward(self.h, sc.ctypes.data, se.ctypes.data, GS_DTYPE_F64, g,
-                                               gc.ctypes.data, ge.ctypes.data, C.c_void_p(stream)),
+        gc = ge = None
+        if outputs:
+            gc = np.empty(self.shape, dtype=np.float64)
+            ge = np.empty((self.params.nvariants,) + self.shape, dtype=np.float64)
+        check(lib().gs_precip_adjoint_backward(self.h, None, None, GS_DTYPE_F64, g,
+                                               None if gc is None else gc.ctypes.data,
+                                               None if ge is None else ge.ctypes.data, C.c_void_p(stream)),
               "gs_precip_adjoint_backward")
         return np.array(g[:]), gc, ge
 

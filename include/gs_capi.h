@@ -284,12 +284,15 @@ int64_t gs_adjoint_launch_count(const gs_adjoint* a);
  * differentiated.  Every state of the run is kept on the device ((nsteps+1)
  * (V+1) N values).  gs_precip_adjoint_backward returns, for J = <seed_c, c_T>
  * + <seed_eta, eta_T>, grads[9] = dJ/d(kappa_c, kappa_eta, coef[1..7]) and
- * dJ/dc0, dJ/deta0 (host buffers of dtype, NULL to skip). */
+ * dJ/dc0, dJ/deta0 (host buffers of dtype, NULL to skip).  NULL seeds reuse
+ * the ones last given (gs_precip_adjoint_set_seed, kept on the device); NULL
+ * c0 and eta0 rerun the forward from the previous initial state. */
 typedef struct gs_padjoint gs_padjoint;
 int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjoint** out);
 int gs_precip_adjoint_destroy(gs_padjoint* a);
 int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
                               void* eta_final, void* stream);
+int gs_precip_adjoint_set_seed(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype);
 int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype, double* grads,
                                void* grad_c0, void* grad_eta0, void* stream);
 size_t gs_precip_adjoint_device_bytes(const gs_padjoint* a);
