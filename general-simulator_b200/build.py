@@ -87,10 +87,26 @@ def build_oracle() -> str:
     return os.path.join(ROOT, "oracle", "liboracle.so")
 
 
+def build_reference() -> str | None:
+    """The reference's own gsi in oracle/_ref/ (test infrastructure: it
+    generated the committed fixtures under tests/golden/).  Built only where
+    the reference tree is present and the binary is missing; a failure is
+    reported, not raised, since nothing at run time needs it."""
+    out = os.path.join(ROOT, "oracle", "_ref", "gsi")
+    if os.path.exists(out):
+        return out
+    r = subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], capture_output=True, text=True)
+    if r.returncode != 0:
+        print("reference build skipped:", (r.stdout + r.stderr).strip().splitlines()[-1:], file=sys.stderr)
+        return None
+    return out
+
+
 def build_all(jobs: int = 8) -> None:
     build_lib(jobs)
     build_frontend()
     build_oracle()
+    build_reference()
 
 
 if __name__ == "__main__":
