@@ -376,11 +376,13 @@ template <int FM> struct TriStride {  // entries per table point, rounded to an 
 };
 
 // B(k) read from the octant table (B even in every axis: see the table fill).
+// The table point of kx is also that of n0 - kx, so the x pass loads it once
+// for the pair (kx_pair).
 struct TableOp {
-  template <typename T, int FM, int GM>
-  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
-                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
-    static_assert(FM == GM, "square tables only");
+  static constexpr bool kx_pair = true;
+  template <typename T, int FM>
+  __device__ __forceinline__ static void load(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                              T (&bv)[TriStride<FM>::v]) {
     constexpr int S = TriStride<FM>::v;
     const int rc = a.ec.refcompat;
     int mx = fold_idx(ix, nn[0], rc), my = fold_idx(iy, nn[1], rc), mz = fold_idx(iz, nn[2], rc);
@@ -388,13 +390,17 @@ struct TableOp {
     my = my < 0 ? -my : my;
     mz = mz < 0 ? -mz : mz;
     const cplx<T>* b2 = reinterpret_cast<const cplx<T>*>(a.btab + (((long long)mx * a.bt_d1 + my) * a.bt_d2 + mz) * S);
-    T bv[S];
 #pragma unroll
     for (int i = 0; i < S / 2; ++i) {
       const cplx<T> w = __ldg(b2 + i);
       bv[2 * i] = w.x;
       bv[2 * i + 1] = w.y;
     }
+  }
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void contract(const XArgs<T>& a, const T (&bv)[TriStride<FM>::v],
+                                                  const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    static_assert(FM == GM, "square tables only");
     const T mult = a.simscale ? a.simscale[blockIdx.z] : (T)1;
 #pragma unroll
     for (int g = 0; g < GM; ++g) {
@@ -405,6 +411,20 @@ struct TableOp {
       out[g] = acc * mult;
     }
   }
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    T bv[TriStride<FM>::v];
+    load<T, FM>(a, nn, ix, iy, iz, bv);
+    contract<T, FM, GM>(a, bv, in, out);
+  }
+};
+
+template <class Op, class = void> struct KxPair {
+  static constexpr bool v = false;
+};
+template <class Op> struct KxPair<Op, decltype(void(Op::kx_pair))> {
+  static constexpr bool v = Op::kx_pair;
 };
 
 // Octant table of the scaled, Nyquist-averaged B(k) of a square contraction
@@ -555,8 +575,11 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const bool special_blk = kz0 == 0 && (n1 == 1 || ky == 0 || ky == HH);
   {
     const int nn[3] = {a.n0, a.n1, a.n2};
+    // with a paired operator one item is kx and N0 - kx (kx <= N0 / 2)
+    constexpr bool PAIR = KxPair<Op>::v;
+    constexpr int NKX = PAIR ? N0 / 2 + 1 : N0;
 #pragma unroll 1
-    for (int idx = threadIdx.x; idx < N0 * TZ; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < NKX * TZ; idx += blockDim.x) {
       const int cc = idx % TZ, kx = idx / TZ;
       const int kz = kz0 + cc;
       int kyA = ky, kzA = kz, kyB = 0, kzB = 0;
@@ -571,42 +594,65 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
           kyA = ky - HH; kzA = h;
         }
       }
-      const V* pin = smb + kx * TZ + cc;
       if (!(special_blk && cc == 0)) {
-        V in[FM], out[GM];
+        if constexpr (PAIR) {
+          T bv[TriStride<FM>::v];
+          Op::template load<T, FM>(a, nn, kx, kyA, kzA, bv);
+          const int kx2 = (N0 - kx) % N0;
 #pragma unroll
-        for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pin[f * region] : mk2((T)0, (T)0);
-        Op::template apply<T, FM, GM>(a, nn, kx, kyA, kzA, in, out);
-        V* pout = smb + kx * TZ + cc;
+          for (int side = 0; side < 2; ++side) {
+            if (side == 1 && kx2 == kx) break;
+            const int px = side ? kx2 : kx;
+            V* pt = smb + px * TZ + cc;
+            V in[FM], out[GM];
 #pragma unroll
-        for (int g = 0; g < GM; ++g)
-          if (g < a.G) pout[g * region] = out[g];
+            for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pt[f * region] : mk2((T)0, (T)0);
+            Op::template contract<T, FM, GM>(a, bv, in, out);
+#pragma unroll
+            for (int g = 0; g < GM; ++g)
+              if (g < a.G) pt[g * region] = out[g];
+          }
+        } else {
+          V* pt = smb + kx * TZ + cc;
+          V in[FM], out[GM];
+#pragma unroll
+          for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pt[f * region] : mk2((T)0, (T)0);
+          Op::template apply<T, FM, GM>(a, nn, kx, kyA, kzA, in, out);
+#pragma unroll
+          for (int g = 0; g < GM; ++g)
+            if (g < a.G) pt[g * region] = out[g];
+        }
       } else {
         // two real sequences packed in one column: A = (W(k) + conj W(-k))/2,
         // B = -i (W(k) - conj W(-k))/2, each contracted with its own k
-        const int kxb = (N0 - kx) % N0;
-        V res[2][GM];
 #pragma unroll 1
-        for (int half = 0; half < 2; ++half) {
-          V in[FM];
+        for (int side = 0; side < (PAIR ? 2 : 1); ++side) {
+          const int kxa = side ? (N0 - kx) % N0 : kx;
+          if (side == 1 && kxa == kx) break;
+          const int kxb = (N0 - kxa) % N0;
+          V res[2][GM];
+#pragma unroll 1
+          for (int half = 0; half < 2; ++half) {
+            V in[FM];
 #pragma unroll
-          for (int f = 0; f < FM; ++f) {
-            const V wa = f < a.F ? smb[f * region + kx * TZ] : mk2((T)0, (T)0);
-            const V wb = f < a.F ? smb[f * region + kxb * TZ] : mk2((T)0, (T)0);
-            if (half == 0) {
-              in[f] = mk2((T)0.5 * (wa.x + wb.x), (T)0.5 * (wa.y - wb.y));
-            } else {
-              in[f] = mk2((T)0.5 * (wa.y + wb.y), (T)-0.5 * (wa.x - wb.x));
+            for (int f = 0; f < FM; ++f) {
+              const V wa = f < a.F ? smb[f * region + kxa * TZ] : mk2((T)0, (T)0);
+              const V wb = f < a.F ? smb[f * region + kxb * TZ] : mk2((T)0, (T)0);
+              if (half == 0) {
+                in[f] = mk2((T)0.5 * (wa.x + wb.x), (T)0.5 * (wa.y - wb.y));
+              } else {
+                in[f] = mk2((T)0.5 * (wa.y + wb.y), (T)-0.5 * (wa.x - wb.x));
+              }
             }
+            V out[GM];
+            Op::template apply<T, FM, GM>(a, nn, kxa, half ? kyB : kyA, half ? kzB : kzA, in, out);
+#pragma unroll
+            for (int g = 0; g < GM; ++g) res[half][g] = out[g];
           }
-          V out[GM];
-          Op::template apply<T, FM, GM>(a, nn, kx, half ? kyB : kyA, half ? kzB : kzA, in, out);
 #pragma unroll
-          for (int g = 0; g < GM; ++g) res[half][g] = out[g];
+          for (int g = 0; g < GM; ++g)
+            if (g < a.G) part[g * N0 + kxa] = mk2(res[0][g].x - res[1][g].y, res[0][g].y + res[1][g].x);
         }
-#pragma unroll
-        for (int g = 0; g < GM; ++g)
-          if (g < a.G) part[g * N0 + kx] = mk2(res[0][g].x - res[1][g].y, res[0][g].y + res[1][g].x);
       }
     }
   }
