@@ -2752,3 +2752,7 @@ extern "C" int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, co
   if (grad_eta0) GS_TRY(download(s, static_cast<char*>(a->lam[c]) + fb, grad_eta0, N * V, dtype));
   return GS_OK;
 }
+
+extern "C" void gs_set_x_prefetch(int on) { set_x_prefetch(on != 0); }
+
+extern "C" unsigned int gs_x_prefetch_timeouts(void) { return x_wait_timeouts(); }

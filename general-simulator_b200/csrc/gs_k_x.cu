@@ -9,6 +9,10 @@ template <typename T, int FM, int GM, class Op> cudaError_t launch_x_class(XArgs
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s) {
   if (a.btab) {  // B from the octant table (square contraction, F = G)
     if (a.F != a.G) return cudaErrorInvalidValue;
+    if constexpr (sizeof(T) == 4) {
+      const cudaError_t e = launch_xtma(a, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
     if (a.F <= 3) return launch_x_class<T, 3, 3, TableOp>(a, s);
     if (a.F <= 5) return launch_x_class<T, 5, 5, TableOp>(a, s);
     return launch_x_class<T, 9, 9, TableOp>(a, s);

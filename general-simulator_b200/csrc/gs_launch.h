@@ -25,6 +25,12 @@ int pick_tz(int h);
 template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s, int lines_req = 0);
 template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req = 0);
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
+// TMA-fed x pass (gs_k_xtma.cu): cudaErrorNotSupported when the case is not
+// covered (the caller then runs the plain pass)
+cudaError_t launch_xtma(XArgs<float>& a, cudaStream_t s);
+void set_x_prefetch(bool on);
+bool x_prefetch();
+unsigned int x_wait_timeouts();
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s);
 // the transposed precipitate update (F = 2, G = 3 per grid-z slice)
 template <typename T> cudaError_t launch_xprecip_adjoint(XArgs<T>& a, cudaStream_t s);

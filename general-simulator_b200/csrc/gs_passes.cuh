@@ -535,35 +535,24 @@ template <int FM, int GM> struct XBounds {
   static constexpr int v = G <= 3 ? 768 : (G <= 10 ? 640 : 576);
 };
 
-template <typename T, int N0, int FM, int GM, int TZC, class Op>
-__global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
+// One (ky, kz tile) column set of the x pass after its inputs are in
+// registers (v, in_pos order, group grp = field grp): forward FFT along x,
+// per-point operation, inverse FFT, store.  smb: the groups' line regions
+// (region = PAD * TZ values each), part: GM x N0 values for the packed
+// columns.  Shared by the plain and the TMA-fed kernels.
+template <typename T, int N0, int FM, int GM, class Op>
+__device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx<T>* part, int TZ, int grp, int c,
+                                           int t, int kz0, int ky, cplx<T>* out_base,
+                                           cplx<T> (&v)[Line<T, N0>::R1]) {
   using L = Line<T, N0>;
   using V = cplx<T>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  V* smb = reinterpret_cast<V*>(smraw);
-  const int TZ = TZC ? TZC : a.tz;  // compile-time tile width when TZC > 0
-  const int gsz = TZ * L::P;
-  const int grp = threadIdx.x / gsz, l = threadIdx.x - grp * gsz;
-  const int c = l % TZ, t = l / TZ;
-  const int kz0 = blockIdx.x * TZ, ky = blockIdx.y;
   const int h = a.h, n1 = a.n1, HH = n1 / 2;
   const long long fstride = (long long)a.n0 * n1 * h;
   const int rstride = n1 * h;
   const int region = L::PAD * TZ;
   V* rg = smb + grp * region + c;
-  // batched simulations: one sim per blockIdx.z, fields stored sim after sim
-  const V* in_base = a.in + (long long)blockIdx.z * a.F * fstride;
-  V* out_base = a.out + (long long)blockIdx.z * a.G * fstride;
   auto sm = [rg, TZ](int pos) -> V& { return rg[pos * TZ]; };
-  V* part = smb + a.groups * region;  // GM x N0 results of the packed column
-  V v[L::R1];
-  // forward FFT, group grp takes field grp
   const bool fw = grp < a.F;
-  {
-    const V* src = in_base + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
-#pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
-  }
   L::template run<-1>(v, t, sm, a.tw);
   __syncthreads();
   if (fw) {
@@ -675,6 +664,36 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
 #pragma unroll
     for (int i = 0; i < L::R1; ++i) dst[(long long)L::out_pos(t, i) * rstride] = v[i];
   }
+}
+
+
+template <typename T, int N0, int FM, int GM, int TZC, class Op>
+__global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
+  using L = Line<T, N0>;
+  using V = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* smb = reinterpret_cast<V*>(smraw);
+  const int TZ = TZC ? TZC : a.tz;  // compile-time tile width when TZC > 0
+  const int gsz = TZ * L::P;
+  const int grp = threadIdx.x / gsz, l = threadIdx.x - grp * gsz;
+  const int c = l % TZ, t = l / TZ;
+  const int kz0 = blockIdx.x * TZ, ky = blockIdx.y;
+  const int h = a.h, n1 = a.n1;
+  const long long fstride = (long long)a.n0 * n1 * h;
+  const int rstride = n1 * h;
+  // batched simulations: one sim per blockIdx.z, fields stored sim after sim
+  const V* in_base = a.in + (long long)blockIdx.z * a.F * fstride;
+  V* out_base = a.out + (long long)blockIdx.z * a.G * fstride;
+  V* part = smb + a.groups * (L::PAD * TZ);  // GM x N0 results of the packed column
+  V v[L::R1];
+  // forward FFT input, group grp takes field grp
+  const bool fw = grp < a.F;
+  {
+    const V* src = in_base + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
+#pragma unroll
+    for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
+  }
+  xpass_tile<T, N0, FM, GM, Op>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v);
 }
 
 // ---------------------------------------------------------------------------

@@ -171,6 +171,8 @@ def lib() -> C.CDLL:
         "gs_precip_adjoint_backward": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(C.c_double), vp, vp, vp]),
         "gs_precip_adjoint_device_bytes": (C.c_size_t, [vp]),
         "gs_precip_adjoint_set_seed": (C.c_int, [vp, vp, vp, C.c_int]),
+        "gs_set_x_prefetch": (None, [C.c_int]),
+        "gs_x_prefetch_timeouts": (C.c_uint, []),
         "gs_sim_set_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_get_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(GsSchedule)]),

@@ -219,6 +219,17 @@ int gs_sim_set_schedule(gs_sim* s, const gs_schedule* sc);
 int gs_sim_get_schedule(const gs_sim* s, gs_schedule* sc);
 int gs_sim_autotune(gs_sim* s, int reps, void* stream, gs_schedule* chosen);
 
+/* gs_set_x_prefetch(1): x passes launched after the call, for three-field
+ * FP32 simulations with n0 = 128 or 256 and an octant B table, run as a
+ * persistent kernel that has the TMA unit fetch its next column tile while
+ * it transforms the current one (the same bits as the one-tile-per-block x
+ * pass; captured graphs keep the kernel they captured).  Off by default: it
+ * measured no faster.  gs_x_prefetch_timeouts counts waits for a fetched
+ * tile that gave up after about a second (the block then ends early); it
+ * stays 0 on a healthy GPU.  No counterpart in the reference. */
+void gs_set_x_prefetch(int on);
+unsigned int gs_x_prefetch_timeouts(void);
+
 /* ---- a martensite step that allocates nothing -------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory when they step: a host whose pool allocator owns all of the GPU's
