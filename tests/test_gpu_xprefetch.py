@@ -43,3 +43,26 @@ def test_prefetched_x_pass_rectangular(gb):
     a, _ = run(gb, p, eta0, 3, True)
     b, _ = run(gb, p, eta0, 3, False)
     assert np.array_equal(a, b)
+
+
+def test_prefetched_x_pass_precipitate_bits_equal_plain(gb):
+    """Five fields (four variants and the concentration) in the elastic
+    chain of the precipitate step."""
+    p = gb.precip3d_params(128, dtype=gb.GS_DTYPE_F32)
+    c0 = gb.initial_c(p, 2)
+    e0 = gb.initial_eta(p, 3, 0.3)
+    out = []
+    for on in (1, 0):
+        gb.lib().gs_set_x_prefetch(on)
+        try:
+            sim = gb.Sim(p)
+            try:
+                sim.set_field("concentration", c0)
+                sim.set_field("eta", e0)
+                sim.step(3)
+                out.append((sim.eta(np.float32), sim.concentration(np.float32)))
+            finally:
+                sim.close()
+        finally:
+            gb.lib().gs_set_x_prefetch(0)
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
