@@ -77,7 +77,7 @@ def build_frontend() -> str:
     srcs = [os.path.join(HOST, f) for f in HOST_SOURCES]
     deps = srcs + [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")] + [LIB]
     if _stale(GSI, deps):
-        _run(["g++", "-O2", "-std=c++17", "-Wall", "-o", GSI, *srcs, "-L" + HERE, "-lgsb200",
+        _run(["g++", "-O2", "-std=c++17", "-Wall", "-pthread", "-o", GSI, *srcs, "-L" + HERE, "-lgsb200",
               "-Wl,-rpath,$ORIGIN"])
     return GSI
 

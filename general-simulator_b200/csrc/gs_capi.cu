@@ -9,6 +9,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <string>
 #include <mutex>
@@ -951,8 +953,11 @@ template <typename T> static int stress_step(gs_sim* s, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 static size_t elt(const gs_sim* s) { return s->p.dtype == GS_DTYPE_F64 ? 8 : 4; }
 
+static void free_snaps(gs_sim* s);
+
 static void free_sim(gs_sim* s) {
   if (!s) return;
+  free_snaps(s);
   void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->rbuf, s->mubuf,
                   s->stressbuf, s->ktab, s->tw, s->partials, s->red, s->btab, s->d_mcs, s->d_simscale};
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
@@ -2756,3 +2761,159 @@ extern "C" int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, co
 extern "C" void gs_set_x_prefetch(int on) { set_x_prefetch(on != 0); }
 
 extern "C" unsigned int gs_x_prefetch_timeouts(void) { return x_wait_timeouts(); }
+
+// ---------------------------------------------------------------------------
+// asynchronous field copies: a dump that overlaps the steps after it
+// ---------------------------------------------------------------------------
+// gs_sim_copy_field_async snapshots the field on the device (a device-to-
+// device copy on the stepping stream, ordered after the steps already
+// issued, so the next steps may overwrite the field at once), then copies the
+// snapshot to page-locked staging memory on the simulation's copy stream.
+// gs_sim_copy_field_wait waits for that copy and converts it into the
+// caller's buffer.  Two copies can be in flight per simulation; a third
+// waits (up to two minutes) for a gs_sim_copy_field_wait to free a slot.
+struct gs_snapslot {
+  void* dev = nullptr;
+  size_t dev_bytes = 0;
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  cudaEvent_t taken = nullptr;   // snapshot done (stepping stream)
+  cudaEvent_t landed = nullptr;  // staging copy done (copy stream)
+  size_t count = 0;
+  int ticket = 0;  // 0: free
+};
+
+struct gs_snaps {
+  static constexpr int kSlots = 2;
+  gs_snapslot slot[kSlots];
+  cudaStream_t copy = nullptr;
+  int next = 1;
+  std::mutex mu;
+  std::condition_variable cv;
+};
+
+static void free_snaps(gs_sim* s) {
+  gs_snaps* q = s->snaps;
+  if (!q) return;
+  for (gs_snapslot& sl : q->slot) {
+    if (sl.landed) cudaEventSynchronize(sl.landed);
+    if (sl.dev) cudaFree(sl.dev);
+    if (sl.pinned) cudaFreeHost(sl.pinned);
+    if (sl.taken) cudaEventDestroy(sl.taken);
+    if (sl.landed) cudaEventDestroy(sl.landed);
+  }
+  if (q->copy) cudaStreamDestroy(q->copy);
+  delete q;
+  s->snaps = nullptr;
+}
+
+// device address and value count of a field the dumps ask for
+static int field_source(gs_sim* s, const std::string& nm, const void** src, size_t* count) {
+  const size_t N = (size_t)s->N;
+  if (nm == "eta") {
+    *src = s->eta[s->cur];
+    *count = N * s->p.nvariants;
+  } else if (nm == "concentration" && s->conc) {
+    *src = s->conc;
+    *count = N;
+  } else if (nm == "stress" && s->stressbuf) {
+    *src = s->stressbuf;
+    *count = 6 * N;
+  } else if (nm == "defect" && s->defect) {
+    *src = s->defect;
+    *count = N;
+  } else {
+    return gs_set_error(GS_EINVAL, "gs_sim_copy_field_async: no field '%s' in this simulation", nm.c_str());
+  }
+  return GS_OK;
+}
+
+extern "C" int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, int* ticket) {
+  if (!s || !name || !ticket) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_async: null argument");
+  const void* src = nullptr;
+  size_t count = 0;
+  GS_TRY(field_source(s, name, &src, &count));
+  if (!s->snaps) {
+    gs_snaps* q = new gs_snaps();
+    if (cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess) {
+      delete q;
+      return gs_set_error(GS_ECUDA, "copy stream: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    s->snaps = q;
+  }
+  gs_snaps* q = s->snaps;
+  std::unique_lock<std::mutex> lk(q->mu);
+  auto free_slot = [q]() {
+    for (int i = 0; i < gs_snaps::kSlots; ++i)
+      if (!q->slot[i].ticket) return i;
+    return -1;
+  };
+  if (!q->cv.wait_for(lk, std::chrono::seconds(120), [&] { return free_slot() >= 0; }))
+    return gs_set_error(GS_ETIMEOUT, "gs_sim_copy_field_async: both copy slots still wait for gs_sim_copy_field_wait");
+  gs_snapslot& sl = q->slot[free_slot()];
+  const size_t bytes = count * elt(s);
+  if (sl.dev_bytes < bytes) {
+    if (sl.dev) cudaFree(sl.dev);
+    sl.dev = nullptr;
+    sl.dev_bytes = 0;
+    GS_CU(cudaMalloc(&sl.dev, bytes), "snapshot buffer");
+    sl.dev_bytes = bytes;
+  }
+  if (sl.pinned_bytes < bytes) {
+    if (sl.pinned) cudaFreeHost(sl.pinned);
+    sl.pinned = nullptr;
+    sl.pinned_bytes = 0;
+    GS_CU(cudaMallocHost(&sl.pinned, bytes), "page-locked staging");
+    sl.pinned_bytes = bytes;
+  }
+  if (!sl.taken) GS_CU(cudaEventCreateWithFlags(&sl.taken, cudaEventDisableTiming), "event");
+  if (!sl.landed) GS_CU(cudaEventCreateWithFlags(&sl.landed, cudaEventDisableTiming), "event");
+  cudaStream_t st = pick_stream(s, stream);
+  GS_CU(cudaMemcpyAsync(sl.dev, src, bytes, cudaMemcpyDeviceToDevice, st), "snapshot");
+  GS_CU(cudaEventRecord(sl.taken, st), "event");
+  GS_CU(cudaStreamWaitEvent(q->copy, sl.taken, 0), "event wait");
+  GS_CU(cudaMemcpyAsync(sl.pinned, sl.dev, bytes, cudaMemcpyDeviceToHost, q->copy), "snapshot D2H");
+  GS_CU(cudaEventRecord(sl.landed, q->copy), "event");
+  sl.count = count;
+  sl.ticket = q->next++;
+  if (q->next <= 0) q->next = 1;
+  *ticket = sl.ticket;
+  return GS_OK;
+}
+
+extern "C" int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t count, int dtype) {
+  if (!s || !host || ticket <= 0) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: bad argument");
+  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  gs_snaps* q = s->snaps;
+  if (!q) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: no copy in flight");
+  gs_snapslot* sl = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(q->mu);
+    for (gs_snapslot& x : q->slot)
+      if (x.ticket == ticket) sl = &x;
+  }
+  if (!sl) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: unknown ticket %d", ticket);
+  int rc = GS_OK;
+  if (count != sl->count) {
+    rc = gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: %zu values asked, the copy holds %zu", count, sl->count);
+  } else if ((rc = gs_cuda_check(cudaEventSynchronize(sl->landed), "copy wait")) == GS_OK) {
+    const bool f64 = s->p.dtype == GS_DTYPE_F64;
+    if ((dtype == GS_DTYPE_F64) == f64) {
+      memcpy(host, sl->pinned, count * elt(s));
+    } else if (f64) {
+      const double* a = static_cast<const double*>(sl->pinned);
+      float* b = static_cast<float*>(host);
+      for (size_t i = 0; i < count; ++i) b[i] = (float)a[i];
+    } else {
+      const float* a = static_cast<const float*>(sl->pinned);
+      double* b = static_cast<double*>(host);
+      for (size_t i = 0; i < count; ++i) b[i] = (double)a[i];
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(q->mu);
+    sl->ticket = 0;
+  }
+  q->cv.notify_all();
+  return rc;
+}

@@ -8,6 +8,7 @@
 #include "../../include/gs_capi.h"
 
 struct gs_plain_state;  // cuFFT comparator buffers (gs_plain.cu)
+struct gs_snaps;        // asynchronous field copies in flight (gs_capi.cu)
 
 struct gs_sim {
   gs_params p;
@@ -71,6 +72,7 @@ struct gs_sim {
   cudaEvent_t marks[kMaxMarks] = {};
   int nmarks = 0;
   bool profiling = false;
+  gs_snaps* snaps = nullptr;  // created by the first gs_sim_copy_field_async
 };
 
 // record a pass boundary when gs_sim_profile_step is active

@@ -152,15 +152,50 @@ void Driver::info_out() {
   log() << "\n";
 }
 
+// Join the oldest asynchronous dumps until at most `keep` are in flight; the
+// joined fields go into the store, as a synchronous dump leaves them.
+int Driver::finish_dumps(size_t keep) {
+  int rc = kNormal;
+  while (pending_.size() > keep) {
+    PendingDump p = std::move(pending_.front());
+    pending_.pop_front();
+    auto r = p.done.get();
+    if (!r.first.empty()) {
+      log() << "Error: dump of " << p.name << ": " << r.first << "\n";
+      rc = kErr;
+    } else {
+      datas[p.name] = std::move(r.second);
+    }
+  }
+  return rc;
+}
+
 void Driver::dump_out() {
   Dynamics* d = current();
   std::string mode = dump_mode_;
+  std::string a;
+  const bool async = !(vars.has("asyncdump") && (a = vars["asyncdump"], a == "0" || a == "off"));
   while (!mode.empty()) {
     const std::string name = take_word(mode);
     if (name.empty()) continue;
+    const std::string file = dump_folder_ + "/" + name + "." + std::to_string(step_) + ".data";
+    Dynamics::DumpJob job = async ? d->DumpAsync(name) : Dynamics::DumpJob();
+    if (job) {
+      // host memory stays bounded: at most two dumps wait for their writer
+      finish_dumps(1);
+      const bool binary = binary_;
+      pending_.push_back({name, std::async(std::launch::async, [job, file, binary]() {
+                            Field f;
+                            std::string err = job(f);
+                            if (err.empty() && !(binary ? f.write_binary(file) : f.write_text(file)))
+                              err = "cannot write " + file;
+                            return std::make_pair(err, std::move(f));
+                          })});
+      continue;
+    }
     d->SyncToHost(name);
     if (datas.has(name)) {
-      dump_field(name, dump_folder_ + "/" + name + "." + std::to_string(step_) + ".data");
+      dump_field(name, file);
     } else {
       log() << "Error: data " << name << " does not exist!\n";
     }
@@ -203,8 +238,9 @@ int Driver::run(std::string args) {
     if (report) info_out();
     if ((i % dump_every == 0) || i == total) dump_out();
   }
+  const int rc = finish_dumps(0);
   log().flush();
-  return kNormal;
+  return rc;
 }
 
 int Driver::runfunc(std::string func) {

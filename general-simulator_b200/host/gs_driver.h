@@ -6,14 +6,22 @@
 // on the device behind the C ABI: SyncToHost copies a field into the store
 // before `dump` / `write` / `writehere`, and WillReport tells the plugin that
 // an info line follows the next Calculate (so force means can be taken from
-// the state the step starts from, as the reference reports them).
+// the state the step starts from, as the reference reports them).  A third,
+// DumpAsync, lets `dump` overlap the steps after it: the plugin snapshots the
+// field on the device and returns a job that waits for the copy and fills a
+// host Field, which a writer thread then writes (`set asyncdump 0` dumps
+// synchronously, as the reference does).
 //
 // Driver is GS (src/gs.cu, src/gs.h): `sys` registry, `set`, `link`,
 // `read`, `readhere`, `write`, `writehere`, `info`, `dump`, `run`, `runfunc`.
 #pragma once
+#include <deque>
+#include <functional>
+#include <future>
 #include <map>
 #include <memory>
 #include <string>
+#include <utility>
 
 #include "gs_data.h"
 #include "gs_script.h"
@@ -34,6 +42,11 @@ class Dynamics {
   virtual std::string Get(std::string key) = 0;
   virtual int SyncToHost(const std::string& field) { (void)field; return kNormal; }
   virtual void WillReport(bool) {}
+  // Start copying `field` off the device for a dump; the returned job (run on
+  // another thread) waits for the copy, fills its Field and returns 0, or a
+  // message.  An empty job: no asynchronous copy for this field.
+  using DumpJob = std::function<std::string(Field&)>;
+  virtual DumpJob DumpAsync(const std::string& field) { (void)field; return {}; }
 };
 
 // factory of the registered plugins: mart, precipitate, stress, cores, pow
@@ -64,6 +77,13 @@ class Driver {
   void info_out();
   void dump_out();
   void dump_field(const std::string& name, const std::string& file);
+  // asynchronous dumps in flight: field name, writer (copy wait + file write)
+  struct PendingDump {
+    std::string name;
+    std::future<std::pair<std::string, Field>> done;
+  };
+  std::deque<PendingDump> pending_;
+  int finish_dumps(size_t keep);  // join all but `keep` of them, oldest first
   std::map<std::string, std::unique_ptr<Dynamics>> systems_;
   std::map<std::string, bool> inited_;
   std::string name_;

@@ -118,6 +118,18 @@ struct PhysicsBase : Dynamics {
     return kNormal;
   }
 
+  // the asynchronous dump job of a device field of extents `dims`
+  Dynamics::DumpJob async_dump(const char* name, std::vector<int> dims) {
+    int ticket = 0;
+    if (gs_sim_copy_field_async(sim, name, nullptr, &ticket) != GS_OK) return {};
+    gs_sim* h = sim;
+    return [h, ticket, dims](Field& f) -> std::string {
+      f.init(dims);
+      if (gs_sim_copy_field_wait(h, ticket, f.v.data(), f.n(), GS_DTYPE_F32) != GS_OK) return capi_error();
+      return std::string();
+    };
+  }
+
   int sync(const char* name, std::vector<int> dims) {
     Field& f = (*Datas)[name];
     size_t n = 1;
@@ -278,6 +290,10 @@ class Mart : public PhysicsBase {
     if (name == "eta") return sync("eta", {V, nx, ny, nz});
     return kNormal;
   }
+  DumpJob DumpAsync(const std::string& name) override {
+    if (name == "eta") return async_dump("eta", {V, nx, ny, nz});
+    return {};
+  }
 };
 
 class Precipitate : public PhysicsBase {
@@ -361,6 +377,11 @@ class Precipitate : public PhysicsBase {
     if (name == "concentration") return sync("concentration", {nx, ny, nz});
     return kNormal;
   }
+  DumpJob DumpAsync(const std::string& name) override {
+    if (name == "eta") return async_dump("eta", {V, nx, ny, nz});
+    if (name == "concentration") return async_dump("concentration", {nx, ny, nz});
+    return {};
+  }
 };
 
 class Stress : public PhysicsBase {
@@ -386,6 +407,11 @@ class Stress : public PhysicsBase {
     if (name == "stress") return sync("stress", {6, nx, ny, nz});
     if (name == "defect") return sync("defect", {nx, ny, nz});
     return kNormal;
+  }
+  DumpJob DumpAsync(const std::string& name) override {
+    if (name == "stress") return async_dump("stress", {6, nx, ny, nz});
+    if (name == "defect") return async_dump("defect", {nx, ny, nz});
+    return {};
   }
 };
 

@@ -172,6 +172,20 @@ int gs_sim_stats(gs_sim* s, gs_stats* out, void* stream);
  * "eta", "spectrum", and "btable" (the octant table of B(k) when the
  * martensite contraction reads one, else NULL and 0 bytes). */
 int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes);
+
+/* A field copy that overlaps the steps after it (the `dump` of a running
+ * script; the reference dumps synchronously, GS::Run src/gs.cu:168-212 with
+ * Data::Dump).  gs_sim_copy_field_async takes a device-side snapshot of the
+ * field ("eta", "concentration", "stress", "defect") on `stream` (NULL: the
+ * simulation's own), after the steps already issued there, and starts its
+ * copy to library-owned page-locked memory; later steps may be issued at
+ * once.  gs_sim_copy_field_wait(ticket) waits for that copy and writes
+ * `count` values of dtype to `host`; it may run on another host thread than
+ * the stepping one.  Two copies per simulation can be in flight; a third
+ * call waits up to two minutes for a slot (GS_ETIMEOUT).  Every ticket must
+ * be waited for once. */
+int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, int* ticket);
+int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t count, int dtype);
 /* Run one step with a CUDA event between consecutive passes on the step's
  * stream; pass_ms[i] receives the device time of pass i (in launch order:
  * z forward, y forward, x contraction, y inverse, update for the

@@ -207,3 +207,25 @@ print since time point {x1} to time point {x2}, {x2-x1} seconds have passed.
     assert m, out
     x1, x2, d = map(int, m.groups())
     assert d == x2 - x1 and 1 <= d <= 3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["mart", "precipitate", "stress"])
+def test_async_dumps_equal_synchronous_dumps(gsi, tmp_path, case):
+    """`dump` overlaps the following steps (device snapshot, copy and file
+    write off the stepping thread); the files must equal those of the
+    synchronous dump (`set asyncdump 0`) byte for byte."""
+    script, inputs = {"mart": (mf.mart_script, mf.mart_inputs), "precipitate": (mf.precip_script, mf.precip_inputs),
+                      "stress": (mf.stress_script, mf.stress_inputs)}[case]
+    files = {}
+    for mode in ("async", "sync"):
+        d = tmp_path / mode
+        d.mkdir()
+        text = script()
+        if mode == "sync":
+            text = "set asyncdump 0\n" + text
+        run_script(gsi, d, "in." + case, text, inputs())
+        files[mode] = {p.name: p.read_bytes() for p in sorted((d / "dumpdir").iterdir())}
+    assert files["async"] and files["async"].keys() == files["sync"].keys()
+    for k in files["async"]:
+        assert files["async"][k] == files["sync"][k], k
