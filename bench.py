@@ -11,9 +11,14 @@ collective, so `value` is the whole-job aggregate of N replicas ("weak").
 value   -- device time of K steps on resident HBM data, CUDA events on the
            launching stream, max over ranks.
 e2e     -- the same metric through the C ABI with host buffers: every step
-           uploads the field set from pinned host memory (gs_sim_set_field),
-           steps once (gs_sim_step) and reads the field set back
-           (gs_sim_get_field); host clock around device synchronisation.
+           uploads the field set from pinned host memory
+           (gs_sim_set_field_async), steps once (gs_sim_step) and reads the
+           field set back into pinned host memory (gs_sim_copy_field_async +
+           gs_sim_copy_field_wait), so that step k's download overlaps step
+           k+1's upload on the two directions of the host link; every copy
+           is waited for inside the timed region; host clock.  The
+           one-at-a-time variant (gs_sim_set_field, gs_sim_step,
+           gs_sim_get_field) is reported beside it as "serial".
 roofline-- the dominant pass, timed live with CUDA events between passes
            (gs_sim_profile_step), algorithmic bytes / time vs measured HBM.
 """
@@ -548,12 +553,40 @@ def run_ours(args, ws, rank, local):
             sim.step(1, sh)
             gb.check(L.gs_sim_get_field(sim.h, b"eta", ptr_out, V * N, 0), "get_field")
         torch.cuda.synchronize()
+        serial_s = time.perf_counter() - t0
+        # pipelined: two page-locked output buffers, step k's download in
+        # flight while step k+1 uploads and runs
+        out2 = [out_pinned, torch.empty(V * N, dtype=torch.float32).pin_memory()]
+        tk = C.c_int(0)
+
+        def pipelined(k):
+            prev = None
+            for i in range(k):
+                gb.check(L.gs_sim_set_field_async(sim.h, b"eta", ptr_in, V * N, 0, C.c_void_p(sh)), "upload")
+                sim.step(1, sh)
+                gb.check(L.gs_sim_copy_field_async(sim.h, b"eta", C.c_void_p(sh),
+                                                   C.c_void_p(out2[i % 2].data_ptr()), C.byref(tk)), "download")
+                if prev is not None:
+                    gb.check(L.gs_sim_copy_field_wait(sim.h, prev, None, 0, 0), "download wait")
+                prev = tk.value
+            gb.check(L.gs_sim_copy_field_wait(sim.h, prev, None, 0, 0), "download wait")
+
+        pipelined(2)
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        pipelined(args.e2e_steps)
+        torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, ws)
+    serial_s = max_over_ranks(serial_s, ws)
     e2e = {"value": N * args.e2e_steps * ws / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * V * N,
            "d2h_bytes_per_step": 4 * V * N, "steps": args.e2e_steps,
-           "how": "per step: gs_sim_set_field(eta, pinned host) + gs_sim_step(1) + gs_sim_get_field(eta, pinned "
-                  "host); host clock with device synchronisation"}
+           "how": "per step: gs_sim_set_field_async(eta, pinned host) + gs_sim_step(1) + gs_sim_copy_field_async"
+                  "(eta, into pinned host) + gs_sim_copy_field_wait of the previous step's download; the last "
+                  "download is waited for inside the timed region; host clock",
+           "serial": {"value": N * args.e2e_steps * ws / serial_s,
+                      "how": "per step: gs_sim_set_field + gs_sim_step(1) + gs_sim_get_field, one after the other"}}
     sim.close()
 
     if rank != 0:

@@ -2780,7 +2780,8 @@ struct gs_snapslot {
   cudaEvent_t taken = nullptr;   // snapshot done (stepping stream)
   cudaEvent_t landed = nullptr;  // staging copy done (copy stream)
   size_t count = 0;
-  int ticket = 0;  // 0: free
+  bool direct = false;  // copied straight into the caller's page-locked buffer
+  int ticket = 0;       // 0: free
 };
 
 struct gs_snaps {
@@ -2828,7 +2829,7 @@ static int field_source(gs_sim* s, const std::string& nm, const void** src, size
   return GS_OK;
 }
 
-extern "C" int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, int* ticket) {
+extern "C" int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, void* pinned_dst, int* ticket) {
   if (!s || !name || !ticket) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_async: null argument");
   const void* src = nullptr;
   size_t count = 0;
@@ -2859,7 +2860,7 @@ extern "C" int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream
     GS_CU(cudaMalloc(&sl.dev, bytes), "snapshot buffer");
     sl.dev_bytes = bytes;
   }
-  if (sl.pinned_bytes < bytes) {
+  if (!pinned_dst && sl.pinned_bytes < bytes) {
     if (sl.pinned) cudaFreeHost(sl.pinned);
     sl.pinned = nullptr;
     sl.pinned_bytes = 0;
@@ -2872,8 +2873,10 @@ extern "C" int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream
   GS_CU(cudaMemcpyAsync(sl.dev, src, bytes, cudaMemcpyDeviceToDevice, st), "snapshot");
   GS_CU(cudaEventRecord(sl.taken, st), "event");
   GS_CU(cudaStreamWaitEvent(q->copy, sl.taken, 0), "event wait");
-  GS_CU(cudaMemcpyAsync(sl.pinned, sl.dev, bytes, cudaMemcpyDeviceToHost, q->copy), "snapshot D2H");
+  GS_CU(cudaMemcpyAsync(pinned_dst ? pinned_dst : sl.pinned, sl.dev, bytes, cudaMemcpyDeviceToHost, q->copy),
+        "snapshot D2H");
   GS_CU(cudaEventRecord(sl.landed, q->copy), "event");
+  sl.direct = pinned_dst != nullptr;
   sl.count = count;
   sl.ticket = q->next++;
   if (q->next <= 0) q->next = 1;
@@ -2882,8 +2885,7 @@ extern "C" int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream
 }
 
 extern "C" int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t count, int dtype) {
-  if (!s || !host || ticket <= 0) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: bad argument");
-  if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
+  if (!s || ticket <= 0) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: bad argument");
   gs_snaps* q = s->snaps;
   if (!q) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: no copy in flight");
   gs_snapslot* sl = nullptr;
@@ -2894,7 +2896,13 @@ extern "C" int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t 
   }
   if (!sl) return gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: unknown ticket %d", ticket);
   int rc = GS_OK;
-  if (count != sl->count) {
+  if (sl->direct) {  // the values are already in the caller's buffer
+    rc = gs_cuda_check(cudaEventSynchronize(sl->landed), "copy wait");
+  } else if (!host || (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64)) {
+    cudaEventSynchronize(sl->landed);
+    rc = gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: a host buffer of dtype 0 or 1 is needed");
+  } else if (count != sl->count) {
+    cudaEventSynchronize(sl->landed);
     rc = gs_set_error(GS_EINVAL, "gs_sim_copy_field_wait: %zu values asked, the copy holds %zu", count, sl->count);
   } else if ((rc = gs_cuda_check(cudaEventSynchronize(sl->landed), "copy wait")) == GS_OK) {
     const bool f64 = s->p.dtype == GS_DTYPE_F64;
@@ -2916,4 +2924,23 @@ extern "C" int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t 
   }
   q->cv.notify_all();
   return rc;
+}
+
+// An upload on a stream: the asynchronous counterpart of gs_sim_set_field for
+// the field set ("eta") in the simulation's own dtype.  From page-locked
+// memory the copy overlaps whatever else runs (a download of the previous
+// state on the copy stream, say); the caller keeps `host` unchanged until
+// the stream has passed the copy.
+extern "C" int gs_sim_set_field_async(gs_sim* s, const char* name, const void* host, size_t count, int dtype,
+                                      void* stream) {
+  if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_set_field_async: null argument");
+  if (std::string(name) != "eta") return gs_set_error(GS_EINVAL, "gs_sim_set_field_async: only \"eta\"");
+  if (dtype != s->p.dtype) return gs_set_error(GS_EINVAL, "gs_sim_set_field_async: dtype must be the simulation's");
+  const size_t n = (size_t)s->N * s->p.nvariants;
+  if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
+  sim_graph_reset(s);
+  s->spec_ready = false;
+  cudaStream_t st = pick_stream(s, stream);
+  GS_CU(cudaMemcpyAsync(s->eta[s->cur], host, n * elt(s), cudaMemcpyHostToDevice, st), "upload");
+  return GS_OK;
 }

@@ -172,6 +172,9 @@ def lib() -> C.CDLL:
         "gs_precip_adjoint_device_bytes": (C.c_size_t, [vp]),
         "gs_precip_adjoint_set_seed": (C.c_int, [vp, vp, vp, C.c_int]),
         "gs_set_x_prefetch": (None, [C.c_int]),
+        "gs_sim_copy_field_async": (C.c_int, [vp, C.c_char_p, vp, vp, C.POINTER(C.c_int)]),
+        "gs_sim_copy_field_wait": (C.c_int, [vp, C.c_int, vp, C.c_size_t, C.c_int]),
+        "gs_sim_set_field_async": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.c_int, vp]),
         "gs_x_prefetch_timeouts": (C.c_uint, []),
         "gs_sim_set_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),
         "gs_sim_get_schedule": (C.c_int, [vp, C.POINTER(GsSchedule)]),

@@ -121,7 +121,7 @@ struct PhysicsBase : Dynamics {
   // the asynchronous dump job of a device field of extents `dims`
   Dynamics::DumpJob async_dump(const char* name, std::vector<int> dims) {
     int ticket = 0;
-    if (gs_sim_copy_field_async(sim, name, nullptr, &ticket) != GS_OK) return {};
+    if (gs_sim_copy_field_async(sim, name, nullptr, nullptr, &ticket) != GS_OK) return {};
     gs_sim* h = sim;
     return [h, ticket, dims](Field& f) -> std::string {
       f.init(dims);

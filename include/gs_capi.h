@@ -178,14 +178,21 @@ int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes)
  * Data::Dump).  gs_sim_copy_field_async takes a device-side snapshot of the
  * field ("eta", "concentration", "stress", "defect") on `stream` (NULL: the
  * simulation's own), after the steps already issued there, and starts its
- * copy to library-owned page-locked memory; later steps may be issued at
- * once.  gs_sim_copy_field_wait(ticket) waits for that copy and writes
- * `count` values of dtype to `host`; it may run on another host thread than
- * the stepping one.  Two copies per simulation can be in flight; a third
- * call waits up to two minutes for a slot (GS_ETIMEOUT).  Every ticket must
- * be waited for once. */
-int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, int* ticket);
+ * copy to the host on a copy stream; later steps may be issued at once.  The
+ * copy goes to library-owned page-locked memory, or, when pinned_dst is not
+ * NULL, straight into that caller-owned page-locked buffer of the
+ * simulation's dtype (which must hold the whole field).
+ * gs_sim_copy_field_wait(ticket) waits for the copy and, for a library-owned
+ * one, writes `count` values of dtype to `host` (for a direct one host may be
+ * NULL); it may run on another host thread than the stepping one.  Two copies
+ * per simulation can be in flight; a third call waits up to two minutes for
+ * a slot (GS_ETIMEOUT).  Every ticket must be waited for once.
+ * gs_sim_set_field_async uploads "eta" in the simulation's dtype on `stream`
+ * without waiting (page-locked `host` overlaps the copy with other work;
+ * `host` must stay unchanged until the stream has passed it). */
+int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, void* pinned_dst, int* ticket);
 int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t count, int dtype);
+int gs_sim_set_field_async(gs_sim* s, const char* name, const void* host, size_t count, int dtype, void* stream);
 /* Run one step with a CUDA event between consecutive passes on the step's
  * stream; pass_ms[i] receives the device time of pass i (in launch order:
  * z forward, y forward, x contraction, y inverse, update for the
