@@ -2,9 +2,6 @@
 // the input spectra, persistent grid of two blocks per SM.
 #include <cudaTypedefs.h>
 
-#include <cstdio>
-#include <cstdlib>
-
 #include "gs_launch.h"
 #include "gs_xtma.cuh"
 
@@ -83,12 +80,6 @@ template <int N0, int FM, int TZ> static cudaError_t xtma_n(XArgs<float>& a, cud
   const int ntiles = (a.h / TZ) * a.n1;
   int grid = per_sm * sm_count();
   if (grid > ntiles) grid = ntiles;
-  static bool told = false;
-  if (!told && getenv("GS_VERBOSE")) {
-    fprintf(stderr, "x pass (TMA-fed, n0 %d): %d blocks per SM, %zu B shared, grid %d, %d tiles\n", N0, per_sm, smem,
-            grid, ntiles);
-    told = true;
-  }
   k_xpass_tma<N0, FM, TZ, TableOp><<<grid, Sh::threads, smem, s>>>(a, map, ntiles);
   return cudaGetLastError();
 }

@@ -234,7 +234,10 @@ int Driver::run(std::string args) {
     d->Fix((float)i / (float)total);
     const bool report = (i % info_every == 0) || i == total;
     d->WillReport(report && !info_mode_.empty());
-    if (d->Calculate() != kNormal) return kErr;
+    if (d->Calculate() != kNormal) {
+      finish_dumps(0);
+      return kErr;
+    }
     if (report) info_out();
     if ((i % dump_every == 0) || i == total) dump_out();
   }
