@@ -153,7 +153,8 @@ template <typename T, int N> struct Line {
   // order on exit.  sm(pos) returns a reference to the line's shared element
   // at padded position pos.  tw: w_N^m = exp(-2 pi i m / N), m < N.
   // Every thread of the block must call this (it synchronises the block).
-  template <int DIR, class SM>
+  // TWS: tw is in shared memory (plain loads) instead of global memory.
+  template <int DIR, bool TWS = false, class SM>
   __device__ __forceinline__ static void run(V (&v)[R1], int t, SM sm, const V* __restrict__ tw) {
     Dft<R1, DIR>::run(v);
     if constexpr (R2 == 1) {
@@ -170,7 +171,7 @@ template <typename T, int N> struct Line {
       for (int r = 0; r < R2; ++r) {
         V x = sm(spos(j + r * R1));
         if (r > 0) {
-          V w = __ldg(&tw[r * j]);
+          V w = TWS ? tw[r * j] : __ldg(&tw[r * j]);
           if (DIR > 0) w.y = -w.y;
           x = cmul(x, w);
         }

@@ -16,8 +16,8 @@ template <typename T, int N0, int FM, int GM, class Op> static cudaError_t xc_n(
   int tz = pick_tz(a.h);
   if (sizeof(T) == 4 && N0 >= 64 && tz > 8) tz = 8;
   if (a.tz_req > 0 && (a.tz_req & (a.tz_req - 1)) == 0 && a.h % a.tz_req == 0) tz = a.tz_req;
-  auto smem_of = [&](int tzv) {
-    return (size_t)groups * tzv * L::PAD * sizeof(cplx<T>) + (size_t)GM * N0 * sizeof(cplx<T>);
+  auto smem_of = [&](int tzv) {  // line regions, packed-column results, twiddles
+    return (size_t)groups * tzv * L::PAD * sizeof(cplx<T>) + (size_t)(GM + 1) * N0 * sizeof(cplx<T>);
   };
   constexpr int maxthr = XBounds<FM, GM>::v;
   while (tz > 1 && (smem_of(tz) > 200 * 1024 || tz * L::P * groups > maxthr)) tz >>= 1;

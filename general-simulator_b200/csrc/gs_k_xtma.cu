@@ -66,7 +66,7 @@ template <int N0, int FM, int TZ> static cudaError_t xtma_n(XArgs<float>& a, cud
   if (a.F != FM) return cudaErrorNotSupported;
   a.tz = TZ;
   a.groups = a.F;
-  const size_t smem = 2 * (size_t)FM * Sh::region_bytes + (size_t)FM * N0 * vb + 2 * sizeof(uint64_t);
+  const size_t smem = 2 * (size_t)FM * Sh::region_bytes + (size_t)(FM + 1) * N0 * vb + 2 * sizeof(uint64_t);
   // two blocks per SM need the largest shared-memory carve-out; the grid is
   // what the occupancy calculator says fits at once
   static int per_sm = 0;

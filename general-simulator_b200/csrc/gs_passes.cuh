@@ -540,10 +540,10 @@ template <int FM, int GM> struct XBounds {
 // per-point operation, inverse FFT, store.  smb: the groups' line regions
 // (region = PAD * TZ values each), part: GM x N0 values for the packed
 // columns.  Shared by the plain and the TMA-fed kernels.
-template <typename T, int N0, int FM, int GM, class Op>
+template <typename T, int N0, int FM, int GM, class Op, bool TWS = false>
 __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx<T>* part, int TZ, int grp, int c,
                                            int t, int kz0, int ky, cplx<T>* out_base,
-                                           cplx<T> (&v)[Line<T, N0>::R1]) {
+                                           cplx<T> (&v)[Line<T, N0>::R1], const cplx<T>* tw) {
   using L = Line<T, N0>;
   using V = cplx<T>;
   const int h = a.h, n1 = a.n1, HH = n1 / 2;
@@ -590,7 +590,7 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
       if constexpr (PAIR) Op::template load<T, FM>(a, nn, kx, kyA, kzA, pre[j]);
     }
   }
-  L::template run<-1>(v, t, sm, a.tw);
+  L::template run<-1, TWS>(v, t, sm, tw);
   __syncthreads();
   if (fw) {
 #pragma unroll
@@ -688,7 +688,7 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
 #pragma unroll
   for (int r = 0; r < L::R1; ++r) v[r] = iv ? sm(L::in_pos(t, r)) : mk2((T)0, (T)0);
   __syncthreads();
-  L::template run<1>(v, t, sm, a.tw);
+  L::template run<1, TWS>(v, t, sm, tw);
   if (iv) {
     V* dst = out_base + grp * fstride + (long long)ky * h + kz0 + c;
 #pragma unroll
@@ -715,6 +715,10 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const V* in_base = a.in + (long long)blockIdx.z * a.F * fstride;
   V* out_base = a.out + (long long)blockIdx.z * a.G * fstride;
   V* part = smb + a.groups * (L::PAD * TZ);  // GM x N0 results of the packed column
+  // the x twiddles in shared memory (read 30 times per thread and tile); the
+  // FFT's first barrier comes before their first use
+  V* tws = part + GM * N0;
+  for (int i = threadIdx.x; i < N0; i += blockDim.x) tws[i] = a.tw[i];
   V v[L::R1];
   // forward FFT input, group grp takes field grp
   const bool fw = grp < a.F;
@@ -723,7 +727,7 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
   }
-  xpass_tile<T, N0, FM, GM, Op>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v);
+  xpass_tile<T, N0, FM, GM, Op, true>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v, tws);
 }
 
 // ---------------------------------------------------------------------------

@@ -103,7 +103,8 @@ __global__ void __launch_bounds__(XTmaShape<N0, FM, TZ>::threads, XTmaShape<N0, 
   const int F = a.F;
   V* const stage0 = reinterpret_cast<V*>(smtma);  // stage s at stage0 + s * F * region
   V* part = stage0 + 2 * F * S::region;           // GM x N0 values of the packed columns
-  uint64_t* bar = reinterpret_cast<uint64_t*>(part + FM * N0);
+  V* tws = part + FM * N0;                          // the x twiddles, as in the plain pass
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tws + N0);
   const int gsz = TZ * L::P;
   const int grp = threadIdx.x / gsz, l = threadIdx.x - grp * gsz;
   const int c = l % TZ, t = l / TZ;
@@ -114,6 +115,7 @@ __global__ void __launch_bounds__(XTmaShape<N0, FM, TZ>::threads, XTmaShape<N0, 
     mbar_arrive_expect_tx(&bar[s], tile_bytes);
     for (int f = 0; f < F; ++f) tma_load_4d(stage0 + (s * F + f) * S::region, &tin, kz0, ky, 0, f, &bar[s]);
   };
+  for (int i = threadIdx.x; i < N0; i += blockDim.x) tws[i] = a.tw[i];
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(XTmaShape<N0, FM, TZ>::threads, XTmaShape<N0, 
       for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[r * L::P * TZ] : mk2((T)0, (T)0);
     }
     __syncthreads();  // the stage becomes the padded working region of the FFTs
-    xpass_tile<T, N0, FM, FM, Op>(a, stage0 + s * F * S::region, part, TZ, grp, c, t, kz0, ky, a.out, v);
+    xpass_tile<T, N0, FM, FM, Op, true>(a, stage0 + s * F * S::region, part, TZ, grp, c, t, kz0, ky, a.out, v, tws);
     __syncthreads();
   }
 }
