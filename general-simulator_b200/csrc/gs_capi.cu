@@ -763,6 +763,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
     pm.c = c;
     pm.eta = eta;
     pm.dst = reinterpret_cast<cplx<T>*>(s->spec2);
+    pm.lr_req = s->sched.update_rows;
     pm.nrows = rows;
     pm.n2 = s->n2;
     pm.F1 = F1;
@@ -809,7 +810,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   za.tw_h = twp<T>(s, 1);
   za.tw_n2 = twp<T>(s, 0);
   if (!fused) {
-    GS_CU(launch_zfwd<T>(za, s->h, st), "z forward (update fields)");
+    GS_CU(launch_zfwd<T>(za, s->h, st, s->sched.z_lines), "z forward (update fields)");
     gs_mark(s, st);
     s->launches += 1;
   }
@@ -819,7 +820,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   ya.n1 = s->n1;
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
-  GS_CU(launch_ypass<T>(ya, s->n1, F2, -1, st), "y forward (update fields)");
+  GS_CU(launch_ypass<T>(ya, s->n1, F2, -1, st, s->sched.y_cols), "y forward (update fields)");
   if (s->n1 > 1) gs_mark(s, st);
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
@@ -836,6 +837,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   xa.F = 2;
   xa.G = 1;
   xa.nsim = G2;
+  xa.tz_req = s->sched.x_cols;
   xa.tw = twp<T>(s, 3);
   xa.pu.V = V;
   xa.pu.mass_proj = p.mass_projection;
@@ -849,7 +851,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   gs_mark(s, st);
   YArgs<T> yo = ya;
   yo.spec = reinterpret_cast<cplx<T>*>(s->spec);
-  GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st), "y inverse (update fields)");
+  GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st, s->sched.y_cols), "y inverse (update fields)");
   if (s->n1 > 1) gs_mark(s, st);
   ZinvArgs<T> zi;
   memset(&zi, 0, sizeof(zi));
@@ -2380,12 +2382,33 @@ extern "C" int gs_sim_get_schedule(const gs_sim* s, gs_schedule* sc) {
 
 extern "C" int gs_sim_autotune(gs_sim* s, int reps, void* stream, gs_schedule* chosen) {
   if (!s) return gs_set_error(GS_EINVAL, "gs_sim_autotune: null sim");
-  if (s->p.model != GS_MODEL_MART || s->plain) return gs_set_error(GS_ENOTSUP, "gs_sim_autotune: martensite only");
+  if (s->plain || s->p.model == GS_MODEL_STRESS)
+    return gs_set_error(GS_ENOTSUP, "gs_sim_autotune: martensite and precipitate simulations only");
   if (reps < 1) reps = 1;
   sim_graph_reset(s);
   cudaStream_t st = pick_stream(s, stream);
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
-  return tune(s, reps, st, [&]() { return f64 ? mart_step<double>(s, st) : mart_step<float>(s, st); }, chosen);
+  if (s->p.model == GS_MODEL_MART)
+    return tune(s, reps, st, [&]() { return f64 ? mart_step<double>(s, st) : mart_step<float>(s, st); }, chosen);
+  // precipitate: the trial steps advance c and eta in place, so the state and
+  // the step counter are kept aside and put back
+  const size_t fb = (size_t)s->N * elt(s), V = (size_t)s->p.nvariants;
+  void* keep = nullptr;
+  GS_CU(cudaMalloc(&keep, fb * (V + 1)), "tuning state copy");
+  const int64_t step0 = s->step;
+  int rc = gs_cuda_check(cudaMemcpyAsync(keep, s->conc, fb, cudaMemcpyDeviceToDevice, st), "keep state");
+  if (rc == GS_OK)
+    rc = gs_cuda_check(
+        cudaMemcpyAsync(static_cast<char*>(keep) + fb, s->eta[0], fb * V, cudaMemcpyDeviceToDevice, st), "keep state");
+  if (rc == GS_OK)
+    rc = tune(s, reps, st, [&]() { return f64 ? precip_step<double>(s, st) : precip_step<float>(s, st); }, chosen);
+  cudaMemcpyAsync(s->conc, keep, fb, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(s->eta[0], static_cast<char*>(keep) + fb, fb * V, cudaMemcpyDeviceToDevice, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(keep);
+  s->step = step0;
+  if (rc == GS_OK) rc = gs_cuda_check(e, "restore state");
+  return rc;
 }
 
 extern "C" int gs_batch_autotune(gs_batch* b, int reps, void* stream) {

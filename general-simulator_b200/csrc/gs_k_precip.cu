@@ -42,6 +42,7 @@ template <typename T, int H, int VM> static cudaError_t pmid_n(PrecipMidArgs<T>&
   const int per = L::P * (2 * a.loc.V + 2);  // threads of one row
   if (per > 256) return cudaErrorInvalidConfiguration;
   long long lr = 256 / per;
+  if (a.lr_req > 0 && (long long)a.lr_req * per <= 256) lr = a.lr_req;
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;
   const int CW = (2 * H) % 4 == 0 ? 4 : 2;

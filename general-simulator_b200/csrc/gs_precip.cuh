@@ -95,6 +95,7 @@ template <typename T> struct PrecipMidArgs {
   const T* c;            // [N]
   const T* eta;          // [V][N]
   cplx<T>* dst;          // [2V+2][rows][H]
+  int lr_req;            // rows per block asked by the schedule (0: the launcher's choice)
   long long nrows;
   int n2, lr, F1;
   const cplx<T>* tw_h;

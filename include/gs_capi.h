@@ -226,12 +226,14 @@ int gs_cores_paint(int nx, int ny, int nz, int nvariants, int ncores, const int*
                    double radius, double c_matrix, double c_core, float* eta_host, float* conc_host);
 
 /* ---- tile schedule and autotuner ---------------------------------------- */
-/* Tile sizes of the martensite passes: z lines per block, y and x columns
- * per block, update rows per block (0 = the launcher's default; sizes a
- * launch cannot take fall back to it).  The reference has no counterpart
- * (cuFFT plans internally).  gs_sim_autotune times candidates with CUDA
- * events over `reps` trial steps that leave the simulation's state as it was
- * (coordinate descent, two sweeps) and keeps the fastest; gs_batch_autotune
+/* Tile sizes of the passes: z lines per block, y and x columns per block,
+ * update rows per block (the martensite update, the precipitate's middle
+ * sweep) (0 = the launcher's default; sizes a launch cannot take fall back
+ * to it).  The reference has no counterpart (cuFFT plans internally).
+ * gs_sim_autotune (martensite and precipitate simulations) times candidates
+ * with CUDA events over `reps` trial steps that leave the simulation's state
+ * and step counter as they were (coordinate descent, two sweeps) and keeps
+ * the fastest; gs_batch_autotune
  * does so per group and drops a captured graph so the next step recaptures. */
 typedef struct gs_schedule {
   int z_lines, y_cols, x_cols, update_rows;

@@ -77,3 +77,26 @@ def test_batch_autotune_matches_untuned(gb):
     assert len(scheds) == 4
     for a, r in zip(got, ref):
         assert np.array_equal(a, r)
+
+
+def test_precipitate_autotune_keeps_state_and_bits(gb):
+    """Tuning a precipitate simulation runs trial steps on a copy of its
+    state; the steps after it match an untuned run bit for bit."""
+    p = gb.precip3d_params(32, dtype=F32)
+    c0 = gb.initial_c(p, 2)
+    e0 = gb.initial_eta(p, 3, 0.3)
+    out = []
+    for tune in (False, True):
+        s = gb.Sim(p)
+        try:
+            s.set_field("concentration", c0)
+            s.set_field("eta", e0)
+            s.step(2)
+            if tune:
+                chosen = s.autotune(reps=2)
+                assert all(v >= 0 for v in chosen.values())
+            s.step(3)
+            out.append((s.concentration(np.float32), s.eta(np.float32)))
+        finally:
+            s.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
