@@ -72,3 +72,31 @@ def test_direct_pinned_copy_and_stream_upload(gb):
     finally:
         sim.close()
         sim2.close()
+
+
+def test_fp64_copy_converted_and_third_copy_waits_for_a_slot(gb):
+    import threading
+
+    p, sim = _sim(gb, 24, dtype=1)
+    L = gb.lib()
+    try:
+        sim.step(2)
+        want = sim.eta(np.float32)
+        t1, t2, t3 = C.c_int(0), C.c_int(0), C.c_int(0)
+        gb.check(L.gs_sim_copy_field_async(sim.h, b"eta", None, None, C.byref(t1)), "async")
+        gb.check(L.gs_sim_copy_field_async(sim.h, b"eta", None, None, C.byref(t2)), "async")
+        rc3 = []
+        th = threading.Thread(target=lambda: rc3.append(
+            L.gs_sim_copy_field_async(sim.h, b"eta", None, None, C.byref(t3))))
+        th.start()
+        th.join(0.5)
+        assert th.is_alive()  # both slots are taken until a wait frees one
+        got = np.empty(want.size, np.float32)
+        gb.check(L.gs_sim_copy_field_wait(sim.h, t1.value, got.ctypes.data, got.size, 0), "wait")
+        th.join(30)
+        assert not th.is_alive() and rc3 == [0]
+        assert np.array_equal(got.reshape(want.shape), want)  # FP64 state rounded to FP32
+        for t in (t2, t3):
+            gb.check(L.gs_sim_copy_field_wait(sim.h, t.value, got.ctypes.data, got.size, 0), "wait")
+    finally:
+        sim.close()
