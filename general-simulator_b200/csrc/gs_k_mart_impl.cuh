@@ -29,9 +29,15 @@ cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks, int nsim) {
 template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaStream_t s, int* nb, int nsim) {
   const bool fu = a.spec_next != nullptr && !stats;
   if (nsim > 0) {  // batched simulations (device-resident constants)
+    if constexpr (sizeof(T) == 4) {
+      if (a.mc.V == 3 && fu) return mu_n<T, H, 3, false, true, true>(a, s, nb, nsim);
+    }
     if (a.mc.V <= 4)
       return fu ? mu_n<T, H, 4, false, true, true>(a, s, nb, nsim) : mu_n<T, H, 4, false, true>(a, s, nb, nsim);
     return fu ? mu_n<T, H, 8, false, true, true>(a, s, nb, nsim) : mu_n<T, H, 8, false, true>(a, s, nb, nsim);
+  }
+  if constexpr (sizeof(T) == 4) {  // three variants exactly: no runtime bound in the variant loops
+    if (a.mc.V == 3 && fu) return mu_n<T, H, 3, false, false, true>(a, s, nb, 1);
   }
   if (a.mc.V <= 4) {
     if (stats) return mu_n<T, H, 4, true, false>(a, s, nb, 1);
