@@ -28,6 +28,13 @@ template <typename T, int N0, int FM, int GM, class Op> static cudaError_t xc_n(
   dim3 grid(a.h / tz, a.n1, a.nsim > 1 ? a.nsim : 1);
   if constexpr (sizeof(T) == 4 && N0 >= 64) {
     if (tz == 8) {
+      if constexpr (FM == 3 && GM == 3 && KxPair<Op>::v) {  // three fields exactly: compile-time counts
+        if (a.F == 3 && a.G == 3) {
+          allow_max_smem<k_xpass<T, N0, FM, GM, 8, Op, true>>();
+          k_xpass<T, N0, FM, GM, 8, Op, true><<<grid, tz * L::P * groups, smem, s>>>(a);
+          return cudaGetLastError();
+        }
+      }
       allow_max_smem<k_xpass<T, N0, FM, GM, 8, Op>>();
       k_xpass<T, N0, FM, GM, 8, Op><<<grid, tz * L::P * groups, smem, s>>>(a);
       return cudaGetLastError();

@@ -397,7 +397,7 @@ struct TableOp {
       bv[2 * i + 1] = w.y;
     }
   }
-  template <typename T, int FM, int GM>
+  template <typename T, int FM, int GM, bool EX = false>
   __device__ __forceinline__ static void contract(const XArgs<T>& a, const T (&bv)[TriStride<FM>::v],
                                                   const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
     static_assert(FM == GM, "square tables only");
@@ -407,7 +407,7 @@ struct TableOp {
       cplx<T> acc = mk2((T)0, (T)0);
 #pragma unroll
       for (int f = 0; f < FM; ++f)
-        if (f < a.F) acc = acc + in[f] * bv[tri_slot<FM>(g, f)];
+        if (EX || f < a.F) acc = acc + in[f] * bv[tri_slot<FM>(g, f)];
       out[g] = acc * mult;
     }
   }
@@ -540,7 +540,7 @@ template <int FM, int GM> struct XBounds {
 // per-point operation, inverse FFT, store.  smb: the groups' line regions
 // (region = PAD * TZ values each), part: GM x N0 values for the packed
 // columns.  Shared by the plain and the TMA-fed kernels.
-template <typename T, int N0, int FM, int GM, class Op, bool TWS = false>
+template <typename T, int N0, int FM, int GM, class Op, bool TWS = false, bool EX = false>
 __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx<T>* part, int TZ, int grp, int c,
                                            int t, int kz0, int ky, cplx<T>* out_base,
                                            cplx<T> (&v)[Line<T, N0>::R1], const cplx<T>* tw) {
@@ -552,7 +552,8 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
   const int region = L::PAD * TZ;
   V* rg = smb + grp * region + c;
   auto sm = [rg, TZ](int pos) -> V& { return rg[pos * TZ]; };
-  const bool fw = grp < a.F;
+  const int Fn = EX ? FM : a.F, Gn = EX ? GM : a.G;  // EX: exactly FM inputs and GM outputs
+  const bool fw = grp < Fn;
   const bool special_blk = kz0 == 0 && (n1 == 1 || ky == 0 || ky == HH);
   const int nn[3] = {a.n0, a.n1, a.n2};
   // with a paired operator one item is kx and N0 - kx (kx <= N0 / 2)
@@ -619,21 +620,21 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
           V* pt = smb + px * TZ + cc;
           V in[FM], out[GM];
 #pragma unroll
-          for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pt[f * region] : mk2((T)0, (T)0);
-          Op::template contract<T, FM, GM>(a, bv, in, out);
+          for (int f = 0; f < FM; ++f) in[f] = f < Fn ? pt[f * region] : mk2((T)0, (T)0);
+          Op::template contract<T, FM, GM, EX>(a, bv, in, out);
 #pragma unroll
           for (int g = 0; g < GM; ++g)
-            if (g < a.G) pt[g * region] = out[g];
+            if (g < Gn) pt[g * region] = out[g];
         }
       } else {
         V* pt = smb + kx * TZ + cc;
         V in[FM], out[GM];
 #pragma unroll
-        for (int f = 0; f < FM; ++f) in[f] = f < a.F ? pt[f * region] : mk2((T)0, (T)0);
+        for (int f = 0; f < FM; ++f) in[f] = f < Fn ? pt[f * region] : mk2((T)0, (T)0);
         Op::template apply<T, FM, GM>(a, nn, kx, kyA, kzA, in, out);
 #pragma unroll
         for (int g = 0; g < GM; ++g)
-          if (g < a.G) pt[g * region] = out[g];
+          if (g < Gn) pt[g * region] = out[g];
       }
     } else {
       // two real sequences packed in one column: A = (W(k) + conj W(-k))/2,
@@ -649,8 +650,8 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
           V in[FM];
 #pragma unroll
           for (int f = 0; f < FM; ++f) {
-            const V wa = f < a.F ? smb[f * region + kxa * TZ] : mk2((T)0, (T)0);
-            const V wb = f < a.F ? smb[f * region + kxb * TZ] : mk2((T)0, (T)0);
+            const V wa = f < Fn ? smb[f * region + kxa * TZ] : mk2((T)0, (T)0);
+            const V wb = f < Fn ? smb[f * region + kxb * TZ] : mk2((T)0, (T)0);
             if (half == 0) {
               in[f] = mk2((T)0.5 * (wa.x + wb.x), (T)0.5 * (wa.y - wb.y));
             } else {
@@ -664,7 +665,7 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
         }
 #pragma unroll
         for (int g = 0; g < GM; ++g)
-          if (g < a.G) part[g * N0 + kxa] = mk2(res[0][g].x - res[1][g].y, res[0][g].y + res[1][g].x);
+          if (g < Gn) part[g * N0 + kxa] = mk2(res[0][g].x - res[1][g].y, res[0][g].y + res[1][g].x);
       }
     }
   };
@@ -677,14 +678,14 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
   for (int idx = threadIdx.x + PF * blockDim.x; idx < NKX * TZ; idx += blockDim.x) point(idx, nullptr);
   __syncthreads();
   if (special_blk) {
-    for (int idx = threadIdx.x; idx < a.G * N0; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < Gn * N0; idx += blockDim.x) {
       const int g = idx / N0, kx = idx - g * N0;
       smb[g * region + kx * TZ] = part[g * N0 + kx];
     }
     __syncthreads();
   }
   // inverse FFT, group grp takes output field grp
-  const bool iv = grp < a.G;
+  const bool iv = grp < Gn;
 #pragma unroll
   for (int r = 0; r < L::R1; ++r) v[r] = iv ? sm(L::in_pos(t, r)) : mk2((T)0, (T)0);
   __syncthreads();
@@ -697,7 +698,7 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
 }
 
 
-template <typename T, int N0, int FM, int GM, int TZC, class Op>
+template <typename T, int N0, int FM, int GM, int TZC, class Op, bool EX = false>
 __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   using L = Line<T, N0>;
   using V = cplx<T>;
@@ -727,7 +728,7 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
   }
-  xpass_tile<T, N0, FM, GM, Op, true>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v, tws);
+  xpass_tile<T, N0, FM, GM, Op, true, EX>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v, tws);
 }
 
 // ---------------------------------------------------------------------------
