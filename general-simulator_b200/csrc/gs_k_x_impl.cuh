@@ -28,8 +28,10 @@ template <typename T, int N0, int FM, int GM, class Op> static cudaError_t xc_n(
   dim3 grid(a.h / tz, a.n1, a.nsim > 1 ? a.nsim : 1);
   if constexpr (sizeof(T) == 4 && N0 >= 64) {
     if (tz == 8) {
-      if constexpr (FM == 3 && GM == 3 && KxPair<Op>::v) {  // three fields exactly: compile-time counts
-        if (a.F == 3 && a.G == 3) {
+      // exact field counts known at compile time: the three- and five-field
+      // table contractions, the precipitate's (state, force) -> state slices
+      if constexpr ((FM == GM && (FM == 3 || FM == 5) && KxPair<Op>::v) || (FM == 2 && GM == 1)) {
+        if (a.F == FM && a.G == GM) {
           allow_max_smem<k_xpass<T, N0, FM, GM, 8, Op, true>>();
           k_xpass<T, N0, FM, GM, 8, Op, true><<<grid, tz * L::P * groups, smem, s>>>(a);
           return cudaGetLastError();
