@@ -25,7 +25,8 @@ template <typename T> cudaError_t launch_adj_update(AdjArgs<T>& a, int H, cudaSt
   switch (H) {
 #define GS_C(N_)                                                                    \
   case N_:                                                                          \
-    return a.mc.V <= 4 ? adj_n<T, N_, 4>(a, s, nblocks) : adj_n<T, N_, 8>(a, s, nblocks);
+    return a.mc.V == 3 ? adj_n<T, N_, 3>(a, s, nblocks)                              \
+           : a.mc.V <= 4 ? adj_n<T, N_, 4>(a, s, nblocks) : adj_n<T, N_, 8>(a, s, nblocks);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:
