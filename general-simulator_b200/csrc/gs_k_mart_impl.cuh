@@ -31,14 +31,17 @@ template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaSt
   if (nsim > 0) {  // batched simulations (device-resident constants)
     if constexpr (sizeof(T) == 4) {
       if (a.mc.V == 3 && fu) return mu_n<T, H, 3, false, true, true>(a, s, nb, nsim);
+      if (a.mc.V == 2 && fu) return mu_n<T, H, 2, false, true, true>(a, s, nb, nsim);
     }
     if (a.mc.V <= 4)
       return fu ? mu_n<T, H, 4, false, true, true>(a, s, nb, nsim) : mu_n<T, H, 4, false, true>(a, s, nb, nsim);
     return fu ? mu_n<T, H, 8, false, true, true>(a, s, nb, nsim) : mu_n<T, H, 8, false, true>(a, s, nb, nsim);
   }
-  if constexpr (sizeof(T) == 4) {  // three variants exactly: no runtime bound in the variant loops
+  // two or three variants exactly: no runtime bound in the variant loops
+  if constexpr (sizeof(T) == 4) {
     if (a.mc.V == 3 && fu) return mu_n<T, H, 3, false, false, true>(a, s, nb, 1);
   }
+  if (a.mc.V == 2 && fu) return mu_n<T, H, 2, false, false, true>(a, s, nb, 1);
   if (a.mc.V <= 4) {
     if (stats) return mu_n<T, H, 4, true, false>(a, s, nb, 1);
     return fu ? mu_n<T, H, 4, false, false, true>(a, s, nb, 1) : mu_n<T, H, 4, false, false>(a, s, nb, 1);
