@@ -95,7 +95,11 @@ def build_reference() -> str | None:
     out = os.path.join(ROOT, "oracle", "_ref", "gsi")
     if os.path.exists(out):
         return out
-    r = subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], capture_output=True, text=True)
+    ref = os.environ.get("REF", "/root/reference")  # where the reference tree sits in the build container
+    if not os.path.isdir(os.path.join(ref, "src")):
+        return None
+    r = subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], capture_output=True, text=True,
+                       env={**os.environ, "REF": ref})
     if r.returncode != 0:
         print("reference build skipped:", (r.stdout + r.stderr).strip().splitlines()[-1:], file=sys.stderr)
         return None

@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <chrono>
 #include <condition_variable>
@@ -1875,6 +1876,9 @@ extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void
                         "gs_mart_step_noalloc: grid %dx%dx%d with %d variants needs %zu bytes of scratch; the "
                         "static scratch holds %zu",
                         p->nx, p->ny, p->nz, p->nvariants, need, kNoallocScratchBytes);
+  // the kernels move fields in 16-byte vectors (float4 / double2)
+  if ((reinterpret_cast<uintptr_t>(eta_in) | reinterpret_cast<uintptr_t>(eta_out)) & 15u)
+    return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: eta_in and eta_out must be 16-byte aligned");
   const char* a = static_cast<const char*>(eta_in);
   const char* b = static_cast<const char*>(eta_out);
   if (a < b + fields && b < a + fields)

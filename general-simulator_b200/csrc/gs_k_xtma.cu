@@ -10,10 +10,10 @@ namespace gs {
 // off by default: at 256^3 x 3 the pass measured 0.167 ms against 0.163 ms
 // for the one-tile-per-block pass, whose second resident block already hides
 // the loads
-static bool g_x_prefetch = false;
+static std::atomic<bool> g_x_prefetch{false};
 
-void set_x_prefetch(bool on) { g_x_prefetch = on; }
-bool x_prefetch() { return g_x_prefetch; }
+void set_x_prefetch(bool on) { g_x_prefetch.store(on); }
+bool x_prefetch() { return g_x_prefetch.load(); }
 
 unsigned int x_wait_timeouts() {
   unsigned int v = 0;
@@ -24,26 +24,26 @@ unsigned int x_wait_timeouts() {
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library); null when the driver does not offer it.
 static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  // a function-local static initialiser runs once, thread-safely
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
+      return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+    return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+  }();
   return fn;
 }
 
 static int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+  const int dev = current_device();
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = 148;
   }
   return n;
 }
@@ -69,13 +69,19 @@ template <int N0, int FM, int TZ> static cudaError_t xtma_n(XArgs<float>& a, cud
   const size_t smem = 2 * (size_t)FM * Sh::region_bytes + (size_t)(FM + 1) * N0 * vb + 2 * sizeof(uint64_t);
   // two blocks per SM need the largest shared-memory carve-out; the grid is
   // what the occupancy calculator says fits at once
-  static int per_sm = 0;
+  // (attributes and occupancy belong to the current device: one entry per device)
+  static std::atomic<int> per_sm_dev[kMaxDevices];
+  const int dev = current_device();
+  int per_sm = dev >= 0 && dev < kMaxDevices ? per_sm_dev[dev].load(std::memory_order_acquire) : 0;
   if (!per_sm) {
     const auto k = k_xpass_tma<N0, FM, TZ, TableOp>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Sh::threads, smem) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Sh::threads, smem) != cudaSuccess || per_sm < 1) {
+      cudaGetLastError();
       per_sm = 1;
+    }
+    if (dev >= 0 && dev < kMaxDevices) per_sm_dev[dev].store(per_sm, std::memory_order_release);
   }
   const int ntiles = (a.h / TZ) * a.n1;
   int grid = per_sm * sm_count();

@@ -3,6 +3,8 @@
 // template instance).
 #pragma once
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include "gs_common.cuh"
 
 namespace gs {
@@ -57,31 +59,51 @@ cudaError_t launch_mart_update(MartArgs<T>& a, int H, bool stats, cudaStream_t s
 template <typename T> struct MartConst;
 template <typename T> cudaError_t launch_bump_step(MartConst<T>* mcs, int n, cudaStream_t s);
 
-// opt a kernel in to the largest dynamic shared memory once (the launch
-// still asks only for what it needs); no attribute calls during capture
-// (one flag per kernel: the template is instantiated per function)
+// the current device, and a bound on the devices the per-device caches below track
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    cudaGetLastError();
+    d = 0;
+  }
+  return d;
+}
+
+// opt a kernel in to the largest dynamic shared memory once per device (the
+// attribute belongs to the current device; the launch still asks only for
+// what it needs); no attribute calls during capture once a device has been
+// used (one flag array per kernel: the template is instantiated per function)
 template <auto Kernel> inline void allow_max_smem() {
-  static bool done = false;
-  if (!done) {
+  static std::atomic<bool> done[kMaxDevices];
+  const int d = current_device();
+  if (d < 0 || d >= kMaxDevices) {
     cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    done = true;
+    return;
+  }
+  if (!done[d].load(std::memory_order_acquire)) {
+    // setting the same value twice from two threads is harmless
+    cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    done[d].store(true, std::memory_order_release);
   }
 }
 cudaError_t launch_reduce(const double* partials, int nb, int n, double* out, cudaStream_t s);
 
 // the largest block a kernel can be launched with (its register use), once
 template <auto Kernel> inline int max_block_threads() {
-  static int v = 0;
-  if (!v) {
+  static std::atomic<int> v{0};
+  int r = v.load(std::memory_order_relaxed);
+  if (!r) {
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, Kernel) == cudaSuccess) {
-      v = fa.maxThreadsPerBlock;
+      r = fa.maxThreadsPerBlock;
     } else {
       cudaGetLastError();
-      v = 256;
+      r = 256;
     }
+    v.store(r, std::memory_order_relaxed);
   }
-  return v;
+  return r;
 }
 
 #define GS_SIZE_CASES(M) \

@@ -573,9 +573,35 @@ def mart2d_params(n: int = 128, dtype: int = GS_DTYPE_F64) -> GsParams:
     return p
 
 
-def mart3d_params(n: int = 256, dtype: int = GS_DTYPE_F32, noise: float = 1e-3) -> GsParams:
-    """3D cubic-to-tetragonal martensite, 3 variants, sigma_zz = 0.005."""
-    p = default_params(GS_MODEL_MART, GS_MODE_BASELINE)
+def _mart_baseline_defaults_host() -> GsParams:
+    """The baseline-mode martensite defaults of gs_params_default, filled in
+    Python without loading libgsb200.so (a CPU-only caller such as the
+    benchmark's CPU arm must not map the product library).  A CPU test keeps
+    the two byte-identical."""
+    p = GsParams()  # zero-filled, like the C function's memset
+    p.model, p.mode, p.dtype = GS_MODEL_MART, GS_MODE_BASELINE, GS_DTYPE_F32
+    p.dx = p.dy = p.dz = 1.0
+    p.weight_elastic = 1.0
+    p.xi = 1.0
+    p.nvariants = 3
+    p.nx = p.ny = p.nz = 256
+    p.dt = 0.005
+    p.landau[0], p.landau[1], p.landau[2], p.landau[3] = 0.2, 3.0, 2.0, 1.0
+    p.kappa = 0.5
+    p.mobility = 1.0
+    p.set_eigenstrain(tetragonal_eigenstrains(3, 0.02, -0.01))
+    p.set_cijkl(cubic_cijkl(1.4, 0.84, 0.56))
+    p.applied_stress[8] = 0.005
+    p.noise_amp = 1e-3
+    p.seed = 1
+    return p
+
+
+def mart3d_params(n: int = 256, dtype: int = GS_DTYPE_F32, noise: float = 1e-3,
+                  host_only: bool = False) -> GsParams:
+    """3D cubic-to-tetragonal martensite, 3 variants, sigma_zz = 0.005.
+    host_only: start from the Python copy of the defaults (no library load)."""
+    p = _mart_baseline_defaults_host() if host_only else default_params(GS_MODEL_MART, GS_MODE_BASELINE)
     p.dtype = dtype
     p.nvariants = 3
     p.nx = p.ny = p.nz = n

@@ -260,7 +260,8 @@ unsigned int gs_x_prefetch_timeouts(void);
  * whose device memory belongs to someone else.  One martensite step (the
  * same passes as gs_sim_step) from eta_in to eta_out, both caller-owned
  * device buffers of [V][nx][ny][nz] elements of p->dtype on the current
- * device, not overlapping; `step` is the global step index that the noise
+ * device, not overlapping, each starting on a 16-byte boundary (the kernels
+ * move fields in 16-byte vectors; other addresses get GS_EINVAL); `step` is the global step index that the noise
  * counter uses (gs_sim_step's k-th step from a fresh simulation has step
  * k).  Defect and dislocation-stress inputs are not taken.  The spectra and
  * twiddle tables live in one static device array of

@@ -9,8 +9,9 @@
 #      leaves p unchanged and INPUT::standardize never ends on {..} scripts);
 #   3. nvcc -O2 for sm_100a, -lcurand -lcufft, as the reference's makefile.
 # The binary only runs on a GPU box; it is test infrastructure.
+# Usage: REF=<path of the reference tree> oracle/build_ref.sh
 set -e
-REF=${REF:-/root/reference}
+if [ -z "$REF" ]; then echo "set REF to the reference tree (the directory holding src/ and include/)"; exit 1; fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then echo "reference tree not found at $REF"; exit 1; fi

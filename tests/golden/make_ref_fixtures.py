@@ -3,7 +3,10 @@
 on small seeded inputs.  The physics cases need a CUDA device (the
 reference's kernels are device-only); the front-end cases run anywhere.
 
-  python tests/golden/make_ref_fixtures.py --out DIR [--physics] [--frontend]
+  REF=<reference tree> python tests/golden/make_ref_fixtures.py --out DIR [--physics] [--frontend]
+
+REF (required for --frontend) names the reference tree whose scripts/ the
+front-end cases read.
 
 Writes DIR/ref_<case>.npz (inputs, dumps, the info lines),
 DIR/frontend_<script>.txt and DIR/ref_cores.npz (the nuclei generator, which
@@ -194,7 +197,7 @@ def case_stress(out: str) -> None:
 
 def case_frontend(out: str) -> None:
     for name in ["in.if.loop.while", "in.pow", "in.expr"]:
-        src = os.path.join(os.environ.get("REF", "/root/reference"), "scripts", name)
+        src = os.path.join(os.environ["REF"], "scripts", name)
         if not os.path.exists(src):
             src = os.path.join(HERE, "scripts", name)  # project scripts in the reference's language
         with tempfile.TemporaryDirectory() as d:

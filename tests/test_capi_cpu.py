@@ -55,6 +55,16 @@ def test_defaults_reference_values(gb):
     assert s.xi == 4000.0 and s.get_cijkl()[2, 2, 2, 2] == 5.22
 
 
+def test_host_only_defaults_equal_the_library_defaults(gb):
+    """The benchmark's CPU arm fills the headline parameters in Python so that
+    it never maps libgsb200.so; the bytes must equal the library's."""
+    for n, noise, dt in ((256, 1e-3, gb.GS_DTYPE_F32), (32, 0.0, gb.GS_DTYPE_F64)):
+        a = gb.mart3d_params(n, dtype=dt, noise=noise)
+        b = gb.mart3d_params(n, dtype=dt, noise=noise, host_only=True)
+        assert bytes(a) == bytes(b)
+    assert bytes(gb._mart_baseline_defaults_host()) == bytes(gb.default_params(gb.GS_MODEL_MART))
+
+
 def test_bad_model_is_einval(gb):
     p = gb.GsParams()
     assert gb.lib().gs_params_default(C.byref(p), 99, 0) == -10
