@@ -184,6 +184,8 @@ def lib() -> C.CDLL:
         "gs_sim_take_field": (C.c_int, [vp, C.c_char_p, vp, C.c_char_p]),
         "gs_cores_paint": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, C.c_double, C.c_double,
                                      C.c_double, vp, vp]),
+        "gs_noise_block": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                     vp, vp]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
         "gs_mart_step_noalloc_max_bytes": (C.c_size_t, []),
     }

@@ -352,6 +352,21 @@ int gs_batch_autotune(gs_batch* b, int reps, void* stream);
 int gs_batch_get_schedule(const gs_batch* b, int group, gs_schedule* sc);
 int64_t gs_batch_launch_count(const gs_batch* b);
 
+/* ---- the noise stream ---------------------------------------------------- */
+/* Replaces the reference's cuRAND normal field (Random::NewNormal_device,
+ * src/random.cu:79-82), which the step kernels no longer store: they draw
+ * Philox4x32-10 in registers on the counter (quad, step, sim, slot) with key
+ * (seed & 0xffffffff, seed >> 32), quad = cell >> 2, slot = the variant (V
+ * for the concentration), and turn words (0,1) and (2,3) into the normals of
+ * cells 4 quad .. 4 quad + 3 by Box-Muller on 24-bit uniforms.  This call
+ * evaluates those same device functions for quads quad0 .. quad0 + nquads - 1
+ * (the quad word wraps modulo 2^32) and writes the raw words [nquads][4] to
+ * `words` and the normals [nquads][4] of `dtype` to `normals` (host buffers;
+ * either may be NULL), so that the stream can be checked against another
+ * Philox4x32-10 implementation bit for bit. */
+int gs_noise_block(uint64_t seed, uint32_t step, uint32_t sim, uint32_t slot, uint32_t quad0, int nquads,
+                   int dtype, uint32_t* words, void* normals);
+
 /* ---- comparator: the same step with cuFFT C2C and unfused sweeps ------ */
 /* The plain GPU step in the reference's structure (cufftPlanMany C2C batch
  * V, B streamed from a [V][V][N] array, one sweep per term); used only as a
