@@ -23,7 +23,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 CU_SOURCES = ["gs_capi.cu", "gs_k_zy.cu", "gs_k_zy_f32.cu", "gs_k_zy_f64.cu", "gs_k_x.cu", "gs_k_x33.cu",
               "gs_k_x55.cu", "gs_k_x86.cu", "gs_k_x99.cu", "gs_k_xt.cu", "gs_k_xp10.cu", "gs_k_xp2.cu", "gs_k_xp18.cu",
               "gs_k_precip.cu", "gs_k_mart.cu", "gs_k_mart_f32.cu", "gs_k_mart_f64.cu",
-              "gs_k_adj_f32.cu", "gs_k_adj_f64.cu", "gs_plain.cu", "gs_cores.cu", "gs_k_padj.cu", "gs_k_xtma.cu", "gs_noise.cu"]
+              "gs_k_adj_f32.cu", "gs_k_adj_f64.cu", "gs_plain.cu", "gs_cores.cu", "gs_k_padj.cu", "gs_k_xtma.cu", "gs_noise.cu", "gs_cufft.cu"]
 LIB = os.path.join(HERE, "libgsb200.so")
 
 

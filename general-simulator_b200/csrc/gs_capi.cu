@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <chrono>
 #include <condition_variable>
@@ -513,7 +514,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   za.tw_n2 = twp<T>(s, 0);
   if (!z_ready) {  // else the previous update left the z spectra of src^2 in place
     GS_CU(launch_zfwd<T>(za, s->h, st, s->sched.z_lines), "z forward pass");
-    gs_mark(s, st);
+    gs_mark(s, st, "z_forward");
     s->launches += 1;
   }
   YArgs<T> ya;
@@ -523,7 +524,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
   GS_CU(launch_ypass<T>(ya, s->n1, F, -1, st, s->sched.y_cols), "y forward pass");
-  if (s->n1 > 1) gs_mark(s, st);
+  if (s->n1 > 1) gs_mark(s, st, "y_forward");
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
   xa.in = reinterpret_cast<cplx<T>*>(s->spec);
@@ -539,11 +540,11 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   if (s->btab_state == 1 && which == btab_which(s) && F == s->btab_fields && G == F) set_btab<T>(s, xa);
   xa.tz_req = s->sched.x_cols;
   GS_CU(launch_xcontract<T>(xa, st), "x contraction pass");
-  gs_mark(s, st);
+  gs_mark(s, st, "x_contraction");
   YArgs<T> yb = ya;
   yb.spec = reinterpret_cast<cplx<T>*>(out_spec);
   GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st, s->sched.y_cols), "y inverse pass");
-  if (s->n1 > 1) gs_mark(s, st);
+  if (s->n1 > 1) gs_mark(s, st, "y_inverse");
   s->launches += 1 + (s->n1 > 1 ? 2 : 0);
   return GS_OK;
 }
@@ -589,7 +590,7 @@ template <typename T> static int mart_step(gs_sim* s, cudaStream_t st) {
   fill_mart_args<T>(s, ma, in, out);
   if (s->fuse) ma.spec_next = reinterpret_cast<cplx<T>*>(s->spec);
   GS_CU(launch_mart_update<T>(ma, s->h, false, st, nullptr), "update pass");
-  gs_mark(s, st);
+  gs_mark(s, st, "update");
   s->launches += 1;
   if (!s->trial) {  // a trial step wrote only the spare field and the spectra
     s->cur ^= 1;
@@ -706,7 +707,7 @@ template <typename T> static int precip_potential(gs_sim* s, cudaStream_t st) {
   zi.tw_n2 = twp<T>(s, 0);
   zi.offset_field = -1;
   GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (elastic potential)");
-  gs_mark(s, st);
+  gs_mark(s, st, "z_inverse_potential");
   s->launches += 1;
   return GS_OK;
 }
@@ -774,7 +775,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
     const cudaError_t e = launch_precip_mid<T>(pm, s->h, st);
     if (e == cudaSuccess) {
       fused = true;
-      gs_mark(s, st);
+      gs_mark(s, st, "precip_mid");
       s->launches += 1;
     } else if (e != cudaErrorInvalidConfiguration) {
       GS_CU(e, "precipitate middle sweep");
@@ -791,9 +792,9 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
     zr.tw_n2 = twp<T>(s, 0);
     zr.offset_field = -1;
     GS_CU(launch_zinv<T>(zr, s->h, st), "z inverse (elastic potential)");
-    gs_mark(s, st);
+    gs_mark(s, st, "z_inverse_potential");
     GS_CU(launch_precip_local<T>(la, st), "precipitate local terms");
-    gs_mark(s, st);
+    gs_mark(s, st, "precip_local");
     s->launches += 2;
   }
   // chain 2: [c, mu, eta_0, g_0, eta_1, g_1, ...] -> k-space update -> [c', eta']
@@ -812,7 +813,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   za.tw_n2 = twp<T>(s, 0);
   if (!fused) {
     GS_CU(launch_zfwd<T>(za, s->h, st, s->sched.z_lines), "z forward (update fields)");
-    gs_mark(s, st);
+    gs_mark(s, st, "z_forward_update_fields");
     s->launches += 1;
   }
   YArgs<T> ya;
@@ -822,7 +823,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
   GS_CU(launch_ypass<T>(ya, s->n1, F2, -1, st, s->sched.y_cols), "y forward (update fields)");
-  if (s->n1 > 1) gs_mark(s, st);
+  if (s->n1 > 1) gs_mark(s, st, "y_forward_update_fields");
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
   xa.in = reinterpret_cast<cplx<T>*>(s->spec2);
@@ -849,11 +850,11 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   xa.pu.scale = (T)(1.0 / (double)N);
   for (int c3 = 0; c3 < 3; ++c3) xa.pu.ktab[c3] = reinterpret_cast<const T*>(s->ktab) + s->ktab_off[c3];
   GS_CU(launch_xprecip<T>(xa, st), "x pass (k-space update)");
-  gs_mark(s, st);
+  gs_mark(s, st, "x_kspace_update");
   YArgs<T> yo = ya;
   yo.spec = reinterpret_cast<cplx<T>*>(s->spec);
   GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st, s->sched.y_cols), "y inverse (update fields)");
-  if (s->n1 > 1) gs_mark(s, st);
+  if (s->n1 > 1) gs_mark(s, st, "y_inverse_update_fields");
   ZinvArgs<T> zi;
   memset(&zi, 0, sizeof(zi));
   zi.spec = reinterpret_cast<const cplx<T>*>(s->spec);
@@ -866,7 +867,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   zi.offset_field = p.mass_projection ? 0 : -1;
   zi.offset = s->mass0 / (double)N;
   GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (c, eta)");
-  gs_mark(s, st);
+  gs_mark(s, st, "z_inverse_c_eta");
   s->launches += 2 + (s->n1 > 1 ? 2 : 0);
   s->step += 1;
   return GS_OK;
@@ -943,9 +944,9 @@ template <typename T> static int stress_step(gs_sim* s, cudaStream_t st) {
   zi.tw_n2 = twp<T>(s, 0);
   zi.offset_field = -1;
   GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (stress)");
-  gs_mark(s, st);
+  gs_mark(s, st, "z_inverse_stress");
   GS_CU(launch_defect<T>(eta, reinterpret_cast<T*>(s->defect), s->N, V, st), "defect mask");
-  gs_mark(s, st);
+  gs_mark(s, st, "defect_mask");
   s->launches += 2;
   s->step += 1;
   return GS_OK;
@@ -970,6 +971,7 @@ static void free_sim(gs_sim* s) {
   for (int i = 0; i < gs_sim::kMaxMarks; ++i)
     if (s->marks[i]) cudaEventDestroy(s->marks[i]);
   gs_plain_free(s);
+  gs_cufft_free(s);
   delete s;
 }
 
@@ -1185,6 +1187,7 @@ extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, s
   if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_set_field: null argument");
   sim_graph_reset(s);
   s->spec_ready = false;
+  gs_cufft_invalidate(s);
   if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
   const int V = s->p.nvariants;
   const size_t N = (size_t)s->N;
@@ -1349,24 +1352,78 @@ template <typename T> static int sim_graph_steps(gs_sim* s, int nsteps, cudaStre
   return GS_OK;
 }
 
+static int step_once(gs_sim* s, cudaStream_t st) {
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  if (s->p.model == GS_MODEL_MART) return f64 ? mart_step<double>(s, st) : mart_step<float>(s, st);
+  if (s->p.model == GS_MODEL_PRECIPITATE) return f64 ? precip_step<double>(s, st) : precip_step<float>(s, st);
+  return f64 ? stress_step<double>(s, st) : stress_step<float>(s, st);
+}
+
+// GS_TIMING (read once per process): unset, empty or "0" = off; "1" = one
+// JSON line per step on stderr with the device time of every pass (CUDA
+// events on the stepping stream, direct launches, the host waits for each
+// step); any other value = the path of a file the lines are appended to.
+static const char* timing_target() {
+  static const char* const v = [] {
+    const char* e = getenv("GS_TIMING");
+    return (e && *e && strcmp(e, "0") != 0) ? e : static_cast<const char*>(nullptr);
+  }();
+  return v;
+}
+
+static int timed_steps(gs_sim* s, int nsteps, cudaStream_t st, const char* target) {
+  for (int i = 0; i < gs_sim::kMaxMarks; ++i)
+    if (!s->marks[i]) GS_CU(cudaEventCreate(&s->marks[i]), "event create");
+  static const char* const models[4] = {"", "martensite", "precipitate", "stress"};
+  for (int k = 0; k < nsteps; ++k) {
+    const int64_t step = s->step;
+    s->nmarks = 0;
+    s->profiling = true;
+    gs_mark(s, st);
+    const int rc = step_once(s, st);
+    s->profiling = false;
+    if (rc != GS_OK) return rc;
+    GS_CU(cudaEventSynchronize(s->marks[s->nmarks - 1]), "event sync");
+    std::string line = "{\"gs_timing\": 1, \"model\": \"";
+    line += models[s->p.model >= 1 && s->p.model <= 3 ? s->p.model : 0];
+    char buf[256];
+    snprintf(buf, sizeof(buf), "\", \"step\": %lld, \"grid\": [%d, %d, %d], \"variants\": %d, \"dtype\": \"%s\", \"passes\": [",
+             (long long)step, s->p.nx, s->p.ny, s->p.nz, s->p.nvariants, s->p.dtype == GS_DTYPE_F64 ? "f64" : "f32");
+    line += buf;
+    double total = 0;
+    for (int i = 0; i + 1 < s->nmarks; ++i) {
+      float ms = 0;
+      GS_CU(cudaEventElapsedTime(&ms, s->marks[i], s->marks[i + 1]), "elapsed");
+      total += ms;
+      snprintf(buf, sizeof(buf), "%s{\"name\": \"%s\", \"ms\": %.6f}", i ? ", " : "",
+               s->mark_names[i + 1] ? s->mark_names[i + 1] : "pass", ms);
+      line += buf;
+    }
+    snprintf(buf, sizeof(buf), "], \"step_ms\": %.6f}\n", total);
+    line += buf;
+    if (strcmp(target, "1") == 0) {
+      fputs(line.c_str(), stderr);
+    } else if (FILE* f = fopen(target, "a")) {
+      fputs(line.c_str(), f);
+      fclose(f);
+    } else {
+      return gs_set_error(GS_EINVAL, "GS_TIMING: cannot append to '%s'", target);
+    }
+  }
+  return GS_OK;
+}
+
 extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
   if (!s) return gs_set_error(GS_EINVAL, "gs_sim_step: null sim");
   if (nsteps < 0) return gs_set_error(GS_EINVAL, "nsteps %d", nsteps);
   cudaStream_t st = pick_stream(s, stream);
   s->launches = 0;
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  if (const char* tt = timing_target())
+    if (!s->profiling && !s->trial) return timed_steps(s, nsteps, st, tt);
   if (s->use_graph && s->p.model == GS_MODEL_MART && !s->plain && nsteps >= 2)
     return f64 ? sim_graph_steps<double>(s, nsteps, st) : sim_graph_steps<float>(s, nsteps, st);
-  for (int i = 0; i < nsteps; ++i) {
-    int rc;
-    if (s->p.model == GS_MODEL_MART)
-      rc = f64 ? mart_step<double>(s, st) : mart_step<float>(s, st);
-    else if (s->p.model == GS_MODEL_PRECIPITATE)
-      rc = f64 ? precip_step<double>(s, st) : precip_step<float>(s, st);
-    else
-      rc = f64 ? stress_step<double>(s, st) : stress_step<float>(s, st);
-    if (rc != GS_OK) return rc;
-  }
+  for (int i = 0; i < nsteps; ++i) GS_TRY(step_once(s, st));
   return GS_OK;
 }
 
@@ -2454,6 +2511,7 @@ extern "C" int gs_sim_take_field(gs_sim* dst, const char* dst_name, gs_sim* src,
   GS_CU(cudaStreamSynchronize(dst->own_stream), "sync destination");
   sim_graph_reset(dst);
   dst->spec_ready = false;
+  gs_cufft_invalidate(dst);
   const size_t N = (size_t)dst->N;
   if (dn == "dislocationstress" && sn == "stress") {
     if (dst->p.model != GS_MODEL_MART || !src->stressbuf)
@@ -2967,6 +3025,7 @@ extern "C" int gs_sim_set_field_async(gs_sim* s, const char* name, const void* h
   if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
   sim_graph_reset(s);
   s->spec_ready = false;
+  gs_cufft_invalidate(s);
   cudaStream_t st = pick_stream(s, stream);
   GS_CU(cudaMemcpyAsync(s->eta[s->cur], host, n * elt(s), cudaMemcpyHostToDevice, st), "upload");
   return GS_OK;

@@ -54,6 +54,8 @@ template <typename T> struct MartArgs {
   T* r_out;           // when set: R_p written out [V][N] (adjoint checkpoints)
   int lr_req;         // rows per block asked by the autotuner (0 = default)
   cplx<T>* spec_next;  // FUSE: packed z spectra of eta'^2 for the next step (may be spec)
+  const T* r_in;       // !ZF: R_p in real space [V][N] (a library FFT's output)
+  T* sq_out;           // !ZF and FUSE: eta'^2 [V][N] (the next step's FFT input)
 };
 
 // advance the step counter of every batched simulation (keeps a captured
@@ -138,7 +140,11 @@ template <int VM, bool STATS> struct UpdBlocks {  // resident blocks asked of th
 // sweep every (variant, row) line transforms its shared-memory row into the
 // packed spectrum of the next step, in the rows of the spectrum buffer this
 // block alone read: the next step then starts at the y forward pass.
-template <typename T, int H, int VM, bool STATS, bool BATCH, bool FUSE = false>
+//
+// ZF = false: the same update without the z transforms, for the cuFFT
+// comparator step -- R_p is read from a.r_in (real space) and, with FUSE,
+// eta'^2 is written to a.sq_out for the library's next forward transform.
+template <typename T, int H, int VM, bool STATS, bool BATCH, bool FUSE = false, bool ZF = true>
 __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(MartArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
@@ -154,7 +160,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     if (FUSE) a.spec_next += off / 2;
   }
   const int Vn = mc.V;
-  {
+  if constexpr (ZF) {
     const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
     const int v = line % Vn, rr = line / Vn;
     const long long row = (long long)blockIdx.x * a.lr + rr;
@@ -230,7 +236,14 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       ldv<CW>(eq + oyp, vyp);
       ldv<CW>(eq + oym, vym);
       const T el_ = eq[ozl], er_ = eq[ozr];
-      const T* Rq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
+      const T* Rq = ZF ? reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0 : nullptr;
+      T Rl[CW];
+      if constexpr (ZF) {
+#pragma unroll
+        for (int j = 0; j < CW; ++j) Rl[j] = Rq[j];
+      } else {
+        ldv<CW>(a.r_in + q * N + cell, Rl);
+      }
       T Kq[CW];
 #pragma unroll
       for (int j = 0; j < CW; ++j) Kq[j] = 0;
@@ -257,7 +270,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
           chem = -mc.L * (mc.A2 * et - mc.A4 * e2 * et + mc.A6 * s2[j] * s2[j] * et +
                           (T)2 * mc.Ac * et * (s2[j] - e2));
         }
-        const T Rv = Rq[j];
+        const T Rv = Rl[j];
         rv[j] = Rv;
         const T el = mc.el * Rv * et;
         const T lin = (lq + mc.kc * Kq[j]) * et;
@@ -286,14 +299,21 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       if (!STATS) stv<CW>(a.eta_out + q * N + cell, out);
       if (!BATCH && a.r_out) stv<CW>(a.r_out + q * N + cell, rv);
       if (FUSE) {
-        T* sq = const_cast<T*>(Rq);
+        if constexpr (ZF) {
+          T* sq = const_cast<T*>(Rq);
 #pragma unroll
-        for (int j = 0; j < CW; ++j) sq[j] = out[j] * out[j];
+          for (int j = 0; j < CW; ++j) sq[j] = out[j] * out[j];
+        } else {
+          T o2[CW];
+#pragma unroll
+          for (int j = 0; j < CW; ++j) o2[j] = out[j] * out[j];
+          stv<CW>(a.sq_out + q * N + cell, o2);
+        }
       }
     }
   }
   if (STATS) block_reduce_store(acc, ACC_N, a.partials);
-  if (FUSE) {
+  if (FUSE && ZF) {
     __syncthreads();
     const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
     const int v = line % Vn, rr = line / Vn;

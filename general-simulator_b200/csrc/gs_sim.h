@@ -7,7 +7,8 @@
 
 #include "../../include/gs_capi.h"
 
-struct gs_plain_state;  // cuFFT comparator buffers (gs_plain.cu)
+struct gs_plain_state;  // comparator in the reference's structure (gs_plain.cu)
+struct gs_cufft_state;  // cuFFT R2C/C2R comparator (gs_cufft.cu)
 struct gs_snaps;        // asynchronous field copies in flight (gs_capi.cu)
 
 struct gs_sim {
@@ -40,6 +41,7 @@ struct gs_sim {
   int64_t launches = 0;
   int use_graph = 0;
   gs_plain_state* plain = nullptr;
+  gs_cufft_state* cufft = nullptr;
   // octant table of B(k) of the martensite contraction: state 1 = valid,
   // 0 = to build, -1 = never (handles that must not allocate), -2 = B is not
   // even in every axis (the contraction is formed on the fly)
@@ -70,16 +72,23 @@ struct gs_sim {
   // per-pass event marks of gs_sim_profile_step
   static constexpr int kMaxMarks = 32;
   cudaEvent_t marks[kMaxMarks] = {};
+  const char* mark_names[kMaxMarks] = {};  // the pass that ends at each mark
   int nmarks = 0;
   bool profiling = false;
   gs_snaps* snaps = nullptr;  // created by the first gs_sim_copy_field_async
 };
 
-// record a pass boundary when gs_sim_profile_step is active
-inline void gs_mark(gs_sim* s, cudaStream_t st) {
-  if (s->profiling && s->nmarks < gs_sim::kMaxMarks) cudaEventRecord(s->marks[s->nmarks++], st);
+// record a pass boundary when gs_sim_profile_step (or GS_TIMING) is active;
+// name: the pass that ends here
+inline void gs_mark(gs_sim* s, cudaStream_t st, const char* name = nullptr) {
+  if (s->profiling && s->nmarks < gs_sim::kMaxMarks) {
+    s->mark_names[s->nmarks] = name;
+    cudaEventRecord(s->marks[s->nmarks++], st);
+  }
 }
 
 int gs_set_error(int code, const char* fmt, ...);
 int gs_cuda_check(cudaError_t e, const char* what);
 void gs_plain_free(gs_sim* s);
+void gs_cufft_free(gs_sim* s);
+void gs_cufft_invalidate(gs_sim* s);

@@ -155,6 +155,8 @@ def lib() -> C.CDLL:
         "gs_batch_launch_count": (C.c_int64, [vp]),
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
+        "gs_cufft_create": (C.c_int, [P, C.POINTER(vp)]),
+        "gs_cufft_step": (C.c_int, [vp, C.c_int, vp]),
         "gs_adjoint_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),
         "gs_adjoint_destroy": (C.c_int, [vp]),
         "gs_adjoint_set_params": (C.c_int, [vp, P]),
@@ -368,18 +370,23 @@ class PrecipAdjoint:
 
 
 class Sim:
-    """One simulation handle (gs_sim*).  `plain=True` builds the cuFFT
-    comparator step instead of the hand-written one."""
+    """One simulation handle (gs_sim*).  `plain=True` builds the comparator
+    in the reference's structure (cuFFT C2C, B streamed, unfused sweeps);
+    `cufft=True` the cuFFT R2C/C2R comparator with this project's contraction
+    and fused update; neither is the product step."""
 
-    def __init__(self, params: GsParams, plain: bool = False):
+    def __init__(self, params: GsParams, plain: bool = False, cufft: bool = False):
         self.params = params.copy()
         h = C.c_void_p()
         if plain:
             check(lib().gs_plain_create(C.byref(self.params), C.byref(h)), "gs_plain_create")
+        elif cufft:
+            check(lib().gs_cufft_create(C.byref(self.params), C.byref(h)), "gs_cufft_create")
         else:
             check(lib().gs_sim_create(C.byref(self.params), C.byref(h)), "gs_sim_create")
         self.h = h
         self.plain = plain
+        self.cufft = cufft
 
     def close(self) -> None:
         if self.h:
@@ -418,6 +425,8 @@ class Sim:
     def step(self, n: int = 1, stream: int = 0) -> None:
         if self.plain:
             check(lib().gs_plain_step(self.h, n, C.c_void_p(stream)), "gs_plain_step")
+        elif self.cufft:
+            check(lib().gs_cufft_step(self.h, n, C.c_void_p(stream)), "gs_cufft_step")
         else:
             check(lib().gs_sim_step(self.h, n, C.c_void_p(stream)), "gs_sim_step")
 

@@ -374,6 +374,17 @@ int gs_noise_block(uint64_t seed, uint32_t step, uint32_t sim, uint32_t slot, ui
 int gs_plain_create(const gs_params* p, gs_sim** out);
 int gs_plain_step(gs_sim* s, int nsteps, void* stream);
 
+/* The cuFFT comparator of the hand-written FFT passes: the same martensite
+ * step with cufftExecR2C / cufftExecC2R batched over the variants (planned
+ * once), one contraction sweep over the half spectrum (the octant B table,
+ * or B formed per k), and the product's fused update kernel without its z
+ * transforms as the single pointwise sweep (it also writes eta'^2 for the
+ * next forward transform).  The reference's own convolution is the C2C one
+ * of gs_plain_* (src/dynamics_mart.cu:113-117,281-303).  Timing only; the
+ * handle otherwise behaves as gs_sim_create's (fields, stats, destroy). */
+int gs_cufft_create(const gs_params* p, gs_sim** out);
+int gs_cufft_step(gs_sim* s, int nsteps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

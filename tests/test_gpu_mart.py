@@ -14,8 +14,8 @@ pytestmark = pytest.mark.gpu
 F64, F32 = 1, 0
 
 
-def gpu_run(gb, p, eta0, steps, defect=None, dstress=None, temperature=None, plain=False):
-    s = gb.Sim(p, plain=plain)
+def gpu_run(gb, p, eta0, steps, defect=None, dstress=None, temperature=None, plain=False, cufft=False):
+    s = gb.Sim(p, plain=plain, cufft=cufft)
     try:
         s.set_field("eta", eta0)
         if defect is not None:
@@ -236,6 +236,47 @@ def test_plain_comparator_matches_oracle(gb, orc, dtype, tol):
     ref = orc.mart_run(p, eta0, 2)
     got = gpu_run(gb, p, eta0, 2, plain=True)
     assert rel_l2(got, ref) < tol
+
+
+@pytest.mark.parametrize("shape,V,dtype,tol", [
+    ((16, 16, 16), 3, F64, 1e-11), ((16, 16, 16), 3, F32, 1e-6), ((8, 12, 24), 4, F64, 1e-11),
+    ((32, 48, 1), 2, F64, 1e-11), ((1, 16, 24), 2, F64, 1e-11), ((64, 64, 64), 3, F32, 1e-6)])
+def test_cufft_comparator_matches_oracle(gb, orc, shape, V, dtype, tol):
+    """The cuFFT R2C/C2R comparator (table or on-the-fly contraction, the
+    product's update without its z transforms) against the FP64 oracle over
+    three steps (the first squares the field in its own sweep, the later ones
+    take eta'^2 from the update)."""
+    p = base3d(gb, shape, dtype, noise=1e-3, V=V)
+    eta0 = gb.initial_eta(p, 18, 0.4)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    ref = orc.mart_run(p, eta0, 3)
+    got = gpu_run(gb, p, eta0, 3, cufft=True)
+    assert rel_l2(got, ref) < tol * (3 if dtype == F32 else 1)
+
+
+def test_cufft_comparator_asymmetric_b_and_reupload(gb, orc):
+    """B not even in an axis (contraction formed per k), and a field upload
+    between steps (the kept eta^2 is dropped)."""
+    p = base3d(gb, (8, 12, 16), F64, noise=1e-3)
+    eps = p.get_eigenstrain()
+    eps[0, 0, 1] = eps[0, 1, 0] = 0.007
+    p.set_eigenstrain(eps)
+    e0 = gb.initial_eta(p, 19, 0.5)
+    e1 = gb.initial_eta(p, 20, 0.5)
+    s = gb.Sim(p, cufft=True)
+    try:
+        s.set_field("eta", e0)
+        s.step(2)
+        a = s.eta()
+        s.set_field("eta", e1)
+        s.set_scalar("step", 2)
+        s.step(1)
+        b = s.eta()
+    finally:
+        s.close()
+    assert rel_l2(a, orc.mart_run(p, e0, 2)) < 1e-11
+    assert rel_l2(b, orc.mart_run(p, e1, 1, step0=2)) < 1e-11
 
 
 @pytest.mark.parametrize("shape,V", [((32, 48, 1), 2), ((1, 16, 24), 2)])
