@@ -392,13 +392,15 @@ def extra_configs() -> dict:
     return out
 
 
-def extra_precip_adjoint(n: int = 128, steps: int = 10) -> dict:
-    """Adjoint of the precipitate run: 128^3, concentration + 4 variants,
-    FP32, 10 steps, noise off.  plain = 10 steps of gs_sim_step; forward =
-    the adjoint's forward run (the same steps, every state kept on the
-    device); backward = gs_precip_adjoint_backward (all ten reverse steps
-    and the nine parameter sums), seeds already on the device.  Device time
-    on one stream."""
+def extra_precip_adjoint(n: int = 256, steps: int = 100, K: int = 10) -> dict:
+    """Adjoint of the precipitate run: 256^3, concentration + 4 variants,
+    FP32, 100 steps, noise off, a checkpoint every 10 steps.  plain = 100
+    steps of gs_sim_step; forward = the adjoint's forward run (the same
+    steps, checkpoints and the last segment kept on the device); backward =
+    gs_precip_adjoint_backward (the earlier segments recomputed from their
+    checkpoints, all reverse steps and the nine parameter sums, replayed as a
+    captured graph), seeds already on the device.  Device time on one
+    stream."""
     import torch
 
     import gs_b200 as gb
@@ -415,19 +417,21 @@ def extra_precip_adjoint(n: int = 128, steps: int = 10) -> dict:
         sim.set_field("concentration", c0)
         sim.set_field("eta", e0)
         sim.step(3, sh)
-        plain = min(_timed(stream, lambda: sim.step(steps, sh)) for _ in range(3))
+        plain = min(_timed(stream, lambda: sim.step(steps, sh)) for _ in range(2))
         sim.close()
-        a = gb.PrecipAdjoint(p, steps)
+        a = gb.PrecipAdjoint(p, steps, K)
         a.forward(c0, e0, sh, outputs=False)
         a.set_seed(rng.standard_normal(c0.shape), rng.standard_normal(e0.shape))
+        a.backward(stream=sh, outputs=False)  # direct; the next ones replay the captured sweep
         a.backward(stream=sh, outputs=False)
-        fwd = min(_timed(stream, lambda: a.forward(stream=sh, outputs=False)) for _ in range(3))
-        bwd = min(_timed(stream, lambda: a.backward(stream=sh, outputs=False)) for _ in range(3))
+        fwd = min(_timed(stream, lambda: a.forward(stream=sh, outputs=False)) for _ in range(2))
+        bwd = min(_timed(stream, lambda: a.backward(stream=sh, outputs=False)) for _ in range(2))
         mem = a.device_bytes()
         a.close()
-    return {"workload": f"{n}^3, concentration + 4 variants, FP32, {steps} steps, noise off",
+    return {"workload": f"{n}^3, concentration + 4 variants, FP32, {steps} steps, noise off, checkpoint every {K}",
             "plain_ms": plain, "forward_ms": fwd, "backward_ms": bwd, "adjoint_to_plain": bwd / plain,
-            "device_bytes": mem, "note": "every state of the run is kept; no recomputation"}
+            "device_bytes": mem,
+            "note": "backward includes recomputing every segment but the last from its checkpoint"}
 
 
 # ---------------------------------------------------------------------------

@@ -2556,7 +2556,10 @@ extern "C" int gs_sim_take_field(gs_sim* dst, const char* dst_name, gs_sim* src,
 struct gs_padjoint {
   gs_sim* s = nullptr;
   int nsteps = 0, F1 = 0;
-  void* states = nullptr;  // [nsteps + 1][V + 1][N] (c, then eta)
+  int K = 1, nseg = 1;     // a checkpoint every K steps; nseg segments
+  void* ckpt = nullptr;    // [nseg + 1][V + 1][N]: the states at steps 0, K, 2K, ... and the final one
+  void* seg = nullptr;     // [K - 1][V + 1][N]: the inner states of one segment (none when K = 1)
+  int seg_valid = -1;      // the segment whose inner states seg holds (-1: none)
   void* lam[2] = {nullptr, nullptr};
   void* Y = nullptr;   // [3 (V + 1)] spectra
   void* Zr = nullptr;  // [3 (V + 1)][N]
@@ -2565,23 +2568,38 @@ struct gs_padjoint {
   void* seed = nullptr;    // [V + 1][N]: dJ/d(c_T, eta_T)
   bool forward_done = false, seeded = false;
   size_t bytes = 0;
+  // the reverse sweep replayed as one captured graph (after a first direct
+  // run); captured with the mass-projection offset of its initial state
+  bool use_graph = true, warm = false;
+  cudaGraphExec_t gbwd = nullptr;
+  cudaStream_t gstream = nullptr;
+  int64_t nl_bwd = 0;
+  double g_mass0 = 0;
 };
+
+static void padj_graph_reset(gs_padjoint* a) {
+  if (a->gbwd) cudaGraphExecDestroy(a->gbwd);
+  a->gbwd = nullptr;
+}
 
 static void free_padjoint(gs_padjoint* a) {
   if (!a) return;
   cudaDeviceSynchronize();
-  for (void* q : {a->states, a->lam[0], a->lam[1], a->Y, a->Zr, a->dP, (void*)a->gsum, a->seed})
+  padj_graph_reset(a);
+  for (void* q : {a->ckpt, a->seg, a->lam[0], a->lam[1], a->Y, a->Zr, a->dP, (void*)a->gsum, a->seed})
     if (q) cudaFree(q);
   if (a->s) free_sim(a->s);
   delete a;
 }
 
-extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjoint** out) {
+extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, int checkpoint_every, gs_padjoint** out) {
   if (!p || !out) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_create: null argument");
   *out = nullptr;
   if (p->model != GS_MODEL_PRECIPITATE) return gs_set_error(GS_EINVAL, "precipitate adjoint: precipitate model only");
   if (p->mode != GS_MODE_BASELINE) return gs_set_error(GS_ENOTSUP, "precipitate adjoint: baseline mode only");
   if (nsteps < 1) return gs_set_error(GS_EINVAL, "precipitate adjoint: nsteps %d", nsteps);
+  if (checkpoint_every < 1 || checkpoint_every > nsteps)
+    return gs_set_error(GS_EINVAL, "precipitate adjoint: checkpoint_every %d outside 1..%d", checkpoint_every, nsteps);
   gs_padjoint* a = new gs_padjoint();
   int rc = gs_sim_create(p, &a->s);
   if (rc != GS_OK) {
@@ -2589,6 +2607,8 @@ extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjo
     return rc;
   }
   a->nsteps = nsteps;
+  a->K = checkpoint_every;
+  a->nseg = (nsteps + a->K - 1) / a->K;
   a->F1 = precip_nfields(a->s);
   const int V = p->nvariants;
   const size_t fb = (size_t)a->s->N * elt(a->s);
@@ -2597,7 +2617,8 @@ extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjo
     if (r == GS_OK) a->bytes += b;
     return r;
   };
-  if ((rc = get(&a->states, fb * (V + 1) * (nsteps + 1), "adjoint states")) != GS_OK ||
+  if ((rc = get(&a->ckpt, fb * (V + 1) * (a->nseg + 1), "adjoint checkpoints")) != GS_OK ||
+      (a->K > 1 && (rc = get(&a->seg, fb * (V + 1) * (a->K - 1), "adjoint segment states")) != GS_OK) ||
       (rc = get(&a->lam[0], fb * (V + 1), "adjoint lambda")) != GS_OK ||
       (rc = get(&a->lam[1], fb * (V + 1), "adjoint lambda")) != GS_OK ||
       (rc = get(&a->seed, fb * (V + 1), "adjoint seed")) != GS_OK ||
@@ -2609,6 +2630,9 @@ extern "C" int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjo
     free_padjoint(a);
     return rc;
   }
+  // the simulation's own buffers count too (fields, spectra, work arrays)
+  const int F2 = 2 * V + 2;
+  a->bytes += fb * ((size_t)V + 1 + (V + 1) + a->F1 + (V + 1) + F2);
   *out = a;
   return GS_OK;
 }
@@ -2620,50 +2644,122 @@ extern "C" int gs_precip_adjoint_destroy(gs_padjoint* a) {
 
 extern "C" size_t gs_precip_adjoint_device_bytes(const gs_padjoint* a) { return a ? a->bytes : 0; }
 
+extern "C" int gs_precip_adjoint_use_graph(gs_padjoint* a, int on) {
+  if (!a) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_use_graph: null handle");
+  a->use_graph = on != 0;
+  if (!a->use_graph) padj_graph_reset(a);
+  return GS_OK;
+}
+
+// copy the simulation's state (c, eta) to / from a [V + 1][N] slot
+static int padj_save(gs_padjoint* a, void* dst, cudaStream_t st) {
+  gs_sim* s = a->s;
+  const size_t fb = (size_t)s->N * elt(s);
+  GS_CU(cudaMemcpyAsync(dst, s->conc, fb, cudaMemcpyDeviceToDevice, st), "keep state");
+  GS_CU(cudaMemcpyAsync(static_cast<char*>(dst) + fb, s->eta[0], fb * s->p.nvariants, cudaMemcpyDeviceToDevice, st),
+        "keep state");
+  return GS_OK;
+}
+static int padj_load(gs_padjoint* a, const void* src, cudaStream_t st) {
+  gs_sim* s = a->s;
+  const size_t fb = (size_t)s->N * elt(s);
+  GS_CU(cudaMemcpyAsync(s->conc, src, fb, cudaMemcpyDeviceToDevice, st), "restore state");
+  GS_CU(cudaMemcpyAsync(s->eta[0], static_cast<const char*>(src) + fb, fb * s->p.nvariants, cudaMemcpyDeviceToDevice,
+                        st),
+        "restore state");
+  return GS_OK;
+}
+static char* padj_slot(void* base, const gs_padjoint* a, int i) {
+  return static_cast<char*>(base) + (size_t)i * (size_t)a->s->N * elt(a->s) * (a->s->p.nvariants + 1);
+}
+
+// the state of step n inside segment j (a0 = jK <= n <= b0): the two
+// checkpoints at its ends, the inner states in seg
+static char* padj_state(gs_padjoint* a, int j, int n) {
+  const int a0 = j * a->K, b0 = std::min(a0 + a->K, a->nsteps);
+  if (n == a0) return padj_slot(a->ckpt, a, j);
+  if (n == b0) return padj_slot(a->ckpt, a, j + 1);
+  return padj_slot(a->seg, a, n - a0 - 1);
+}
+
+// the inner states of segment j into seg, recomputed from checkpoint j with
+// the forward's own step counters (the same bits as the forward's states)
+static int padj_recompute(gs_padjoint* a, int j, cudaStream_t st) {
+  gs_sim* s = a->s;
+  const int a0 = j * a->K, b0 = std::min(a0 + a->K, a->nsteps);
+  if (b0 - a0 > 1) {
+    GS_TRY(padj_load(a, padj_slot(a->ckpt, a, j), st));
+    s->step = a0;
+    const bool f64 = s->p.dtype == GS_DTYPE_F64;
+    for (int n = a0 + 1; n < b0; ++n) {
+      GS_TRY(f64 ? precip_step<double>(s, st) : precip_step<float>(s, st));
+      GS_TRY(padj_save(a, padj_state(a, j, n), st));
+    }
+  }
+  a->seg_valid = j;
+  return GS_OK;
+}
+
 extern "C" int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
                                          void* eta_final, void* stream) {
   if (!a) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: null handle");
   if (!c0 != !eta0) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: give both c0 and eta0, or neither");
   gs_sim* s = a->s;
   const int V = s->p.nvariants;
-  const size_t N = (size_t)s->N, fb = N * elt(s);
+  const size_t N = (size_t)s->N;
   cudaStream_t st = pick_stream(s, stream);
-  char* S = static_cast<char*>(a->states);
   if (c0) {
     GS_TRY(gs_sim_set_field(s, "concentration", c0, N, dtype));
     GS_TRY(gs_sim_set_field(s, "eta", eta0, N * V, dtype));
   } else {  // again from the initial state of the previous forward run
     if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: no initial state yet");
-    GS_CU(cudaMemcpyAsync(s->conc, S, fb, cudaMemcpyDeviceToDevice, st), "initial state");
-    GS_CU(cudaMemcpyAsync(s->eta[0], S + fb, fb * V, cudaMemcpyDeviceToDevice, st), "initial state");
+    GS_TRY(padj_load(a, padj_slot(a->ckpt, a, 0), st));
   }
   s->step = 0;
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  const int last = a->nseg - 1, last0 = last * a->K;  // the last segment's inner states stay in seg
   for (int n = 0; n <= a->nsteps; ++n) {
-    char* dst = S + (size_t)n * fb * (V + 1);
-    GS_CU(cudaMemcpyAsync(dst, s->conc, fb, cudaMemcpyDeviceToDevice, st), "keep state");
-    GS_CU(cudaMemcpyAsync(dst + fb, s->eta[0], fb * V, cudaMemcpyDeviceToDevice, st), "keep state");
+    if (n % a->K == 0 || n == a->nsteps) GS_TRY(padj_save(a, padj_slot(a->ckpt, a, (n + a->K - 1) / a->K), st));
+    else if (n > last0) GS_TRY(padj_save(a, padj_state(a, last, n), st));
     if (n < a->nsteps) GS_TRY(f64 ? precip_step<double>(s, st) : precip_step<float>(s, st));
   }
   GS_CU(cudaStreamSynchronize(st), "forward sync");
+  a->seg_valid = a->nseg - 1;
   a->forward_done = true;
   if (c_final) GS_TRY(download(s, s->conc, c_final, N, dtype));
   if (eta_final) GS_TRY(download(s, s->eta[0], eta_final, N * V, dtype));
   return GS_OK;
 }
 
+// one reverse step n from lam[c] into lam[c ^ 1]; st0, st1: the states of
+// steps n and n + 1
+template <typename T>
+static int padj_reverse_step(gs_padjoint* a, int n, const T* st0, const T* st1, int c, cudaStream_t st);
+
 template <typename T> static int padj_backward(gs_padjoint* a, cudaStream_t st, int* cur) {
+  int c = 0;
+  for (int j = a->nseg - 1; j >= 0; --j) {
+    if (a->seg_valid != j) GS_TRY(padj_recompute(a, j, st));
+    const int a0 = j * a->K, b0 = std::min(a0 + a->K, a->nsteps);
+    for (int n = b0 - 1; n >= a0; --n) {
+      const T* st0 = reinterpret_cast<const T*>(padj_state(a, j, n));
+      const T* st1 = reinterpret_cast<const T*>(padj_state(a, j, n + 1));
+      GS_TRY(padj_reverse_step<T>(a, n, st0, st1, c, st));
+      c ^= 1;
+    }
+  }
+  *cur = c;
+  return GS_OK;
+}
+
+template <typename T>
+static int padj_reverse_step(gs_padjoint* a, int n, const T* st0, const T* st1, int c, cudaStream_t st) {
   gs_sim* s = a->s;
   const gs_params& p = s->p;
   const int V = p.nvariants, F1 = a->F1, FV = V + 1;
   const long long N = s->N, rows = (long long)s->n0 * s->n1;
-  const size_t fstate = (size_t)N * FV;
-  const T* S = reinterpret_cast<const T*>(a->states);
   T* Zr = reinterpret_cast<T*>(a->Zr);
-  int c = 0;
-  for (int n = a->nsteps - 1; n >= 0; --n) {
-    const T* st0 = S + (size_t)n * fstate;
-    const T* st1 = S + (size_t)(n + 1) * fstate;
+  {
     const T* lin = reinterpret_cast<const T*>(a->lam[c]);
     T* lout = reinterpret_cast<T*>(a->lam[c ^ 1]);
     // spectral pass over the pairs (lambda', state')
@@ -2794,9 +2890,7 @@ template <typename T> static int padj_backward(gs_padjoint* a, cudaStream_t st, 
     }
     GS_CU(launch_padj<T>(pa, true, st, &nb), "adjoint lambda");
     GS_CU(launch_reduce(s->partials, nb, 7, a->gsum + (size_t)n * PADJ_N + PADJ_A1, st), "adjoint reduce");
-    c ^= 1;
   }
-  *cur = c;
   return GS_OK;
 }
 
@@ -2823,9 +2917,46 @@ extern "C" int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, co
   const int V = s->p.nvariants;
   const size_t N = (size_t)s->N, fb = N * elt(s);
   cudaStream_t st = pick_stream(s, stream);
-  GS_CU(cudaMemcpyAsync(a->lam[0], a->seed, fb * (V + 1), cudaMemcpyDeviceToDevice, st), "seed");
+  const bool f64 = s->p.dtype == GS_DTYPE_F64;
+  // the sweep: the seed into lambda, then every segment (recomputed from its
+  // checkpoint unless its states are in seg) and its reverse steps
+  auto body = [&](int* cur) -> int {
+    GS_CU(cudaMemcpyAsync(a->lam[0], a->seed, fb * (V + 1), cudaMemcpyDeviceToDevice, st), "seed");
+    return f64 ? padj_backward<double>(a, st, cur) : padj_backward<float>(a, st, cur);
+  };
+  // a replayed graph starts from the forward's last segment, as captured
+  if (a->seg_valid != a->nseg - 1) GS_TRY(padj_recompute(a, a->nseg - 1, st));
   int c = 0;
-  GS_TRY(s->p.dtype == GS_DTYPE_F64 ? padj_backward<double>(a, st, &c) : padj_backward<float>(a, st, &c));
+  if (a->gbwd && (a->gstream != st || a->g_mass0 != s->mass0)) padj_graph_reset(a);
+  if (!a->use_graph || !a->warm) {
+    GS_TRY(body(&c));
+    a->warm = true;  // kernel attributes are set: later sweeps may be captured
+  } else {
+    if (!a->gbwd) {
+      cudaGraph_t g;
+      const int64_t l0 = s->launches;
+      const int64_t step0 = s->step;
+      GS_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+      const int rc = body(&c);
+      const cudaError_t e = cudaStreamEndCapture(st, &g);
+      s->step = step0;
+      if (rc != GS_OK) return rc;
+      GS_CU(e, "end capture");
+      GS_CU(cudaGraphInstantiate(&a->gbwd, g, 0), "instantiate graph");
+      cudaGraphDestroy(g);
+      a->gstream = st;
+      a->g_mass0 = s->mass0;
+      a->nl_bwd = s->launches - l0;
+      s->launches = l0;
+    } else {
+      c = a->nsteps % 2;  // lambda swaps once per step
+    }
+    GS_CU(cudaGraphLaunch(a->gbwd, st), "graph launch");
+    s->launches += a->nl_bwd;
+  }
+  // seg now holds segment 0 (the last one the sweep visits); the next sweep
+  // recomputes the last segment first
+  a->seg_valid = 0;
   std::vector<double> h((size_t)a->nsteps * PADJ_N);
   GS_CU(cudaMemcpyAsync(h.data(), a->gsum, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "sums D2H");
   GS_CU(cudaStreamSynchronize(st), "adjoint sync");

@@ -167,7 +167,8 @@ def lib() -> C.CDLL:
         "gs_adjoint_device_bytes": (C.c_size_t, [vp]),
         "gs_adjoint_use_graph": (C.c_int, [vp, C.c_int]),
         "gs_adjoint_launch_count": (C.c_int64, [vp]),
-        "gs_precip_adjoint_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
+        "gs_precip_adjoint_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),
+        "gs_precip_adjoint_use_graph": (C.c_int, [vp, C.c_int]),
         "gs_precip_adjoint_destroy": (C.c_int, [vp]),
         "gs_precip_adjoint_forward": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp]),
         "gs_precip_adjoint_backward": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(C.c_double), vp, vp, vp]),
@@ -294,18 +295,23 @@ class Adjoint:
 
 class PrecipAdjoint:
     """Adjoint of a precipitate run (gs_precip_adjoint*): forward() runs
-    (c0, eta0) -> (c_T, eta_T) keeping every state; backward(seed_c,
-    seed_eta) returns (grads[9], dJ/dc0, dJ/deta0) for J = <seed_c, c_T> +
-    <seed_eta, eta_T>, grads over (kappa_c, kappa_eta, coef[1..7])."""
+    (c0, eta0) -> (c_T, eta_T) keeping a checkpoint every `checkpoint_every`
+    steps; backward(seed_c, seed_eta) recomputes each segment and returns
+    (grads[9], dJ/dc0, dJ/deta0) for J = <seed_c, c_T> + <seed_eta, eta_T>,
+    grads over (kappa_c, kappa_eta, coef[1..7])."""
 
     PARAM_NAMES = ("kappa_c", "kappa_eta", "A1", "A2", "A3", "A4", "A5", "A6", "A7")
 
-    def __init__(self, params: GsParams, nsteps: int):
+    def __init__(self, params: GsParams, nsteps: int, checkpoint_every: int = 1):
         self.params = params.copy()
         self.nsteps = nsteps
         h = C.c_void_p()
-        check(lib().gs_precip_adjoint_create(C.byref(self.params), nsteps, C.byref(h)), "gs_precip_adjoint_create")
+        check(lib().gs_precip_adjoint_create(C.byref(self.params), nsteps, checkpoint_every, C.byref(h)),
+              "gs_precip_adjoint_create")
         self.h = h
+
+    def use_graph(self, on: bool) -> None:
+        check(lib().gs_precip_adjoint_use_graph(self.h, 1 if on else 0), "gs_precip_adjoint_use_graph")
 
     def close(self) -> None:
         if self.h:

@@ -316,20 +316,31 @@ int64_t gs_adjoint_launch_count(const gs_adjoint* a);
  * transposes; the local terms' Jacobians are applied pointwise and the
  * elastic coupling through the same B convolution.  The noise is additive
  * and drops out; the mass projection only corrects rounding and is not
- * differentiated.  Every state of the run is kept on the device ((nsteps+1)
- * (V+1) N values).  gs_precip_adjoint_backward returns, for J = <seed_c, c_T>
+ * differentiated.  The forward keeps the state every checkpoint_every = K
+ * steps and the states of the last segment; the backward recomputes each
+ * earlier segment from its checkpoint (with the forward's own step
+ * counters, so the states are the same bits) before sweeping it back, so
+ * the device holds (ceil(nsteps/K) + K + 1) (V+1) N state values (K = 1:
+ * every state, no recomputation).  After a first direct run the reverse
+ * sweep (recomputes included) is replayed as one captured CUDA graph
+ * (gs_precip_adjoint_use_graph(a, 0) launches directly; a new initial
+ * concentration mass or stream recaptures).  gs_precip_adjoint_backward
+ * returns, for J = <seed_c, c_T>
  * + <seed_eta, eta_T>, grads[9] = dJ/d(kappa_c, kappa_eta, coef[1..7]) and
  * dJ/dc0, dJ/deta0 (host buffers of dtype, NULL to skip).  NULL seeds reuse
  * the ones last given (gs_precip_adjoint_set_seed, kept on the device); NULL
  * c0 and eta0 rerun the forward from the previous initial state. */
 typedef struct gs_padjoint gs_padjoint;
-int gs_precip_adjoint_create(const gs_params* p, int nsteps, gs_padjoint** out);
+int gs_precip_adjoint_create(const gs_params* p, int nsteps, int checkpoint_every, gs_padjoint** out);
 int gs_precip_adjoint_destroy(gs_padjoint* a);
+int gs_precip_adjoint_use_graph(gs_padjoint* a, int on);
 int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
                               void* eta_final, void* stream);
 int gs_precip_adjoint_set_seed(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype);
 int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype, double* grads,
                                void* grad_c0, void* grad_eta0, void* stream);
+/* Device bytes of the handle: checkpoints, segment, adjoint work arrays and
+ * the simulation's own buffers. */
 size_t gs_precip_adjoint_device_bytes(const gs_padjoint* a);
 
 /* ---- batched ensembles ------------------------------------------------- */

@@ -27,8 +27,8 @@ def setup(gb, shape, V=4, dtype=F64, noise=0.0, c_elastic=1, seed=2):
     return p, c0, e0, rng.standard_normal(c0.shape), rng.standard_normal(e0.shape)
 
 
-def gpu_adjoint(gb, p, c0, e0, ns, sc, se):
-    a = gb.PrecipAdjoint(p, ns)
+def gpu_adjoint(gb, p, c0, e0, ns, sc, se, K=1):
+    a = gb.PrecipAdjoint(p, ns, K)
     try:
         cT, eT = a.forward(c0, e0)
         g, gc, ge = a.backward(sc, se)
@@ -42,15 +42,17 @@ def close_vec(g, og, rtol):
     return np.all(np.abs(g - og) <= rtol * np.abs(og) + 1e-12 * np.abs(og).max())
 
 
-@pytest.mark.parametrize("shape,V,ns,noise,ce", [
-    ((6, 8, 4), 4, 3, 0.0, 1),
-    ((8, 8, 12), 3, 4, 1e-3, 1),
-    ((8, 12, 2), 2, 5, 0.0, 0),
-    ((1, 16, 24), 2, 4, 1e-3, 1),
+@pytest.mark.parametrize("shape,V,ns,noise,ce,K", [
+    ((6, 8, 4), 4, 3, 0.0, 1, 1),
+    ((8, 8, 12), 3, 4, 1e-3, 1, 3),
+    ((8, 12, 2), 2, 5, 0.0, 0, 2),
+    ((1, 16, 24), 2, 4, 1e-3, 1, 4),
+    ((8, 8, 8), 4, 7, 1e-3, 1, 3),
 ])
-def test_precip_adjoint_f64_matches_oracle(gb, orc, shape, V, ns, noise, ce):
+def test_precip_adjoint_f64_matches_oracle(gb, orc, shape, V, ns, noise, ce, K):
+    """K: a checkpoint every K steps, the other states recomputed."""
     p, c0, e0, sc, se = setup(gb, shape, V, F64, noise, ce)
-    g, gc, ge, cT, eT = gpu_adjoint(gb, p, c0, e0, ns, sc, se)
+    g, gc, ge, cT, eT = gpu_adjoint(gb, p, c0, e0, ns, sc, se, K)
     og, ogc, oge = orc.precip_adjoint(p, c0, e0, ns, sc, se)
     oc, oe = orc.precip_run(p, c0, e0, ns)
     assert rel_l2(cT, oc) < 1e-11 and rel_l2(eT, oe) < 1e-11
@@ -115,6 +117,10 @@ def test_precip_adjoint_rejects(gb):
     q = gb.precip3d_params(8, dtype=F64)
     with pytest.raises(RuntimeError):
         gb.PrecipAdjoint(q, 0)
+    with pytest.raises(RuntimeError):
+        gb.PrecipAdjoint(q, 3, 4)  # a checkpoint spacing beyond the run
+    with pytest.raises(RuntimeError):
+        gb.PrecipAdjoint(q, 3, 0)
     a = gb.PrecipAdjoint(q, 2)
     try:
         c0 = np.zeros((8, 8, 8))
@@ -142,3 +148,52 @@ def test_precip_adjoint_replay(gb):
     assert np.array_equal(cT, cT2) and np.array_equal(eT, eT2)
     assert np.array_equal(g, g2) and np.array_equal(g, g3)
     assert np.array_equal(gc, gc2) and np.array_equal(ge, ge2)
+
+
+@pytest.mark.parametrize("dtype", [F32, F64])
+def test_precip_adjoint_checkpoints_and_graph_give_the_same_bits(gb, dtype):
+    """Every checkpoint spacing recomputes the same states (the forward's
+    step counters, noise on), so the gradients equal those of the run that
+    keeps every state bit for bit; the captured reverse sweep equals the
+    direct one; repeated sweeps (the last segment recomputed first) too."""
+    p, c0, e0, sc, se = setup(gb, (8, 8, 12), 3, dtype, 1e-3, 1, seed=9)
+    ns = 7
+    ref = None
+    for K in (1, 2, 3, 7):
+        for graph in (False, True):
+            a = gb.PrecipAdjoint(p, ns, K)
+            try:
+                a.use_graph(graph)
+                a.forward(c0, e0)
+                outs = [a.backward(sc, se) for _ in range(3)]  # the third replays the captured graph
+                nbytes = a.device_bytes()
+            finally:
+                a.close()
+            for g, gc, ge in outs:
+                assert np.isfinite(g).all()
+                if ref is None:
+                    ref = (g, gc, ge, nbytes)
+                assert np.array_equal(g, ref[0]) and np.array_equal(gc, ref[1]) and np.array_equal(ge, ref[2]), (K, graph)
+            if K in (2, 3):  # (ceil(7 / K) + 1) + (K - 1) kept states against 8
+                assert nbytes < ref[3]
+
+
+def test_precip_adjoint_graph_recaptured_for_a_new_initial_mass(gb, orc):
+    """A forward from a new initial concentration changes the mass projection
+    offset baked into the captured sweep: the sweep is captured again and the
+    gradients follow the new run."""
+    p, c0, e0, sc, se = setup(gb, (8, 8, 8), 3, F64, 0.0, 1, seed=13)
+    ns = 4
+    c1 = c0 + 0.01
+    a = gb.PrecipAdjoint(p, ns, 2)
+    try:
+        a.forward(c0, e0)
+        for _ in range(2):
+            a.backward(sc, se)
+        a.forward(c1, e0)
+        g, gc, ge = a.backward(sc, se)
+    finally:
+        a.close()
+    og, ogc, oge = orc.precip_adjoint(p, c1, e0, ns, sc, se)
+    assert close_vec(g, og, 1e-9), (g, og)
+    assert rel_l2(gc, ogc) < 1e-10 and rel_l2(ge, oge) < 1e-10
