@@ -339,6 +339,23 @@ def extra_ensemble(steps: int = 100, total_steps: int = 2000) -> dict:
             "per_shape_ms_per_step": per_shape, "timed_steps": steps}
 
 
+def precip_pass_bytes(names: list, p) -> dict:
+    """Algorithmic HBM bytes of each pass of the precipitate step (FP32, V
+    variants, F1 = V + 1 chain-1 fields with the concentration's misfit):
+    every field or spectrum a pass must read or write once.  At V = 4 the
+    step moves 460 N bytes."""
+    V, N = p.nvariants, p.ncells
+    F1 = V + (1 if p.c_elastic else 0)
+    f = 4 * N
+    table = {"z_forward": 2 * F1 * f, "y_forward": 2 * F1 * f, "x_contraction": 2 * F1 * f,
+             "y_inverse": 2 * F1 * f, "precip_mid": (F1 + (V + 1) + (2 * V + 2)) * f,
+             "z_inverse_potential": 2 * F1 * f, "precip_local": (F1 + (V + 1) + (V + 1)) * f,
+             "z_forward_update_fields": (2 * V + 2) * 2 * f, "y_forward_update_fields": 2 * (2 * V + 2) * f,
+             "x_kspace_update": ((2 * V + 2) + (V + 1)) * f, "y_inverse_update_fields": 2 * (V + 1) * f,
+             "z_inverse_c_eta": 2 * (V + 1) * f}
+    return {nm: table[nm] for nm in names}
+
+
 def extra_configs() -> dict:
     """The other workloads of the step, timed the same way: the 2D FP64
     martensite (128^2, 2 variants, 1000-step runs), the headline martensite
@@ -385,10 +402,26 @@ def extra_configs() -> dict:
         ms = _timed(stream, lambda: sim.step(steps, sh)) / steps
         m1 = sim.stats(sh)["mass"]
         launches = sim.launch_count()
+        passes = [sim.profile_step(sh) for _ in range(3)]
+        names = sim.pass_names()
         sim.close()
-        out["precipitate_fp32_256"] = {"ms_per_step": ms, "cell_updates_per_s": p.ncells * 1e3 / ms, "steps": steps,
-                                       "launches_per_step": launches / steps,
-                                       "mass_drift_relative": abs(m1 - m0) / abs(m0)}
+        pass_ms = np.median(np.array(passes), axis=0)
+        algo = precip_pass_bytes(names, p)
+        dom = int(np.argmax(pass_ms))
+        peak = measured_peaks()
+        step_bytes = sum(algo.values())
+        out["precipitate_fp32_256"] = {
+            "ms_per_step": ms, "cell_updates_per_s": p.ncells * 1e3 / ms, "steps": steps,
+            "launches_per_step": launches / steps, "mass_drift_relative": abs(m1 - m0) / abs(m0),
+            "step_bytes_algorithmic": step_bytes,
+            "step_gbs_algorithmic": step_bytes / (ms / 1e3) / 1e9,
+            "roofline": {"bound": "hbm", "kernel": names[dom], "launch_ms": float(pass_ms[dom]),
+                         "algorithmic_bytes_per_launch": algo[names[dom]],
+                         "achieved": algo[names[dom]] / (pass_ms[dom] / 1e3) / 1e9, "peak": peak["hbm_gbs"],
+                         "unit": "GB/s", "frac": algo[names[dom]] / (pass_ms[dom] / 1e3) / 1e9 / peak["hbm_gbs"],
+                         "peak_source": peak["source"],
+                         "pass_ms": {nm: float(t) for nm, t in zip(names, pass_ms)},
+                         "pass_bytes": algo}}
     return out
 
 

@@ -1499,6 +1499,11 @@ extern "C" int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int
   return GS_OK;
 }
 
+extern "C" const char* gs_sim_pass_name(const gs_sim* s, int i) {
+  if (!s || i < 0 || i + 1 >= s->nmarks) return nullptr;
+  return s->mark_names[i + 1];
+}
+
 // ---------------------------------------------------------------------------
 // batched ensembles: many independent martensite simulations, one launch per
 // pass per shape group, optionally replayed as a captured CUDA graph

@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
 #pragma unroll
     for (int p = 0; p < VM; ++p)
       if (p < Vn) ldv<CW>(a.eta_in + p * N + cell, e[p]);
-    T s2[CW], s4[CW], pr[CW];
+    T s2[CW], s4[CW], pr[CW], P0[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
       T a2 = 0, a4 = 0, ap = 0;
@@ -215,7 +215,16 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       s2[j] = a2;
       s4[j] = a4;
       pr[j] = ap;
+      // the part of the baseline Landau factor shared by every variant of
+      // the cell: A2 + 2 Ac S + A6 S^2, S = sum of eta^2
+      P0[j] = mc.A2 + a2 * ((T)2 * mc.Ac + mc.A6 * a2);
     }
+    // baseline factored update (not the statistics sweep): per variant
+    //   rhs = g + eta (m - L (P0 - (A4 + 2 Ac) eta^2) + el R),
+    // g the stencil's neighbour sums, its centre term -2 sum(lapc) eta folded
+    // into m = lin_p - 2 sum(lapc) (+ kc K_p)
+    const T cA = mc.A4 + (T)2 * mc.Ac;
+    const T lapsum2 = (T)2 * (mc.lapc[0] + mc.lapc[1] + mc.lapc[2]);
     T dfc[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) dfc[j] = 1;
@@ -252,12 +261,27 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       if (!STATS && mc.noise != (T)0)
         normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
       const T lq = mc.lin[q];
+      const T lqc = lq - lapsum2;
       T out[CW], rv[CW];
 #pragma unroll
       for (int j = 0; j < CW; ++j) {
         const T et = e[q][j];
         const T zlv = j == 0 ? el_ : e[q][j - 1];
         const T zrv = j == CW - 1 ? er_ : e[q][j + 1];
+        const T xij = CW == 2 ? (hi_pair ? xi[j + 2 < 4 ? j + 2 : 3] : xi[j]) : xi[j];
+        if (!STATS && !mc.refcompat) {
+          const T Rv = Rl[j];
+          const T e2 = et * et;
+          const T g = mc.lapc[0] * (vxp[j] + vxm[j]) + (mc.lapc[1] * (vyp[j] + vym[j]) + mc.lapc[2] * (zlv + zrv));
+          const T m = lqc + mc.kc * Kq[j];
+          const T coef = -mc.L * (P0[j] - cA * e2) + (mc.el * Rv + m);
+          const T rhs = et * coef + g;
+          T en = et + mc.dt * rhs + mc.noise * xij;
+          if (mc.has_defect) en *= dfc[j];
+          out[j] = en;
+          rv[j] = Rv;
+          continue;
+        }
         const T d0 = vxp[j] + vxm[j] - 2 * et, d1 = vyp[j] + vym[j] - 2 * et, d2 = zlv + zrv - 2 * et;
         const T grad = mc.lapc[0] * d0 + mc.lapc[1] * d1 + mc.lapc[2] * d2;
         T chem;
@@ -275,7 +299,6 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
         const T el = mc.el * Rv * et;
         const T lin = (lq + mc.kc * Kq[j]) * et;
         const T rhs = grad + chem + el + lin;
-        const T xij = CW == 2 ? (hi_pair ? xi[j + 2 < 4 ? j + 2 : 3] : xi[j]) : xi[j];
         T en = et + mc.dt * rhs + mc.noise * xij;
         if (mc.has_defect) en *= dfc[j];
         out[j] = en;

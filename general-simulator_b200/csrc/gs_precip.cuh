@@ -104,8 +104,11 @@ template <typename T> struct PrecipMidArgs {
   PrecipLocalArgs<T> loc;  // coefficients, noise, V, c_elastic (pointers unused)
 };
 
+// three resident blocks of 240 threads (the 256^3 tile): at 101 registers
+// only two fitted, and the sweep waited on its loads and barriers with 24 %
+// of the warp slots occupied
 template <typename T, int H, int VM>
-__global__ void __launch_bounds__(256) k_precip_mid(PrecipMidArgs<T> a) {
+__global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
   constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;

@@ -155,6 +155,7 @@ def lib() -> C.CDLL:
         "gs_batch_launch_count": (C.c_int64, [vp]),
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
+        "gs_sim_pass_name": (C.c_char_p, [vp, C.c_int]),
         "gs_cufft_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_cufft_step": (C.c_int, [vp, C.c_int, vp]),
         "gs_adjoint_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),
@@ -452,6 +453,15 @@ class Sim:
         n = C.c_int()
         check(lib().gs_sim_profile_step(self.h, C.c_void_p(stream), buf, 32, C.byref(n)), "profile_step")
         return [buf[i] for i in range(n.value)]
+
+    def pass_names(self) -> list:
+        """Names of the passes of the last profile_step, in launch order."""
+        out = []
+        while True:
+            nm = lib().gs_sim_pass_name(self.h, len(out))
+            if nm is None:
+                return out
+            out.append(nm.decode())
 
     def launch_count(self) -> int:
         return int(lib().gs_sim_launch_count(self.h))

@@ -198,6 +198,11 @@ int gs_sim_set_field_async(gs_sim* s, const char* name, const void* host, size_t
  * z forward, y forward, x contraction, y inverse, update for the
  * martensite step; y passes are absent when the middle axis is 1). */
 int gs_sim_profile_step(gs_sim* s, void* stream, double* pass_ms, int max_pass, int* npass);
+/* The name of pass i of the last gs_sim_profile_step (or GS_TIMING step):
+ * "z_forward", "y_forward", "x_contraction", "y_inverse", "update",
+ * "precip_mid", "x_kspace_update", ...; NULL past the last pass.  The string
+ * is static. */
+const char* gs_sim_pass_name(const gs_sim* s, int i);
 /* Hand a field from one simulation to another on the device, replacing the
  * reference's file hand-off between stages (dump stress/defect, then read
  * dislocationstress/defect: scripts/in.precipitate.sh; remap on the host,
