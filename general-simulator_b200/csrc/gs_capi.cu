@@ -3166,3 +3166,318 @@ extern "C" int gs_sim_set_field_async(gs_sim* s, const char* name, const void* h
   GS_CU(cudaMemcpyAsync(s->eta[s->cur], host, n * elt(s), cudaMemcpyHostToDevice, st), "upload");
   return GS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// a simulation split into slabs along axis 0, one slab per rank
+// ---------------------------------------------------------------------------
+// The reference holds a whole grid on one device (one cuFFT plan over it,
+// src/dynamics_mart.cu:113-117).  Here a martensite grid nx x ny x nz is cut
+// into R slabs of nx/R x-planes.  A step is three local phases with two
+// all-to-all transposes and a halo exchange between them, which the caller
+// performs (NCCL through torch.distributed on GPUs, device copies when all
+// slabs share one device):
+//   begin: z forward of eta^2 (or the spectra the last update left), y
+//          forward, pack the spectra by destination kz range
+//          [R][V][nx/R][ny][h/R] into `send`; the slab's two face planes
+//          [2][V][ny][nz] into `halo_send`;
+//   xpass: unpack the received pieces into x-pencils [V][nx][ny][h/R] (all
+//          x for this rank's kz range), x forward -> B contraction -> x
+//          inverse, pack by destination x range into `send`;
+//   end:   unpack into the slab's spectra, y inverse, the fused update with
+//          the neighbours' face planes as halos (and the next z forward).
+// Every line transform, table point and cell update is the single-grid
+// kernels' own arithmetic, so the slabs reproduce the one-device step bit for
+// bit.  No load of another device's memory is issued here.
+struct gs_slab {
+  gs_sim* loc = nullptr;  // this rank's slab: fields, local spectra, stream, twiddles of y and z
+  gs_sim geo;             // the whole grid's geometry and parameters (no buffers)
+  int rank = 0, nranks = 1, x0 = 0, hr = 0;
+  void* pencil = nullptr;  // x-pencil spectra [V][nx][ny][h/R]
+  void* twx = nullptr;     // twiddles of the whole x axis
+  void* btab = nullptr;    // octant B table of the whole grid (null: B formed per k)
+  int btab_fields = 0;
+  bool z_ready = false;    // the slab's spectra hold the z transforms of eta[cur]^2
+};
+
+template <typename T>
+__global__ void k_copy5(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, long long n, int d1, int d2, int d3,
+                        int d4, long long s0, long long s1, long long s2, long long s3, long long t0, long long t1,
+                        long long t2, long long t3) {
+  // dims (d0, d1, d2, d3, d4), innermost contiguous on both sides
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    long long r = i;
+    const int i4 = (int)(r % d4);
+    r /= d4;
+    const int i3 = (int)(r % d3);
+    r /= d3;
+    const int i2 = (int)(r % d2);
+    r /= d2;
+    const int i1 = (int)(r % d1);
+    const long long i0 = r / d1;
+    dst[i0 * t0 + i1 * t1 + i2 * t2 + i3 * t3 + i4] = src[i0 * s0 + i1 * s1 + i2 * s2 + i3 * s3 + i4];
+  }
+}
+
+template <typename T>
+static int copy5(const void* src, void* dst, const int d[5], const long long ss[4], const long long ts[4],
+                 cudaStream_t st) {
+  const long long n = (long long)d[0] * d[1] * d[2] * d[3] * d[4];
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_copy5<T><<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<const cplx<T>*>(src), reinterpret_cast<cplx<T>*>(dst),
+                                                 n, d[1], d[2], d[3], d[4], ss[0], ss[1], ss[2], ss[3], ts[0], ts[1],
+                                                 ts[2], ts[3]);
+  GS_CU(cudaGetLastError(), "slab transpose copy");
+  return GS_OK;
+}
+
+static void free_slab(gs_slab* sl) {
+  if (!sl) return;
+  cudaDeviceSynchronize();
+  for (void* q : {sl->pencil, sl->twx, sl->btab})
+    if (q) cudaFree(q);
+  if (sl->loc) free_sim(sl->loc);
+  delete sl;
+}
+
+template <typename T> static int slab_init(gs_slab* sl) {
+  gs_sim& g = sl->geo;
+  const int gn0 = g.n0;
+  // twiddles of the whole x axis
+  std::vector<cplx<T>> tw(gn0);
+  for (int m = 0; m < gn0; ++m) {
+    const double a = 2.0 * M_PI * (double)m / (double)gn0;
+    tw[m] = mk2((T)std::cos(a), (T)-std::sin(a));
+  }
+  GS_CU(cudaMalloc(&sl->twx, sizeof(cplx<T>) * gn0), "cudaMalloc x twiddles");
+  GS_CU(cudaMemcpy(sl->twx, tw.data(), sizeof(cplx<T>) * gn0, cudaMemcpyHostToDevice), "upload x twiddles");
+  // the octant table of the whole grid (as build_btab makes it)
+  if (btab_symmetric(&g)) {
+    ElasticConst<T> ec;
+    build_elastic<T>(&g, 0, 1.0 / (double)g.N, ec);
+    sl->btab_fields = ec.nb;
+    const size_t npt = (size_t)(g.n0 / 2 + 1) * (g.n1 / 2 + 1) * (g.n2 / 2 + 1);
+    GS_CU(cudaMalloc(&sl->btab, npt * btab_stride(ec.nb) * sizeof(T)), "cudaMalloc B table");
+    GS_CU(launch_btab_fill<T>(ec, g.n0, g.n1, g.n2, reinterpret_cast<T*>(sl->btab), sl->loc->own_stream),
+          "B table fill");
+  }
+  const size_t pb = sizeof(cplx<T>) * (size_t)g.p.nvariants * gn0 * g.n1 * sl->hr;
+  GS_CU(cudaMalloc(&sl->pencil, pb), "cudaMalloc x pencils");
+  GS_CU(cudaStreamSynchronize(sl->loc->own_stream), "slab init");
+  return GS_OK;
+}
+
+extern "C" int gs_slab_create(const gs_params* p, int rank, int nranks, gs_slab** out) {
+  if (!p || !out) return gs_set_error(GS_EINVAL, "gs_slab_create: null argument");
+  *out = nullptr;
+  if (p->model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "gs_slab_create: martensite only");
+  if (nranks < 1 || rank < 0 || rank >= nranks)
+    return gs_set_error(GS_EINVAL, "gs_slab_create: rank %d of %d", rank, nranks);
+  if (p->nx < 2 || p->ny < 2 || p->nz < 2)
+    return gs_set_error(GS_ENOTSUP, "gs_slab_create: a 3D grid is split (got %dx%dx%d)", p->nx, p->ny, p->nz);
+  if (p->nx % nranks != 0 || (p->nz / 2) % nranks != 0)
+    return gs_set_error(GS_EINVAL, "gs_slab_create: nx %d and nz/2 %d must be multiples of %d ranks", p->nx,
+                        p->nz / 2, nranks);
+  gs_slab* sl = new gs_slab();
+  sl->geo.p = *p;
+  int rc = canonicalize(&sl->geo);
+  if (rc != GS_OK) {
+    delete sl;
+    return rc;
+  }
+  sl->rank = rank;
+  sl->nranks = nranks;
+  sl->x0 = rank * (p->nx / nranks);
+  sl->hr = sl->geo.h / nranks;
+  gs_params lp = *p;
+  lp.nx = p->nx / nranks;
+  if ((rc = gs_sim_create(&lp, &sl->loc)) != GS_OK) {
+    delete sl;
+    return rc;
+  }
+  // the slab's own table would describe a grid of nx/R planes: the whole
+  // grid's table replaces it
+  if (sl->loc->btab) cudaFree(sl->loc->btab);
+  sl->loc->btab = nullptr;
+  sl->loc->btab_state = -1;
+  rc = p->dtype == GS_DTYPE_F64 ? slab_init<double>(sl) : slab_init<float>(sl);
+  if (rc != GS_OK) {
+    free_slab(sl);
+    return rc;
+  }
+  *out = sl;
+  return GS_OK;
+}
+
+extern "C" int gs_slab_destroy(gs_slab* sl) {
+  free_slab(sl);
+  return GS_OK;
+}
+
+extern "C" int gs_slab_info(const gs_slab* sl, gs_slab_geometry* out) {
+  if (!sl || !out) return gs_set_error(GS_EINVAL, "gs_slab_info: null argument");
+  const gs_sim* l = sl->loc;
+  out->rank = sl->rank;
+  out->nranks = sl->nranks;
+  out->x0 = sl->x0;
+  out->nx_local = l->n0;
+  out->kz0 = sl->rank * sl->hr;
+  out->nkz_local = sl->hr;
+  out->a2a_bytes = (size_t)l->N * l->p.nvariants * elt(l);  // the slab's spectra: [R][V][nx/R][ny][h/R] complex
+  out->halo_bytes = 2 * (size_t)l->n1 * l->n2 * l->p.nvariants * elt(l);
+  out->step = l->step;
+  return GS_OK;
+}
+
+extern "C" int gs_slab_set_field(gs_slab* sl, const char* name, const void* host, size_t count, int dtype) {
+  if (!sl) return gs_set_error(GS_EINVAL, "gs_slab_set_field: null handle");
+  if (!name || std::string(name) != "eta") return gs_set_error(GS_EINVAL, "gs_slab_set_field: only \"eta\"");
+  sl->z_ready = false;
+  return gs_sim_set_field(sl->loc, name, host, count, dtype);
+}
+
+extern "C" int gs_slab_get_field(gs_slab* sl, const char* name, void* host, size_t count, int dtype) {
+  if (!sl) return gs_set_error(GS_EINVAL, "gs_slab_get_field: null handle");
+  return gs_sim_get_field(sl->loc, name, host, count, dtype);
+}
+
+extern "C" int gs_slab_set_step(gs_slab* sl, int64_t step) {
+  if (!sl || step < 0) return gs_set_error(GS_EINVAL, "gs_slab_set_step: bad argument");
+  sl->loc->step = step;
+  return GS_OK;
+}
+
+template <typename T> static int slab_begin(gs_slab* sl, void* send, void* halo_send, cudaStream_t st) {
+  gs_sim* l = sl->loc;
+  const int V = l->p.nvariants, R = sl->nranks, n0r = l->n0, n1 = l->n1, h = l->h, hr = sl->hr;
+  const T* eta = reinterpret_cast<const T*>(l->eta[l->cur]);
+  if (!sl->z_ready) {
+    ZfwdArgs<T> za;
+    memset(&za, 0, sizeof(za));
+    for (int f = 0; f < V; ++f) {
+      za.src[f] = eta + (long long)f * l->N;
+      za.square[f] = 1;
+    }
+    za.dst = reinterpret_cast<cplx<T>*>(l->spec);
+    za.rows_per_field = (long long)n0r * n1;
+    za.nrows = za.rows_per_field * V;
+    za.tw_h = twp<T>(l, 1);
+    za.tw_n2 = twp<T>(l, 0);
+    GS_CU(launch_zfwd<T>(za, h, st, l->sched.z_lines), "slab z forward");
+  }
+  YArgs<T> ya;
+  ya.spec = reinterpret_cast<cplx<T>*>(l->spec);
+  ya.n0 = n0r;
+  ya.n1 = n1;
+  ya.h = h;
+  ya.tw = twp<T>(l, 2);
+  GS_CU(launch_ypass<T>(ya, n1, V, -1, st, l->sched.y_cols), "slab y forward");
+  // [V][x][y][kz = r hr + k] -> send [r][V][x][y][k]
+  const int d[5] = {R, V, n0r, n1, hr};
+  const long long ss[4] = {hr, (long long)n0r * n1 * h, (long long)n1 * h, h};
+  const long long ts[4] = {(long long)V * n0r * n1 * hr, (long long)n0r * n1 * hr, (long long)n1 * hr, hr};
+  GS_TRY(copy5<T>(l->spec, send, d, ss, ts, st));
+  // face planes: [0] = plane 0, [1] = plane nx/R - 1, each [V][ny][nz]
+  const size_t plane = (size_t)n1 * l->n2 * sizeof(T);
+  char* hs = static_cast<char*>(halo_send);
+  GS_CU(cudaMemcpy2DAsync(hs, plane, eta, (size_t)l->N * sizeof(T), plane, V, cudaMemcpyDeviceToDevice, st),
+        "slab face plane");
+  GS_CU(cudaMemcpy2DAsync(hs + plane * V, plane, eta + (size_t)(n0r - 1) * n1 * l->n2, (size_t)l->N * sizeof(T), plane,
+                          V, cudaMemcpyDeviceToDevice, st),
+        "slab face plane");
+  return GS_OK;
+}
+
+template <typename T> static int slab_xpass(gs_slab* sl, const void* recv, void* send, cudaStream_t st) {
+  gs_sim* l = sl->loc;
+  gs_sim& g = sl->geo;
+  const int V = l->p.nvariants, R = sl->nranks, n0r = l->n0, n1 = l->n1, hr = sl->hr, gn0 = g.n0;
+  // recv [s][V][x][y][k] -> pencil [V][s nx/R + x][y][k]
+  const int d[5] = {R, V, n0r, n1, hr};
+  const long long rs[4] = {(long long)V * n0r * n1 * hr, (long long)n0r * n1 * hr, (long long)n1 * hr, hr};
+  const long long ps[4] = {(long long)n0r * n1 * hr, (long long)gn0 * n1 * hr, (long long)n1 * hr, hr};
+  GS_TRY(copy5<T>(recv, sl->pencil, d, rs, ps, st));
+  XArgs<T> xa;
+  memset(&xa, 0, sizeof(xa));
+  xa.in = reinterpret_cast<cplx<T>*>(sl->pencil);
+  xa.out = reinterpret_cast<cplx<T>*>(sl->pencil);
+  xa.n0 = gn0;
+  xa.n1 = n1;
+  xa.n2 = g.n2;
+  xa.h = hr;
+  xa.hg = g.h;
+  xa.kz_off = sl->rank * hr;
+  xa.F = V;
+  xa.G = V;
+  xa.tw = reinterpret_cast<const cplx<T>*>(sl->twx);
+  build_elastic<T>(&g, 0, 1.0 / (double)g.N, xa.ec);
+  if (sl->btab && sl->btab_fields == V) {
+    xa.btab = reinterpret_cast<const T*>(sl->btab);
+    xa.bt_d1 = n1 / 2 + 1;
+    xa.bt_d2 = g.n2 / 2 + 1;
+    xa.bt_stride = btab_stride(V);
+  }
+  xa.tz_req = l->sched.x_cols;
+  GS_CU(launch_xcontract<T>(xa, st), "slab x pass");
+  // pencil -> send [s][V][x][y][k] (destination s takes its x range)
+  GS_TRY(copy5<T>(sl->pencil, send, d, ps, rs, st));
+  return GS_OK;
+}
+
+template <typename T> static int slab_end(gs_slab* sl, const void* recv, const void* halo_recv, cudaStream_t st) {
+  gs_sim* l = sl->loc;
+  const int V = l->p.nvariants, R = sl->nranks, n0r = l->n0, n1 = l->n1, h = l->h, hr = sl->hr;
+  // recv [r][V][x][y][k] -> spectra [V][x][y][r hr + k]
+  const int d[5] = {R, V, n0r, n1, hr};
+  const long long rs[4] = {(long long)V * n0r * n1 * hr, (long long)n0r * n1 * hr, (long long)n1 * hr, hr};
+  const long long ss[4] = {hr, (long long)n0r * n1 * h, (long long)n1 * h, h};
+  GS_TRY(copy5<T>(recv, l->spec, d, rs, ss, st));
+  YArgs<T> ya;
+  ya.spec = reinterpret_cast<cplx<T>*>(l->spec);
+  ya.n0 = n0r;
+  ya.n1 = n1;
+  ya.h = h;
+  ya.tw = twp<T>(l, 2);
+  GS_CU(launch_ypass<T>(ya, n1, V, 1, st, l->sched.y_cols), "slab y inverse");
+  T* in = reinterpret_cast<T*>(l->eta[l->cur]);
+  T* out = reinterpret_cast<T*>(l->eta[l->cur ^ 1]);
+  MartArgs<T> ma;
+  fill_mart_args<T>(l, ma, in, out);
+  build_mart_p<T>(&sl->geo, sl->geo.p, l->step, ma.mc);  // the whole grid's stencil and constants
+  ma.spec_next = reinterpret_cast<cplx<T>*>(l->spec);
+  ma.halo = reinterpret_cast<const T*>(halo_recv);
+  ma.cell_off = (long long)sl->x0 * n1 * l->n2;
+  GS_CU(launch_mart_update<T>(ma, h, false, st, nullptr), "slab update");
+  l->cur ^= 1;
+  l->step += 1;
+  sl->z_ready = true;
+  return GS_OK;
+}
+
+static int slab_check(gs_slab* sl, const void* a, const void* b, const char* what) {
+  if (!sl || !a || !b) return gs_set_error(GS_EINVAL, "%s: null argument", what);
+  if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15u)
+    return gs_set_error(GS_EINVAL, "%s: buffers must be 16-byte aligned", what);
+  return GS_OK;
+}
+
+extern "C" int gs_slab_begin(gs_slab* sl, void* send, void* halo_send, void* stream) {
+  GS_TRY(slab_check(sl, send, halo_send, "gs_slab_begin"));
+  cudaStream_t st = pick_stream(sl->loc, stream);
+  return sl->loc->p.dtype == GS_DTYPE_F64 ? slab_begin<double>(sl, send, halo_send, st)
+                                          : slab_begin<float>(sl, send, halo_send, st);
+}
+
+extern "C" int gs_slab_xpass(gs_slab* sl, const void* recv, void* send, void* stream) {
+  GS_TRY(slab_check(sl, recv, send, "gs_slab_xpass"));
+  cudaStream_t st = pick_stream(sl->loc, stream);
+  return sl->loc->p.dtype == GS_DTYPE_F64 ? slab_xpass<double>(sl, recv, send, st)
+                                          : slab_xpass<float>(sl, recv, send, st);
+}
+
+extern "C" int gs_slab_end(gs_slab* sl, const void* recv, const void* halo_recv, void* stream) {
+  GS_TRY(slab_check(sl, recv, halo_recv, "gs_slab_end"));
+  cudaStream_t st = pick_stream(sl->loc, stream);
+  return sl->loc->p.dtype == GS_DTYPE_F64 ? slab_end<double>(sl, recv, halo_recv, st)
+                                          : slab_end<float>(sl, recv, halo_recv, st);
+}

@@ -6,7 +6,7 @@
 
 namespace gs {
 
-template <typename T, int H, int VM, bool ST, bool BA, bool FU = false>
+template <typename T, int H, int VM, bool ST, bool BA, bool FU = false, bool HA = false>
 cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks, int nsim) {
   using L = Line<T, H>;
   const int per = L::P * a.mc.V;
@@ -19,15 +19,24 @@ cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks, int nsim) {
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;
   const size_t smem = (size_t)lr * a.mc.V * L::PAD * sizeof(cplx<T>);
-  allow_max_smem<k_mart_update<T, H, VM, ST, BA, FU>>();
+  allow_max_smem<k_mart_update<T, H, VM, ST, BA, FU, true, HA>>();
   const long long grid = (a.nrows + lr - 1) / lr;
   if (nblocks) *nblocks = (int)grid;
-  k_mart_update<T, H, VM, ST, BA, FU><<<dim3((unsigned)grid, (unsigned)nsim), (unsigned)(per * lr), smem, s>>>(a);
+  k_mart_update<T, H, VM, ST, BA, FU, true, HA>
+      <<<dim3((unsigned)grid, (unsigned)nsim), (unsigned)(per * lr), smem, s>>>(a);
   return cudaGetLastError();
 }
 
 template <typename T, int H> cudaError_t mu_h(MartArgs<T>& a, bool stats, cudaStream_t s, int* nb, int nsim) {
   const bool fu = a.spec_next != nullptr && !stats;
+  if (a.halo) {  // a slab of a split grid: one simulation, fused z forward, no statistics
+    if (!fu || nsim > 0) return cudaErrorInvalidValue;
+    if constexpr (sizeof(T) == 4) {
+      if (a.mc.V == 3) return mu_n<T, H, 3, false, false, true, true>(a, s, nb, 1);
+    }
+    if (a.mc.V <= 4) return mu_n<T, H, 4, false, false, true, true>(a, s, nb, 1);
+    return mu_n<T, H, 8, false, false, true, true>(a, s, nb, 1);
+  }
   if (nsim > 0) {  // batched simulations (device-resident constants)
     if constexpr (sizeof(T) == 4) {
       if (a.mc.V == 3 && fu) return mu_n<T, H, 3, false, true, true>(a, s, nb, nsim);

@@ -94,7 +94,8 @@ template <int N0, int FM, int TZ> static cudaError_t xtma_n(XArgs<float>& a, cud
 // fields of one FP32 simulation on n0 = 128 or 256 (8-column tiles, so
 // h % 8 == 0); cudaErrorNotSupported sends the caller to the plain pass.
 cudaError_t launch_xtma(XArgs<float>& a, cudaStream_t s) {
-  if (!g_x_prefetch || !a.btab || a.F != a.G || a.nsim > 1 || a.simscale) return cudaErrorNotSupported;
+  if (!g_x_prefetch || !a.btab || a.F != a.G || a.nsim > 1 || a.simscale || a.kz_off || a.hg)
+    return cudaErrorNotSupported;
   if (a.h % 8 != 0 || (reinterpret_cast<uintptr_t>(a.in) & 15) != 0) return cudaErrorNotSupported;
   if (a.F == 3) {
     if (a.n0 == 256) return xtma_n<256, 3, 8>(a, s);

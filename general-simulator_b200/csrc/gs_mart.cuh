@@ -56,6 +56,11 @@ template <typename T> struct MartArgs {
   cplx<T>* spec_next;  // FUSE: packed z spectra of eta'^2 for the next step (may be spec)
   const T* r_in;       // !ZF: R_p in real space [V][N] (a library FFT's output)
   T* sq_out;           // !ZF and FUSE: eta'^2 [V][N] (the next step's FFT input)
+  // HALO (a slab of a simulation split along axis 0): the planes beyond the
+  // slab's faces [2][V][n1][n2] (the neighbour below, then above), and the
+  // global index of the slab's first cell (the noise counter)
+  const T* halo;
+  long long cell_off;
 };
 
 // advance the step counter of every batched simulation (keeps a captured
@@ -144,7 +149,11 @@ template <int VM, bool STATS> struct UpdBlocks {  // resident blocks asked of th
 // ZF = false: the same update without the z transforms, for the cuFFT
 // comparator step -- R_p is read from a.r_in (real space) and, with FUSE,
 // eta'^2 is written to a.sq_out for the library's next forward transform.
-template <typename T, int H, int VM, bool STATS, bool BATCH, bool FUSE = false, bool ZF = true>
+//
+// HALO: the field is a slab of a grid split along axis 0; the x neighbours
+// across its two faces come from a.halo, and the noise counter uses global
+// cell indices.
+template <typename T, int H, int VM, bool STATS, bool BATCH, bool FUSE = false, bool ZF = true, bool HALO = false>
 __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(MartArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
@@ -196,6 +205,10 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     const int oxp = x + 1 == n0 ? -(n0 - 1) * sx : sx, oxm = x == 0 ? (n0 - 1) * sx : -sx;
     const int oyp = y + 1 == n1 ? -(n1 - 1) * n2 : n2, oym = y == 0 ? (n1 - 1) * n2 : -n2;
     const int ozl = (z0 == 0 ? n2 - 1 : z0 - 1) - z0, ozr = (z0 + CW == n2 ? 0 : z0 + CW) - z0;
+    const bool hlo = HALO && x == 0, hhi = HALO && x == n0 - 1;  // neighbour plane from the halo
+    const long long hplane = (long long)n1 * n2;
+    const int yz = cell - x * sx;
+    const long long gcell = HALO ? (long long)cell + a.cell_off : (long long)cell;
     T e[VM][CW];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
@@ -234,14 +247,14 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       for (int j = 0; j < CW; ++j) dfc[j] = (T)1 - dfc[j];
     }
     // a run of 2 (n2 = 2 mod 4) may sit in the upper half of its Philox quad
-    const bool hi_pair = CW == 2 && (cell & 2);
+    const bool hi_pair = CW == 2 && (gcell & 2);
 #pragma unroll
     for (int q = 0; q < VM; ++q) {
       if (q >= Vn) break;
       const T* eq = a.eta_in + q * N + cell;
       T vxp[CW], vxm[CW], vyp[CW], vym[CW];
-      ldv<CW>(eq + oxp, vxp);
-      ldv<CW>(eq + oxm, vxm);
+      ldv<CW>(hhi ? a.halo + ((long long)(Vn + q) * hplane + yz) : eq + oxp, vxp);
+      ldv<CW>(hlo ? a.halo + ((long long)q * hplane + yz) : eq + oxm, vxm);
       ldv<CW>(eq + oyp, vyp);
       ldv<CW>(eq + oym, vym);
       const T el_ = eq[ozl], er_ = eq[ozr];
@@ -259,7 +272,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       if (mc.has_K) ldv<CW>(a.K + q * N + cell, Kq);
       T xi[4] = {0, 0, 0, 0};
       if (!STATS && mc.noise != (T)0)
-        normal_quad<T>((uint32_t)(cell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
+        normal_quad<T>((uint32_t)(gcell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
       const T lq = mc.lin[q];
       const T lqc = lq - lapsum2;
       T out[CW], rv[CW];

@@ -357,6 +357,11 @@ template <typename T> struct XArgs {
   const T* btab;
   int bt_d1, bt_d2, bt_stride;
   int tz_req;  // column tile asked by the autotuner (0 = default)
+  // x-pencil of a slab-decomposed simulation: this array holds the kz slots
+  // kz_off .. kz_off + h - 1 of a spectrum of hg slots (hg = 0: the whole
+  // spectrum, kz_off = 0); the kz = 0 packed columns exist only where
+  // kz_off = 0, and wave vectors use the global slot index
+  int kz_off, hg;
 };
 
 // per-point operations of the x pass
@@ -554,7 +559,9 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
   auto sm = [rg, TZ](int pos) -> V& { return rg[pos * TZ]; };
   const int Fn = EX ? FM : a.F, Gn = EX ? GM : a.G;  // EX: exactly FM inputs and GM outputs
   const bool fw = grp < Fn;
-  const bool special_blk = kz0 == 0 && (n1 == 1 || ky == 0 || ky == HH);
+  const int kzg0 = kz0 + a.kz_off;       // global slot of the tile's first column
+  const int hg = a.hg ? a.hg : h;        // global slot count (Nyquist index of z)
+  const bool special_blk = kzg0 == 0 && (n1 == 1 || ky == 0 || ky == HH);
   const int nn[3] = {a.n0, a.n1, a.n2};
   // with a paired operator one item is kx and N0 - kx (kx <= N0 / 2)
   constexpr bool PAIR = KxPair<Op>::v;
@@ -567,17 +574,17 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
   auto coords = [&](int idx, int& cc, int& kx, int& kyA, int& kzA, int& kyB, int& kzB) {
     cc = idx % TZ;
     kx = idx / TZ;
-    const int kz = kz0 + cc;
+    const int kz = kzg0 + cc;
     kyA = ky; kzA = kz; kyB = 0; kzB = 0;
     if (kz == 0) {
       if (n1 == 1) {
-        kyA = 0; kzA = 0; kyB = 0; kzB = h;
+        kyA = 0; kzA = 0; kyB = 0; kzB = hg;
       } else if (ky == 0) {
         kyA = 0; kzA = 0; kyB = HH; kzB = 0;
       } else if (ky == HH) {
-        kyA = 0; kzA = h; kyB = HH; kzB = h;
+        kyA = 0; kzA = hg; kyB = HH; kzB = hg;
       } else if (ky > HH) {
-        kyA = ky - HH; kzA = h;
+        kyA = ky - HH; kzA = hg;
       }
     }
   };

@@ -113,6 +113,12 @@ class GsStats(C.Structure):
         return d
 
 
+class GsSlabGeometry(C.Structure):
+    _fields_ = [("rank", C.c_int), ("nranks", C.c_int), ("x0", C.c_int), ("nx_local", C.c_int),
+                ("kz0", C.c_int), ("nkz_local", C.c_int), ("a2a_bytes", C.c_size_t), ("halo_bytes", C.c_size_t),
+                ("step", C.c_int64)]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -188,6 +194,15 @@ def lib() -> C.CDLL:
         "gs_sim_take_field": (C.c_int, [vp, C.c_char_p, vp, C.c_char_p]),
         "gs_cores_paint": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, C.c_double, C.c_double,
                                      C.c_double, vp, vp]),
+        "gs_slab_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),
+        "gs_slab_destroy": (C.c_int, [vp]),
+        "gs_slab_info": (C.c_int, [vp, C.POINTER(GsSlabGeometry)]),
+        "gs_slab_set_field": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.c_int]),
+        "gs_slab_get_field": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.c_int]),
+        "gs_slab_set_step": (C.c_int, [vp, C.c_int64]),
+        "gs_slab_begin": (C.c_int, [vp, vp, vp, vp]),
+        "gs_slab_xpass": (C.c_int, [vp, vp, vp, vp]),
+        "gs_slab_end": (C.c_int, [vp, vp, vp, vp]),
         "gs_noise_block": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
                                      vp, vp]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),

@@ -368,6 +368,50 @@ int gs_batch_autotune(gs_batch* b, int reps, void* stream);
 int gs_batch_get_schedule(const gs_batch* b, int group, gs_schedule* sc);
 int64_t gs_batch_launch_count(const gs_batch* b);
 
+/* ---- a simulation split into slabs across devices -------------------------- */
+/* The reference keeps a whole grid on one device (one cuFFT plan over it,
+ * src/dynamics_mart.cu:113-117); a grid too large for one GPU is split here
+ * into R slabs of nx/R x-planes, one per rank (martensite, 3D grids, nx and
+ * nz/2 multiples of R).  A step is three local phases; between them the
+ * caller exchanges buffers it owns (device memory of `a2a_bytes` and
+ * `halo_bytes`, 16-byte aligned):
+ *   gs_slab_begin(send, halo_send): spectra along z and y of this slab,
+ *     packed by destination rank into send = [R][V][nx/R][ny][h/R] complex
+ *     (h = nz/2), and the slab's first and last x-plane into halo_send =
+ *     [2][V][ny][nz];
+ *   all-to-all of send into recv (equal pieces of a2a_bytes / R), and the
+ *   halo: this rank's halo_recv[0] = halo_send[1] of rank - 1, halo_recv[1]
+ *   = halo_send[0] of rank + 1 (periodic);
+ *   gs_slab_xpass(recv, send): the x transforms and the B contraction of this
+ *     rank's kz slots h/R rank .. h/R (rank + 1) - 1, packed back by
+ *     destination x range;
+ *   all-to-all again;
+ *   gs_slab_end(recv, halo_recv): y inverse, the update (its x neighbours
+ *     across the slab faces from halo_recv; the noise counter on global cell
+ *     indices) and the next step's z forward.
+ * The arithmetic of every line, table point and cell is that of gs_sim_step,
+ * so the slabs reproduce a one-device run bit for bit.  Defect and
+ * dislocation-stress fields and statistics are not taken on this path. */
+typedef struct gs_slab gs_slab;
+typedef struct gs_slab_geometry {
+  int rank, nranks;
+  int x0, nx_local;    /* the x-planes this rank owns */
+  int kz0, nkz_local;  /* the kz slots of its x pass */
+  size_t a2a_bytes;    /* bytes of the send and receive buffers (R equal pieces) */
+  size_t halo_bytes;   /* bytes of halo_send and halo_recv */
+  int64_t step;
+} gs_slab_geometry;
+int gs_slab_create(const gs_params* p, int rank, int nranks, gs_slab** out);
+int gs_slab_destroy(gs_slab* sl);
+int gs_slab_info(const gs_slab* sl, gs_slab_geometry* out);
+/* "eta" of this slab: [V][nx/R][ny][nz] host values of dtype */
+int gs_slab_set_field(gs_slab* sl, const char* name, const void* host, size_t count, int dtype);
+int gs_slab_get_field(gs_slab* sl, const char* name, void* host, size_t count, int dtype);
+int gs_slab_set_step(gs_slab* sl, int64_t step);
+int gs_slab_begin(gs_slab* sl, void* send, void* halo_send, void* stream);
+int gs_slab_xpass(gs_slab* sl, const void* recv, void* send, void* stream);
+int gs_slab_end(gs_slab* sl, const void* recv, const void* halo_recv, void* stream);
+
 /* ---- the noise stream ---------------------------------------------------- */
 /* Replaces the reference's cuRAND normal field (Random::NewNormal_device,
  * src/random.cu:79-82), which the step kernels no longer store: they draw
