@@ -523,7 +523,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   ya.n1 = s->n1;
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
-  GS_CU(launch_ypass<T>(ya, s->n1, F, -1, st, s->sched.y_cols), "y forward pass");
+  GS_CU(launch_ypass<T>(ya, s->n1, F, -1, st, s->sched.y_cols, s->sched.y_radix), "y forward pass");
   if (s->n1 > 1) gs_mark(s, st, "y_forward");
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
@@ -543,7 +543,7 @@ static int elastic_chain_g(gs_sim* s, const T* const* src, const int* square, in
   gs_mark(s, st, "x_contraction");
   YArgs<T> yb = ya;
   yb.spec = reinterpret_cast<cplx<T>*>(out_spec);
-  GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st, s->sched.y_cols), "y inverse pass");
+  GS_CU(launch_ypass<T>(yb, s->n1, G, 1, st, s->sched.y_cols, s->sched.y_radix), "y inverse pass");
   if (s->n1 > 1) gs_mark(s, st, "y_inverse");
   s->launches += 1 + (s->n1 > 1 ? 2 : 0);
   return GS_OK;
@@ -822,7 +822,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   ya.n1 = s->n1;
   ya.h = s->h;
   ya.tw = twp<T>(s, 2);
-  GS_CU(launch_ypass<T>(ya, s->n1, F2, -1, st, s->sched.y_cols), "y forward (update fields)");
+  GS_CU(launch_ypass<T>(ya, s->n1, F2, -1, st, s->sched.y_cols, s->sched.y_radix), "y forward (update fields)");
   if (s->n1 > 1) gs_mark(s, st, "y_forward_update_fields");
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
@@ -853,7 +853,7 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   gs_mark(s, st, "x_kspace_update");
   YArgs<T> yo = ya;
   yo.spec = reinterpret_cast<cplx<T>*>(s->spec);
-  GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st, s->sched.y_cols), "y inverse (update fields)");
+  GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st, s->sched.y_cols, s->sched.y_radix), "y inverse (update fields)");
   if (s->n1 > 1) gs_mark(s, st, "y_inverse_update_fields");
   ZinvArgs<T> zi;
   memset(&zi, 0, sizeof(zi));
@@ -1517,6 +1517,14 @@ struct gs_batch {
   cudaStream_t exec_stream = nullptr;
   std::vector<int> exec_cur;  // which field of each pair the graph reads first
   int64_t launches = 0;
+  // the groups are independent: each steps on a branch stream of its own,
+  // forked from and joined to the caller's stream by events (in a captured
+  // graph: parallel branches), so one group's passes fill the GPU while
+  // another's run their last waves
+  bool concurrent = true;
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> joined;
+  cudaEvent_t forked = nullptr;
 };
 
 // ratio r with b = r a for every eigenstrain component (-1 if not proportional)
@@ -1587,7 +1595,7 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   ya.n1 = g->n1;
   ya.h = g->h;
   ya.tw = twp<T>(g, 2);
-  GS_CU(launch_ypass<T>(ya, g->n1, VT, -1, st, g->sched.y_cols), "batch y forward");
+  GS_CU(launch_ypass<T>(ya, g->n1, VT, -1, st, g->sched.y_cols, g->sched.y_radix), "batch y forward");
   XArgs<T> xa;
   memset(&xa, 0, sizeof(xa));
   xa.in = reinterpret_cast<cplx<T>*>(g->spec);
@@ -1605,7 +1613,7 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
   if (g->btab_state == 1) set_btab<T>(g, xa);
   xa.tz_req = g->sched.x_cols;
   GS_CU(launch_xcontract<T>(xa, st), "batch x pass");
-  GS_CU(launch_ypass<T>(ya, g->n1, VT, 1, st, g->sched.y_cols), "batch y inverse");
+  GS_CU(launch_ypass<T>(ya, g->n1, VT, 1, st, g->sched.y_cols, g->sched.y_radix), "batch y inverse");
   MartArgs<T> ma;
   fill_mart_args<T>(g, ma, in, out);
   ma.mcs = reinterpret_cast<MartConst<T>*>(g->d_mcs);
@@ -1627,10 +1635,35 @@ template <typename T> static int batch_group_step(gs_sim* g, cudaStream_t st) {
 }
 
 static int batch_step_once(gs_batch* b, cudaStream_t st) {
-  for (gs_sim* g : b->groups) {
-    int rc = g->p.dtype == GS_DTYPE_F64 ? batch_group_step<double>(g, st) : batch_group_step<float>(g, st);
-    if (rc != GS_OK) return rc;
+  const size_t ng = b->groups.size();
+  if (!b->concurrent || ng < 2) {
+    for (gs_sim* g : b->groups) {
+      int rc = g->p.dtype == GS_DTYPE_F64 ? batch_group_step<double>(g, st) : batch_group_step<float>(g, st);
+      if (rc != GS_OK) return rc;
+    }
+    return GS_OK;
   }
+  if (b->branch.size() != ng) {  // created on the first direct step, never during a capture
+    for (size_t k = b->branch.size(); k < ng; ++k) {
+      cudaStream_t bs;
+      cudaEvent_t ev;
+      GS_CU(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking), "branch stream");
+      GS_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "branch event");
+      b->branch.push_back(bs);
+      b->joined.push_back(ev);
+    }
+    if (!b->forked) GS_CU(cudaEventCreateWithFlags(&b->forked, cudaEventDisableTiming), "fork event");
+  }
+  GS_CU(cudaEventRecord(b->forked, st), "fork");
+  for (size_t k = 0; k < ng; ++k) {
+    gs_sim* g = b->groups[k];
+    GS_CU(cudaStreamWaitEvent(b->branch[k], b->forked, 0), "branch wait");
+    int rc = g->p.dtype == GS_DTYPE_F64 ? batch_group_step<double>(g, b->branch[k])
+                                        : batch_group_step<float>(g, b->branch[k]);
+    if (rc != GS_OK) return rc;
+    GS_CU(cudaEventRecord(b->joined[k], b->branch[k]), "branch done");
+  }
+  for (size_t k = 0; k < ng; ++k) GS_CU(cudaStreamWaitEvent(st, b->joined[k], 0), "join");
   return GS_OK;
 }
 
@@ -1705,12 +1738,25 @@ extern "C" int gs_batch_destroy(gs_batch* b) {
   for (gs_sim* g : b->groups) {
     free_sim(g);  // frees the per-sim constants too
   }
+  for (cudaStream_t bs : b->branch) cudaStreamDestroy(bs);
+  for (cudaEvent_t ev : b->joined) cudaEventDestroy(ev);
+  if (b->forked) cudaEventDestroy(b->forked);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return GS_OK;
 }
 
 extern "C" int gs_batch_groups(const gs_batch* b) { return b ? (int)b->groups.size() : 0; }
+
+extern "C" int gs_batch_set_concurrent(gs_batch* b, int on) {
+  if (!b) return gs_set_error(GS_EINVAL, "gs_batch_set_concurrent: null handle");
+  if (b->concurrent != (on != 0) && b->exec) {  // the captured graph has the other shape
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  b->concurrent = on != 0;
+  return GS_OK;
+}
 extern "C" int64_t gs_batch_launch_count(const gs_batch* b) { return b ? b->launches : 0; }
 
 extern "C" int gs_batch_use_graph(gs_batch* b, int on) {
@@ -2420,6 +2466,18 @@ template <class StepFn> static int tune(gs_sim* s, int reps, cudaStream_t st, St
         }
       }
     }
+    // the radix split of the y lines: the default plan or its alternative
+    // (the rounding differs between plans, within the step's accuracy bar)
+    const int alt = ypass_alt_radix(s->n1);
+    if (alt && rc == GS_OK) {
+      gs_schedule sc = best;
+      sc.y_radix = best.y_radix == alt ? 0 : alt;
+      float ms = 0;
+      if ((rc = time_sched(sc, &ms)) == GS_OK && ms < 0.98f * best_ms) {
+        best = sc;
+        best_ms = ms;
+      }
+    }
   }
   s->trial = false;
   s->spec_ready = false;  // the trial steps left other spectra behind
@@ -2436,6 +2494,9 @@ extern "C" int gs_sim_set_schedule(gs_sim* s, const gs_schedule* sc) {
   sim_graph_reset(s);
   if (sc->z_lines < 0 || sc->y_cols < 0 || sc->x_cols < 0 || sc->update_rows < 0)
     return gs_set_error(GS_EINVAL, "gs_sim_set_schedule: negative tile size");
+  if (sc->y_radix != 0 && sc->y_radix != ypass_alt_radix(s->n1))
+    return gs_set_error(GS_EINVAL, "gs_sim_set_schedule: y radix %d: 0 or %d for lines of %d", sc->y_radix,
+                        ypass_alt_radix(s->n1), s->n1);
   s->sched = *sc;
   return GS_OK;
 }
@@ -3371,7 +3432,7 @@ template <typename T> static int slab_begin(gs_slab* sl, void* send, void* halo_
   ya.n1 = n1;
   ya.h = h;
   ya.tw = twp<T>(l, 2);
-  GS_CU(launch_ypass<T>(ya, n1, V, -1, st, l->sched.y_cols), "slab y forward");
+  GS_CU(launch_ypass<T>(ya, n1, V, -1, st, l->sched.y_cols, l->sched.y_radix), "slab y forward");
   // [V][x][y][kz = r hr + k] -> send [r][V][x][y][k]
   const int d[5] = {R, V, n0r, n1, hr};
   const long long ss[4] = {hr, (long long)n0r * n1 * h, (long long)n1 * h, h};
@@ -3438,7 +3499,7 @@ template <typename T> static int slab_end(gs_slab* sl, const void* recv, const v
   ya.n1 = n1;
   ya.h = h;
   ya.tw = twp<T>(l, 2);
-  GS_CU(launch_ypass<T>(ya, n1, V, 1, st, l->sched.y_cols), "slab y inverse");
+  GS_CU(launch_ypass<T>(ya, n1, V, 1, st, l->sched.y_cols, l->sched.y_radix), "slab y inverse");
   T* in = reinterpret_cast<T*>(l->eta[l->cur]);
   T* out = reinterpret_cast<T*>(l->eta[l->cur ^ 1]);
   MartArgs<T> ma;

@@ -33,17 +33,51 @@ __host__ __device__ constexpr double cos48(int k) {
 }
 __host__ __device__ constexpr double sin48(int k) { return cos48(k - 12); }
 
+// cos(2 pi k / 64), k = 0..16 (the radix-32 and radix-64 register DFTs)
+__host__ __device__ constexpr double c64_tab(int k) {
+  return k == 0   ? 1.0
+         : k == 1 ? 0.9951847266721968862448
+         : k == 2 ? 0.9807852804032304491262
+         : k == 3 ? 0.9569403357322088649357
+         : k == 4 ? 0.9238795325112867561282
+         : k == 5 ? 0.8819212643483550297128
+         : k == 6 ? 0.8314696123025452370788
+         : k == 7 ? 0.7730104533627369608109
+         : k == 8 ? 0.7071067811865475244008
+         : k == 9 ? 0.6343932841636454982151
+         : k == 10 ? 0.5555702330196022247428
+         : k == 11 ? 0.4713967368259976485564
+         : k == 12 ? 0.3826834323650897717285
+         : k == 13 ? 0.2902846772544623676362
+         : k == 14 ? 0.1950903220161282678483
+         : k == 15 ? 0.0980171403295606019942
+                   : 0.0;
+}
+__host__ __device__ constexpr double cos64(int k) {
+  return (k = ((k % 64) + 64) % 64, k = (k > 32 ? 64 - k : k), k <= 16 ? c64_tab(k) : -c64_tab(32 - k));
+}
+__host__ __device__ constexpr double sin64(int k) { return cos64(k - 16); }
+
+// cos and sin of 2 pi m / R for the radices the plans use (R | 48 or R | 64)
+template <int R> __host__ __device__ constexpr double cos_r(int m) {
+  return 48 % R == 0 ? cos48(m * (48 / R)) : cos64(m * (64 / R));
+}
+template <int R> __host__ __device__ constexpr double sin_r(int m) {
+  return 48 % R == 0 ? sin48(m * (48 / R)) : sin64(m * (64 / R));
+}
+
 // a * exp(DIR * 2 pi i m / R), m a compile-time value after unrolling.
 template <int R, int DIR, typename V>
 __device__ __forceinline__ V twmul(V a, int m) {
+  static_assert(48 % R == 0 || 64 % R == 0, "radix without a twiddle table");
   m = ((m % R) + R) % R;
   if (m == 0) return a;
   if (2 * m == R) return mk2(-a.x, -a.y);
   if (4 * m == R) return DIR > 0 ? mk2(-a.y, a.x) : mk2(a.y, -a.x);
   if (4 * m == 3 * R) return DIR > 0 ? mk2(a.y, -a.x) : mk2(-a.y, a.x);
   using T = decltype(a.x);
-  const T c = (T)cos48(m * (48 / R));
-  const T s = (T)(DIR * sin48(m * (48 / R)));
+  const T c = (T)cos_r<R>(m);
+  const T s = (T)(DIR * sin_r<R>(m));
   return mk2(a.x * c - a.y * s, a.x * s + a.y * c);
 }
 
@@ -132,9 +166,11 @@ GS_PLAN(128, 16, 8)
 GS_PLAN(256, 16, 16)
 #undef GS_PLAN
 
-template <typename T, int N> struct Line {
+// Line<T, N>: the default plan of length N; Line<T, N, R1>: another split
+// N = R1 * (N / R1) (the y pass's alternative plans, chosen by the autotuner)
+template <typename T, int N, int R1_ = Plan<N>::R1> struct Line {
   using V = cplx<T>;
-  static constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+  static constexpr int R1 = R1_, R2 = N / R1_;
   static constexpr int P = R2;        // threads per line
   static constexpr int NB = R1 / R2;  // stage-2 butterflies per thread
   static constexpr int PAD = N + N / R1;  // padded shared-memory line length

@@ -2,5 +2,5 @@
 #include "gs_k_zy_impl.cuh"
 namespace gs {
 template cudaError_t launch_zfwd<double>(ZfwdArgs<double>&, int, cudaStream_t, int);
-template cudaError_t launch_ypass<double>(YArgs<double>&, int, int, int, cudaStream_t, int);
+template cudaError_t launch_ypass<double>(YArgs<double>&, int, int, int, cudaStream_t, int, int);
 }  // namespace gs

@@ -37,22 +37,33 @@ template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_
   }
 }
 
-template <typename T, int N1, int DIR> static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s, int cols_req) {
-  using L = Line<T, N1>;
+template <typename T, int N1, int DIR, int R1 = Plan<N1>::R1>
+static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s, int cols_req) {
+  using L = Line<T, N1, R1>;
   // a requested column count (autotuner): a power of two dividing h that the
   // kernel can launch with and whose tile fits the shared-memory opt-in
   if (cols_req > 0 && (cols_req & (cols_req - 1)) == 0 && a.h % cols_req == 0 &&
-      (long long)cols_req * L::P <= max_block_threads<k_ypass<T, N1, DIR>>() &&
+      (long long)cols_req * L::P <= max_block_threads<k_ypass<T, N1, DIR, R1>>() &&
       (size_t)cols_req * L::PAD * sizeof(cplx<T>) <= 200 * 1024)
     a.tz = cols_req;
   const size_t smem = (size_t)a.tz * L::PAD * sizeof(cplx<T>);
-  allow_max_smem<k_ypass<T, N1, DIR>>();
+  allow_max_smem<k_ypass<T, N1, DIR, R1>>();
   dim3 grid(a.h / a.tz, a.n0, F);
-  k_ypass<T, N1, DIR><<<grid, a.tz * L::P, smem, s>>>(a);
+  k_ypass<T, N1, DIR, R1><<<grid, a.tz * L::P, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req) {
+template <typename T, int N1, int DIR>
+static cudaError_t ypass_plan(YArgs<T>& a, int F, cudaStream_t s, int cols_req, int radix) {
+  if constexpr (N1 == 64 || N1 == 128 || N1 == 256) {
+    constexpr int ALT = N1 == 64 ? 16 : 32;
+    if (radix == ALT) return ypass_n<T, N1, DIR, ALT>(a, F, s, cols_req);
+  }
+  return ypass_n<T, N1, DIR>(a, F, s, cols_req);
+}
+
+template <typename T>
+cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req, int radix) {
   if (n1 == 1) return cudaSuccess;
   a.tz = pick_tz(a.h);
   // FP32 columns of 8 on lines of 256: y forward 0.076 against 0.087 ms for 16
@@ -61,7 +72,7 @@ template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int d
   switch (n1) {
 #define GS_C(N_) \
   case N_:       \
-    return dir < 0 ? ypass_n<T, N_, -1>(a, F, s, cols_req) : ypass_n<T, N_, 1>(a, F, s, cols_req);
+    return dir < 0 ? ypass_plan<T, N_, -1>(a, F, s, cols_req, radix) : ypass_plan<T, N_, 1>(a, F, s, cols_req, radix);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:

@@ -25,7 +25,11 @@ int pick_tz(int h);
 // lines_req / cols_req: tile sizes asked by the autotuner (0 = the default
 // choice; values the launch cannot take fall back to it)
 template <typename T> cudaError_t launch_zfwd(ZfwdArgs<T>& a, int H, cudaStream_t s, int lines_req = 0);
-template <typename T> cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req = 0);
+// radix: the first-stage radix of the y lines (0: the default plan;
+// ypass_alt_radix(n1): the alternative split, for lines of 64, 128 and 256)
+template <typename T>
+cudaError_t launch_ypass(YArgs<T>& a, int n1, int F, int dir, cudaStream_t s, int cols_req = 0, int radix = 0);
+inline int ypass_alt_radix(int n1) { return n1 == 256 ? 32 : n1 == 128 ? 32 : n1 == 64 ? 16 : 0; }
 template <typename T> cudaError_t launch_xcontract(XArgs<T>& a, cudaStream_t s);
 // TMA-fed x pass (gs_k_xtma.cu): cudaErrorNotSupported when the case is not
 // covered (the caller then runs the plain pass)

@@ -242,9 +242,11 @@ template <typename T> struct YArgs {
   const cplx<T>* tw;  // w_n1^m
 };
 
-template <typename T, int N1, int DIR>
+// R1: the first-stage radix of the line plan (the default plan, or the
+// alternative split the autotuner may pick)
+template <typename T, int N1, int DIR, int R1 = Plan<N1>::R1>
 __global__ void k_ypass(YArgs<T> a) {
-  using L = Line<T, N1>;
+  using L = Line<T, N1, R1>;
   using V = cplx<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* smb = reinterpret_cast<V*>(smraw);

@@ -47,7 +47,7 @@ struct gs_sim {
   // even in every axis (the contraction is formed on the fly)
   // tile schedule of the passes (0 = each launcher's default); set by the
   // autotuner or the caller
-  gs_schedule sched = {0, 0, 0, 0};
+  gs_schedule sched = {0, 0, 0, 0, 0};
   bool trial = false;  // steps that leave the state as it was (autotuner timing)
   // the martensite update also writes the next step's z spectra (fused z
   // forward); spec_ready says the spectrum buffer holds those of eta[spec_cur]

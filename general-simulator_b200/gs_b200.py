@@ -29,7 +29,8 @@ GS_MAX_V = 8
 
 
 class GsSchedule(C.Structure):
-    _fields_ = [("z_lines", C.c_int), ("y_cols", C.c_int), ("x_cols", C.c_int), ("update_rows", C.c_int)]
+    _fields_ = [("z_lines", C.c_int), ("y_cols", C.c_int), ("x_cols", C.c_int), ("update_rows", C.c_int),
+                ("y_radix", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -158,6 +159,7 @@ def lib() -> C.CDLL:
         "gs_batch_stats": (C.c_int, [vp, C.c_int, S, vp]),
         "gs_batch_use_graph": (C.c_int, [vp, C.c_int]),
         "gs_batch_groups": (C.c_int, [vp]),
+        "gs_batch_set_concurrent": (C.c_int, [vp, C.c_int]),
         "gs_batch_launch_count": (C.c_int64, [vp]),
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
@@ -552,6 +554,9 @@ class Batch:
 
     def groups(self) -> int:
         return int(lib().gs_batch_groups(self.h))
+
+    def set_concurrent(self, on: bool) -> None:
+        check(lib().gs_batch_set_concurrent(self.h, 1 if on else 0), "gs_batch_set_concurrent")
 
     def autotune(self, reps: int = 5, stream: int = 0) -> list:
         check(lib().gs_batch_autotune(self.h, reps, C.c_void_p(stream)), "gs_batch_autotune")

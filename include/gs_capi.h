@@ -242,6 +242,11 @@ int gs_cores_paint(int nx, int ny, int nz, int nvariants, int ncores, const int*
  * does so per group and drops a captured graph so the next step recaptures. */
 typedef struct gs_schedule {
   int z_lines, y_cols, x_cols, update_rows;
+  /* radix split of the y lines: 0 = the default two-stage plan (16 x 16 for
+   * 256, 16 x 8 for 128, 8 x 8 for 64), or the alternative first-stage radix
+   * (32, 32, 16); other lengths have one plan.  The plans round differently,
+   * within the step's accuracy bar. */
+  int y_radix;
 } gs_schedule;
 int gs_sim_set_schedule(gs_sim* s, const gs_schedule* sc);
 int gs_sim_get_schedule(const gs_sim* s, gs_schedule* sc);
@@ -364,6 +369,11 @@ int gs_batch_step(gs_batch* b, int nsteps, void* stream);
 int gs_batch_stats(gs_batch* b, int sim, gs_stats* out, void* stream);
 int gs_batch_use_graph(gs_batch* b, int on);
 int gs_batch_groups(const gs_batch* b);
+/* 1 (default): every shape group steps on a branch stream of its own, forked
+ * from and joined to the caller's stream (parallel branches in the captured
+ * graph), so the groups' passes overlap; 0: one group after the other on the
+ * caller's stream.  The results are the same bits either way. */
+int gs_batch_set_concurrent(gs_batch* b, int on);
 int gs_batch_autotune(gs_batch* b, int reps, void* stream);
 int gs_batch_get_schedule(const gs_batch* b, int group, gs_schedule* sc);
 int64_t gs_batch_launch_count(const gs_batch* b);

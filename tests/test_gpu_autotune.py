@@ -1,8 +1,12 @@
-"""The tile-schedule autotuner: tuning leaves the state untouched, every
-schedule gives the same bits (lines, columns and rows are independent), and
-tuned batches still match their untuned results."""
+"""The schedule autotuner: tuning leaves the state untouched; every tile
+schedule gives the same bits (lines, columns and rows are independent); the
+alternative radix split of the y lines rounds differently but meets the
+oracle's tolerances (FP64 1e-11, FP32 1e-6 per step); tuned batches match
+their untuned results within those tolerances."""
 import numpy as np
 import pytest
+
+from conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -39,9 +43,15 @@ def test_autotune_keeps_state_and_bits(gb, shape):
     eta0 = gb.initial_eta(p, 3, 0.2)
     ref, _ = _run(gb, p, eta0, 3)
     got, chosen = _run(gb, p, eta0, 3, tune=True)
-    assert set(chosen) == {"z_lines", "y_cols", "x_cols", "update_rows"}
+    assert set(chosen) == {"z_lines", "y_cols", "x_cols", "update_rows", "y_radix"}
     assert all(v >= 0 for v in chosen.values())
-    assert np.array_equal(got, ref)
+    # tuning left the state as it was: the same bits as the chosen schedule set directly
+    again, _ = _run(gb, p, eta0, 3, sched=chosen)
+    assert np.array_equal(got, again)
+    if chosen["y_radix"] == 0:
+        assert np.array_equal(got, ref)
+    else:
+        assert rel_l2(got, ref) < 3e-6
 
 
 @pytest.mark.parametrize("sched", [dict(z_lines=1, y_cols=1, x_cols=1, update_rows=1),
@@ -75,8 +85,33 @@ def test_batch_autotune_matches_untuned(gb):
     ref, _ = run(False)
     got, scheds = run(True)
     assert len(scheds) == 4
-    for a, r in zip(got, ref):
-        assert np.array_equal(a, r)
+    for a, r, sc in zip(got, ref, [None] * len(ref)):
+        assert rel_l2(a, r) < 6e-6  # six FP32 steps; bit-equal unless a group chose the other y radix
+    if all(sc["y_radix"] == 0 for sc in scheds):
+        for a, r in zip(got, ref):
+            assert np.array_equal(a, r)
+
+
+@pytest.mark.parametrize("shape", [(8, 64, 16), (4, 128, 32), (2, 256, 8), (16, 256, 64)])
+@pytest.mark.parametrize("dtype,tol", [(F64, 1e-11), (F32, 1e-6)])
+def test_alternative_y_radix_matches_oracle(gb, orc, shape, dtype, tol):
+    p = _params(gb, shape, dtype=dtype)
+    eta0 = gb.initial_eta(p, 5, 0.4)
+    if dtype == F32:
+        eta0 = eta0.astype(np.float32).astype(np.float64)
+    alt = {64: 16, 128: 32, 256: 32}[shape[1]]
+    got, _ = _run(gb, p, eta0, 1, sched=dict(y_radix=alt))
+    assert rel_l2(got, orc.mart_run(p, eta0, 1)) < tol
+
+
+def test_bad_y_radix_rejected(gb):
+    p = _params(gb, (8, 64, 16))
+    s = gb.Sim(p)
+    try:
+        with pytest.raises(RuntimeError):
+            s.set_schedule(y_radix=8)
+    finally:
+        s.close()
 
 
 def test_precipitate_autotune_keeps_state_and_bits(gb):

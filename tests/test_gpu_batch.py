@@ -54,11 +54,14 @@ def test_batch_fp64_each_sim_matches_oracle(gb, orc):
 
 @pytest.mark.parametrize("dtype", [F32, F64])
 def test_batch_graph_replay_matches_direct(gb, dtype):
+    """Direct launches, graph replay, groups on concurrent branches or one
+    after another: the same bits."""
     ps = mixed_params(gb, dtype)
     etas = [gb.initial_eta(p, 40 + i, 0.4) for i, p in enumerate(ps)]
     outs = []
-    for graph in (False, True):
+    for graph, conc in ((False, False), (True, True), (False, True), (True, False)):
         b = gb.Batch(ps)
+        b.set_concurrent(conc)
         b.use_graph(graph)
         for i, e in enumerate(etas):
             b.set_eta(i, e)
@@ -66,8 +69,9 @@ def test_batch_graph_replay_matches_direct(gb, dtype):
         b.step(4)
         outs.append([b.eta(i) for i in range(len(ps))])
         b.close()
-    for a, c in zip(*outs):
-        assert np.array_equal(a, c)
+    for other in outs[1:]:
+        for a, c in zip(outs[0], other):
+            assert np.array_equal(a, c)
 
 
 def test_ensemble_builder_shapes(gb):
