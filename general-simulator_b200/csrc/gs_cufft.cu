@@ -86,12 +86,11 @@ template <typename T> cudaError_t launch_contract(XArgs<T>& a, cplx<T>* spec, lo
 // about 256 threads (one run of CW cells each), no shared memory
 template <typename T, int H, int VM> cudaError_t upd_n(MartArgs<T>& a, cudaStream_t st) {
   constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
-  constexpr int maxt = UpdBlocks<VM, false>::threads;  // the kernel's launch bound
   const int upr = a.n2 / CW;
-  long long lr = upr >= maxt ? 1 : maxt / upr;
+  long long lr = upr >= 256 ? 1 : 256 / upr;
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;
-  const int threads = (int)(lr * upr < maxt ? lr * upr : maxt);
+  const int threads = (int)(lr * upr < 256 ? lr * upr : 256);
   const long long grid = (a.nrows + lr - 1) / lr;
   k_mart_update<T, H, VM, false, false, true, false><<<dim3((unsigned)grid, 1), (unsigned)threads, 0, st>>>(a);
   return cudaGetLastError();

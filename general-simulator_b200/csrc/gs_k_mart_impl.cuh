@@ -13,10 +13,8 @@ cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks, int nsim) {
   // default: blocks of about 192 threads (8 rows of 3 variants of length-128
   // lines measured 0.300 ms against 0.322 ms for 10 rows at 256^3 x 3); the
   // kernel's launch bounds allow 256 threads
-  constexpr int maxt = UpdBlocks<VM, ST>::threads;  // the kernel's launch bound
   long long lr = 192 / per;
-  if (a.lr_req > 0 && (long long)a.lr_req * per <= maxt) lr = a.lr_req;
-  if (lr * per > maxt) lr = maxt / per;
+  if (a.lr_req > 0 && (long long)a.lr_req * per <= 256) lr = a.lr_req;
   if (lr < 1) lr = 1;
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;

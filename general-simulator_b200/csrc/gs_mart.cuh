@@ -137,10 +137,7 @@ template <int CW> __device__ __forceinline__ void stv(double* p, const double (&
 // centre values, the Landau coupling sums and the defect mask are loaded and
 // formed once per run, and one Philox block per variant serves the run.
 template <int VM, bool STATS> struct UpdBlocks {  // resident blocks asked of the register allocator
-  // exactly three variants: blocks of at most 192 threads (8 rows of 3
-  // length-128 lines), five of them per SM
-  static constexpr int threads = (VM == 3 && !STATS) ? 192 : 256;
-  static constexpr int v = (VM == 3 && !STATS) ? 5 : (VM <= 4 && !STATS) ? 3 : 1;
+  static constexpr int v = (VM <= 4 && !STATS) ? 3 : 1;
 };
 
 // FUSE: the next step's z forward runs here too.  Each thread overwrites the
@@ -157,8 +154,7 @@ template <int VM, bool STATS> struct UpdBlocks {  // resident blocks asked of th
 // across its two faces come from a.halo, and the noise counter uses global
 // cell indices.
 template <typename T, int H, int VM, bool STATS, bool BATCH, bool FUSE = false, bool ZF = true, bool HALO = false>
-__global__ void __launch_bounds__(UpdBlocks<VM, STATS>::threads, UpdBlocks<VM, STATS>::v)
-    k_mart_update(MartArgs<T> a) {
+__global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(MartArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
   constexpr int CW = (2 * H) % 4 == 0 ? 4 : 2;
