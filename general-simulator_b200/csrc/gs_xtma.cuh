@@ -19,53 +19,13 @@
 #pragma once
 #include <cuda.h>
 
+#include "gs_bulk.cuh"
 #include "gs_passes.cuh"
 
 namespace gs {
 
 // waits that gave up (device counter; this header belongs to one translation unit)
 static __device__ unsigned int g_x_wait_timeouts = 0;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n"
-      "  .reg .pred p;\n"
-      "  mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      "  selp.u32 %0, 1, 0, p;\n"
-      "}\n"
-      : "=r"(done)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Wait for phase `parity` of bar to complete; false after ~2^31 cycles (about
-// a second at the B200's clocks).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1LL << 31)) return false;
-  }
-  return true;
-}
 
 // One 4D tiled box (coordinates innermost first) into shared memory; the
 // bytes are counted on bar.
