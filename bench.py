@@ -467,6 +467,37 @@ def extra_precip_adjoint(n: int = 256, steps: int = 100, K: int = 10) -> dict:
             "note": "backward includes recomputing every segment but the last from its checkpoint"}
 
 
+def extra_slab(n: int = 256, nranks: int = 2, steps: int = 20) -> dict:
+    """The slab-decomposed step on one GPU: nranks slabs of the headline grid
+    in one process, the transposes and halos as device copies (the exchange
+    a multi-GPU run does over NVLink), device time per step against the
+    one-device step.  Measures the decomposition's own cost (packing, the
+    x-pencil passes on kz sub-ranges); the cross-GPU exchange itself is not
+    measured here (one GPU)."""
+    import torch
+
+    import gs_b200 as gb
+    import gs_slab
+
+    p = gb.mart3d_params(n, dtype=gb.GS_DTYPE_F32, noise=1e-3)
+    eta0 = gb.initial_eta(p, 1).astype(np.float32)
+    slabs = [gs_slab.Slab(p, r, nranks) for r in range(nranks)]
+    try:
+        for r, sl in enumerate(slabs):
+            sl.set_eta(eta0[:, sl.plan.x_range(r)])
+        stream = torch.cuda.current_stream()
+        gs_slab.step_local(slabs, 3)
+        ms = min(_timed(stream, lambda: gs_slab.step_local(slabs, steps)) for _ in range(2)) / steps
+        xfer = 2 * sum(int(sl.geom.a2a_bytes) for sl in slabs) + sum(int(sl.geom.halo_bytes) for sl in slabs)
+    finally:
+        for sl in slabs:
+            sl.close()
+    return {"workload": f"{n}^3, 3 variants, FP32, noise 1e-3, {nranks} x-slabs on one GPU",
+            "ms_per_step": ms, "exchange_bytes_per_step": xfer,
+            "note": "all-to-all and halo exchanges as device copies on the same GPU; a multi-GPU run replaces "
+                    "them with NCCL collectives (unmeasured on hardware: one GPU in this run)"}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: the FP64 oracle on the host cores
 # ---------------------------------------------------------------------------
@@ -691,6 +722,7 @@ def run_ours(args, ws, rank, local):
         extras["ensemble"] = extra_ensemble()
         extras["other_workloads"] = extra_configs()
         extras["precip_adjoint"] = extra_precip_adjoint()
+        extras["slab"] = extra_slab(n)
     cpu = None
     if ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(n, args.cpu_seconds)
