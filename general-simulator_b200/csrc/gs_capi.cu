@@ -741,7 +741,9 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   la.k1 = (uint32_t)(p.seed >> 32);
   la.sim = p.sim_id;
   la.step = (uint32_t)s->step;
-  const int F2 = 2 * V + 2, G2 = V + 1;
+  la.fold = 1;  // the sweeps form u_p = eta_p - dt L g_p (see k_precip_mid)
+  la.dtL = (T)(p.dt * p.mobility_eta);
+  const int F2 = V + 2, G2 = V + 1;
   const long long rows = (long long)s->n0 * s->n1;
   // chain 1 to its y inverse, then one sweep: z C2R of R, local terms, z R2C
   // of the update fields (k_precip_mid); rows too wide for one block take the
@@ -758,7 +760,10 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
       src[V] = c;
       sq[V] = 0;
     }
-    GS_TRY(elastic_chain_g<T>(s, src, sq, F1, 2, 1.0 / (double)N, s->spec, F1, st));
+    // the previous step's fused z inverse may have left the z spectra of
+    // [eta_p^2, c] in the spectrum buffer
+    const bool z_ready = s->spec_ready && s->spec_cur == 0;
+    GS_TRY(elastic_chain_g<T>(s, src, sq, F1, 2, 1.0 / (double)N, s->spec, F1, st, nullptr, z_ready));
     PrecipMidArgs<T> pm;
     memset(&pm, 0, sizeof(pm));
     pm.rspec = reinterpret_cast<const cplx<T>*>(s->spec);
@@ -797,15 +802,13 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
     gs_mark(s, st, "precip_local");
     s->launches += 2;
   }
-  // chain 2: [c, mu, eta_0, g_0, eta_1, g_1, ...] -> k-space update -> [c', eta']
+  // chain 2: [c, mu, u_0, u_1, ...] -> k-space update -> [c', eta'] (u_p
+  // formed by the local terms in place of g_p)
   ZfwdArgs<T> za;
   memset(&za, 0, sizeof(za));
   za.src[0] = c;
   za.src[1] = mu;
-  for (int v = 0; v < V; ++v) {
-    za.src[2 + 2 * v] = eta + (long long)v * N;
-    za.src[3 + 2 * v] = g + (long long)v * N;
-  }
+  for (int v = 0; v < V; ++v) za.src[2 + v] = g + (long long)v * N;
   za.dst = reinterpret_cast<cplx<T>*>(s->spec2);
   za.rows_per_field = rows;
   za.nrows = rows * F2;
@@ -832,13 +835,12 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   xa.n1 = s->n1;
   xa.n2 = s->n2;
   xa.h = s->h;
-  // one (field, force) pair per grid-z slice, written to the chain-1
-  // spectrum buffer (free by now): a slice's output rows overlap another
-  // slice's input rows, so the update is not done in place
+  // the (c, mu) pair -> c', then one u_p per grid-z slice -> eta_p', written
+  // to the chain-1 spectrum buffer (free by now), not in place
   xa.out = reinterpret_cast<cplx<T>*>(s->spec);
   xa.F = 2;
   xa.G = 1;
-  xa.nsim = G2;
+  xa.nsim = 1;
   xa.tz_req = s->sched.x_cols;
   xa.tw = twp<T>(s, 3);
   xa.pu.V = V;
@@ -849,26 +851,59 @@ template <typename T> static int precip_step(gs_sim* s, cudaStream_t st) {
   xa.pu.ke = (T)p.kappa_eta;
   xa.pu.scale = (T)(1.0 / (double)N);
   for (int c3 = 0; c3 < 3; ++c3) xa.pu.ktab[c3] = reinterpret_cast<const T*>(s->ktab) + s->ktab_off[c3];
-  GS_CU(launch_xprecip<T>(xa, st), "x pass (k-space update)");
+  GS_CU(launch_xprecip<T>(xa, st), "x pass (k-space update of c)");
+  {
+    const long long fs = (long long)s->n0 * s->n1 * s->h;  // complex values per field
+    XArgs<T> xe = xa;
+    xe.in = reinterpret_cast<cplx<T>*>(s->spec2) + 2 * fs;
+    xe.out = reinterpret_cast<cplx<T>*>(s->spec) + fs;
+    xe.F = 1;
+    xe.G = 1;
+    xe.nsim = V;
+    GS_CU(launch_xprecip_eta<T>(xe, st), "x pass (k-space update of eta)");
+  }
   gs_mark(s, st, "x_kspace_update");
   YArgs<T> yo = ya;
   yo.spec = reinterpret_cast<cplx<T>*>(s->spec);
   GS_CU(launch_ypass<T>(yo, s->n1, G2, 1, st, s->sched.y_cols, s->sched.y_radix), "y inverse (update fields)");
   if (s->n1 > 1) gs_mark(s, st, "y_inverse_update_fields");
-  ZinvArgs<T> zi;
-  memset(&zi, 0, sizeof(zi));
-  zi.spec = reinterpret_cast<const cplx<T>*>(s->spec);
-  zi.dst[0] = c;
-  for (int v = 0; v < V; ++v) zi.dst[1 + v] = eta + (long long)v * N;
-  zi.rows_per_field = rows;
-  zi.nrows = rows * G2;
-  zi.tw_h = twp<T>(s, 1);
-  zi.tw_n2 = twp<T>(s, 0);
-  zi.offset_field = p.mass_projection ? 0 : -1;
-  zi.offset = s->mass0 / (double)N;
-  GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (c, eta)");
-  gs_mark(s, st, "z_inverse_c_eta");
-  s->launches += 2 + (s->n1 > 1 ? 2 : 0);
+  // z inverse of [c', eta'] fused with the next step's chain-1 z forward
+  // (rows whose lines exceed one block take the plain z inverse)
+  PrecipZArgs<T> pz;
+  memset(&pz, 0, sizeof(pz));
+  pz.spec = reinterpret_cast<cplx<T>*>(s->spec);
+  pz.c = c;
+  pz.eta = eta;
+  pz.nrows = rows;
+  pz.N = N;
+  pz.V = V;
+  pz.F1 = F1;
+  pz.mass = p.mass_projection;
+  pz.offset = s->mass0 / (double)N;
+  pz.tw_h = twp<T>(s, 1);
+  pz.tw_n2 = twp<T>(s, 0);
+  const cudaError_t ez = launch_precip_zinv_fwd<T>(pz, s->h, st);
+  if (ez == cudaSuccess) {
+    gs_mark(s, st, "z_inverse_c_eta_next_z_forward");
+    s->spec_ready = true;  // the next step skips its z forward
+    s->spec_cur = 0;
+  } else {
+    if (ez != cudaErrorInvalidConfiguration) GS_CU(ez, "z inverse (c, eta) + next z forward");
+    ZinvArgs<T> zi;
+    memset(&zi, 0, sizeof(zi));
+    zi.spec = reinterpret_cast<const cplx<T>*>(s->spec);
+    zi.dst[0] = c;
+    for (int v = 0; v < V; ++v) zi.dst[1 + v] = eta + (long long)v * N;
+    zi.rows_per_field = rows;
+    zi.nrows = rows * G2;
+    zi.tw_h = twp<T>(s, 1);
+    zi.tw_n2 = twp<T>(s, 0);
+    zi.offset_field = p.mass_projection ? 0 : -1;
+    zi.offset = s->mass0 / (double)N;
+    GS_CU(launch_zinv<T>(zi, s->h, st), "z inverse (c, eta)");
+    gs_mark(s, st, "z_inverse_c_eta");
+  }
+  s->launches += 3 + (s->n1 > 1 ? 2 : 0);
   s->step += 1;
   return GS_OK;
 }
@@ -2729,6 +2764,7 @@ static int padj_save(gs_padjoint* a, void* dst, cudaStream_t st) {
 static int padj_load(gs_padjoint* a, const void* src, cudaStream_t st) {
   gs_sim* s = a->s;
   const size_t fb = (size_t)s->N * elt(s);
+  s->spec_ready = false;  // the spectra left by the last step are not this state's
   GS_CU(cudaMemcpyAsync(s->conc, src, fb, cudaMemcpyDeviceToDevice, st), "restore state");
   GS_CU(cudaMemcpyAsync(s->eta[0], static_cast<const char*>(src) + fb, fb * s->p.nvariants, cudaMemcpyDeviceToDevice,
                         st),

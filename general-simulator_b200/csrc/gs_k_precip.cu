@@ -39,7 +39,7 @@ static unsigned grid_for(long long n, int block) {
 
 template <typename T, int H, int VM> static cudaError_t pmid_n(PrecipMidArgs<T>& a, cudaStream_t s) {
   using L = Line<T, H>;
-  const int per = L::P * (2 * a.loc.V + 2);  // threads of one row
+  const int per = L::P * (a.loc.V + 2);  // threads of one row
   if (per > 256) return cudaErrorInvalidConfiguration;
   long long lr = 256 / per;
   if (a.lr_req > 0 && (long long)a.lr_req * per <= 256) lr = a.lr_req;
@@ -47,7 +47,7 @@ template <typename T, int H, int VM> static cudaError_t pmid_n(PrecipMidArgs<T>&
   a.lr = (int)lr;
   const int CW = (2 * H) % 4 == 0 ? 4 : 2;
   a.fd_upr = FastDiv((uint32_t)(a.n2 / CW));
-  const size_t smem = (size_t)lr * (2 * a.loc.V + 2) * L::PAD * sizeof(cplx<T>);
+  const size_t smem = (size_t)lr * (a.loc.V + 2) * L::PAD * sizeof(cplx<T>);
   allow_max_smem<k_precip_mid<T, H, VM>>();
   const long long grid = (a.nrows + lr - 1) / lr;
   k_precip_mid<T, H, VM><<<(unsigned)grid, (unsigned)(per * lr), smem, s>>>(a);
@@ -59,6 +59,32 @@ template <typename T> cudaError_t launch_precip_mid(PrecipMidArgs<T>& a, int H, 
 #define GS_C(N_) \
   case N_:       \
     return a.loc.V <= 4 ? pmid_n<T, N_, 4>(a, s) : pmid_n<T, N_, 8>(a, s);
+    GS_SIZE_CASES(GS_C)
+#undef GS_C
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int H> static cudaError_t pzf_n(PrecipZArgs<T>& a, cudaStream_t s) {
+  using L = Line<T, H>;
+  const int per = L::P * (a.V + 1);  // threads of one row
+  if (per > 256) return cudaErrorInvalidConfiguration;
+  long long lr = 256 / per;
+  if (lr > a.nrows) lr = a.nrows;
+  a.lr = (int)lr;
+  const size_t smem = (size_t)lr * (a.V + 1) * L::PAD * sizeof(cplx<T>);
+  allow_max_smem<k_precip_zinv_fwd<T, H>>();
+  const long long grid = (a.nrows + lr - 1) / lr;
+  k_precip_zinv_fwd<T, H><<<(unsigned)grid, (unsigned)(per * lr), smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_precip_zinv_fwd(PrecipZArgs<T>& a, int H, cudaStream_t s) {
+  switch (H) {
+#define GS_C(N_) \
+  case N_:       \
+    return pzf_n<T, N_>(a, s);
     GS_SIZE_CASES(GS_C)
 #undef GS_C
     default:
@@ -87,6 +113,7 @@ template <typename T> cudaError_t launch_precip_stats(PrecipStatsArgs<T>& a, cud
   template cudaError_t launch_zinv<T>(ZinvArgs<T>&, int, cudaStream_t);                    \
   template cudaError_t launch_precip_local<T>(PrecipLocalArgs<T>&, cudaStream_t);          \
   template cudaError_t launch_precip_mid<T>(PrecipMidArgs<T>&, int, cudaStream_t);          \
+  template cudaError_t launch_precip_zinv_fwd<T>(PrecipZArgs<T>&, int, cudaStream_t);       \
   template cudaError_t launch_defect<T>(const T*, T*, long long, int, cudaStream_t);       \
   template cudaError_t launch_precip_stats<T>(PrecipStatsArgs<T>&, cudaStream_t, int*);
 GS_INST(float)

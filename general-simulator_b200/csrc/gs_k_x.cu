@@ -30,8 +30,15 @@ template <typename T> cudaError_t launch_xprecip_adjoint(XArgs<T>& a, cudaStream
 template cudaError_t launch_xprecip_adjoint<float>(XArgs<float>&, cudaStream_t);
 template cudaError_t launch_xprecip_adjoint<double>(XArgs<double>&, cudaStream_t);
 
+template <typename T> cudaError_t launch_xprecip_eta(XArgs<T>& a, cudaStream_t s) {
+  if (a.F != 1 || a.G != 1) return cudaErrorInvalidValue;
+  return launch_x_class<T, 1, 1, PrecipEtaOp>(a, s);
+}
+template cudaError_t launch_xprecip_eta<float>(XArgs<float>&, cudaStream_t);
+template cudaError_t launch_xprecip_eta<double>(XArgs<double>&, cudaStream_t);
+
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s) {
-  if (a.F == 2 && a.G == 1 && a.nsim > 1) return launch_x_class<T, 2, 1, PrecipPairOp>(a, s);  // pair slices
+  if (a.F == 2 && a.G == 1 && a.nsim >= 1) return launch_x_class<T, 2, 1, PrecipPairOp>(a, s);  // pair slices
   if (a.F <= 10 && a.G <= 5) return launch_x_class<T, 10, 5, PrecipOp>(a, s);
   return launch_x_class<T, 18, 9, PrecipOp>(a, s);
 }

@@ -30,7 +30,8 @@ template <typename T, int N0, int FM, int GM, class Op> static cudaError_t xc_n(
     if (tz == 8) {
       // exact field counts known at compile time: the three- and five-field
       // table contractions, the precipitate's (state, force) -> state slices
-      if constexpr ((FM == GM && (FM == 3 || FM == 5) && KxPair<Op>::v) || (FM == 2 && GM == 1)) {
+      if constexpr ((FM == GM && (FM == 3 || FM == 5) && KxPair<Op>::v) || (FM == 2 && GM == 1) ||
+                    (FM == 1 && GM == 1)) {
         if (a.F == FM && a.G == GM) {
           allow_max_smem<k_xpass<T, N0, FM, GM, 8, Op, true>>();
           k_xpass<T, N0, FM, GM, 8, Op, true><<<grid, tz * L::P * groups, smem, s>>>(a);

@@ -38,6 +38,8 @@ void set_x_prefetch(bool on);
 bool x_prefetch();
 unsigned int x_wait_timeouts();
 template <typename T> cudaError_t launch_xprecip(XArgs<T>& a, cudaStream_t s);
+// eta_p' = D u_p, one field per grid-z slice (F = G = 1)
+template <typename T> cudaError_t launch_xprecip_eta(XArgs<T>& a, cudaStream_t s);
 // the transposed precipitate update (F = 2, G = 3 per grid-z slice)
 template <typename T> cudaError_t launch_xprecip_adjoint(XArgs<T>& a, cudaStream_t s);
 // field-count class (3, 5 or 9) of the B octant table of V variants
@@ -52,6 +54,9 @@ cudaError_t launch_btab_fill(const ElasticConst<T>& ec, int n0, int n1, int n2, 
 template <typename T> cudaError_t launch_zinv(ZinvArgs<T>& a, int H, cudaStream_t s);
 template <typename T> cudaError_t launch_precip_local(PrecipLocalArgs<T>& a, cudaStream_t s);
 template <typename T> struct PrecipMidArgs;
+template <typename T> struct PrecipZArgs;
+// returns cudaErrorInvalidConfiguration when a row's lines exceed one block
+template <typename T> cudaError_t launch_precip_zinv_fwd(PrecipZArgs<T>& a, int H, cudaStream_t s);
 // returns cudaErrorInvalidConfiguration when a row's lines exceed one block
 template <typename T> cudaError_t launch_precip_mid(PrecipMidArgs<T>& a, int H, cudaStream_t s);
 template <typename T> cudaError_t launch_defect(const T* eta, T* defect, long long N, int V, cudaStream_t s);

@@ -396,12 +396,26 @@ struct TableOp {
     mx = mx < 0 ? -mx : mx;
     my = my < 0 ? -my : my;
     mz = mz < 0 ? -mz : mz;
-    const cplx<T>* b2 = reinterpret_cast<const cplx<T>*>(a.btab + (((long long)mx * a.bt_d1 + my) * a.bt_d2 + mz) * S);
+    const T* pt = a.btab + (((long long)mx * a.bt_d1 + my) * a.bt_d2 + mz) * S;
+    if constexpr (sizeof(T) == 4 && S % 4 == 0) {
+      const float4* b4 = reinterpret_cast<const float4*>(pt);
 #pragma unroll
-    for (int i = 0; i < S / 2; ++i) {
-      const cplx<T> w = __ldg(b2 + i);
-      bv[2 * i] = w.x;
-      bv[2 * i + 1] = w.y;
+      for (int i = 0; i < S / 4; ++i) {
+        const float4 w = __ldg(b4 + i);
+        bv[4 * i] = w.x;
+        bv[4 * i + 1] = w.y;
+        bv[4 * i + 2] = w.z;
+        bv[4 * i + 3] = w.w;
+      }
+    } else {
+      const cplx<T>* b2 = reinterpret_cast<const cplx<T>*>(pt);
+      const uint64_t keep = l2_evict_last();  // the table is read again for the other ky, kz signs
+#pragma unroll
+      for (int i = 0; i < S / 2; ++i) {
+        const cplx<T> w = ld_hint(b2 + i, keep);
+        bv[2 * i] = w.x;
+        bv[2 * i + 1] = w.y;
+      }
     }
   }
   template <typename T, int FM, int GM, bool EX = false>
@@ -506,6 +520,21 @@ struct PrecipPairOp {
       const T ie = u.scale / ((T)1 + u.dtL * u.ke * K);
       out[0] = (in[0] - in[1] * u.dtL) * ie;
     }
+  }
+};
+
+// The Allen-Cahn half of the same update when the real-space sweep already
+// formed u_p = eta_p - dt L g_p: one field per grid-z slice, eta_p' = D u_p
+// with D = 1/(1 + dt L kappa_eta K).
+struct PrecipEtaOp {
+  template <typename T, int FM, int GM>
+  __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
+                                               const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
+    const PrecipUpd<T>& u = a.pu;
+    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+#pragma unroll
+    for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
+    out[0] = in[0] * (u.scale / ((T)1 + u.dtL * u.ke * K));
   }
 };
 
@@ -734,8 +763,9 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const bool fw = grp < a.F;
   {
     const V* src = in_base + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
+    const uint64_t stream = l2_evict_first();  // read once: leave L2 to the B table
 #pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
+    for (int r = 0; r < L::R1; ++r) v[r] = fw ? ld_hint(src + (long long)r * (L::P * rstride), stream) : mk2((T)0, (T)0);
   }
   xpass_tile<T, N0, FM, GM, Op, true, EX>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v, tws);
 }

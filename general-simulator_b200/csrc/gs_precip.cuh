@@ -21,6 +21,10 @@ template <typename T> struct PrecipLocalArgs {
   int V, c_elastic;
   T A[8], c1, c2, Es, an;  // coefficients, Xi * w_el, noise amplitude
   uint32_t k0, k1, sim, step;
+  // fold = 1: g holds u_p = eta_p - dt L g_p (the only combination of eta_p
+  // and g_p the semi-implicit update transforms: FFT is linear)
+  int fold;
+  T dtL;
 };
 
 // mu_c at one cell (s1 = sum_p eta_p^2; rc = R of c when c couples)
@@ -76,7 +80,9 @@ __global__ void k_precip_local(PrecipLocalArgs<T> a) {
             t2 += e * e;
             t4 += e * e * e * e;
           }
-        a.g[p * a.N + i] = precip_g(a, c, a.eta[p * a.N + i], t2, t4, a.R[p * a.N + i], zp[j]);
+        const T x = a.eta[p * a.N + i];
+        const T gv = precip_g(a, c, x, t2, t4, a.R[p * a.N + i], zp[j]);
+        a.g[p * a.N + i] = a.fold ? x - a.dtL * gv : gv;
       }
     }
   }
@@ -84,17 +90,20 @@ __global__ void k_precip_local(PrecipLocalArgs<T> a) {
 
 // The middle of the precipitate step in one sweep over rows: the z C2R of
 // the elastic potentials R (chain 1 after its y inverse), the local terms
-// mu_c and g_p, and the z R2C of the update fields [c, mu, eta_0, g_0, ...]
-// (chain 2).  Shared memory holds, per row, one line per update field in
-// chain-2 order: c and eta_p are loaded into their lines, R_c and R_p are
-// transformed into the lines of mu and g_p, each thread overwrites the R of
-// its own cells with mu and g_p, and every line is transformed to the
-// chain-2 spectrum rows.  R, mu and g never go to HBM.
+// mu_c and g_p, and the z R2C of the update fields [c, mu, u_0, .., u_V-1]
+// (chain 2), u_p = eta_p - dt L g_p: the Allen-Cahn update
+// eta_p' = D (FFT(eta_p) - dt L FFT(g_p)) needs only that combination, which
+// FFT linearity lets the sweep form in real space (V + 2 transformed fields
+// instead of 2V + 2).  Shared memory holds, per row, one line per update
+// field in chain-2 order: c is loaded into its line, R_c and R_p are
+// transformed into the lines of mu and u_p, each thread overwrites the R of
+// its own cells with mu and u_p, and every line is transformed to the
+// chain-2 spectrum rows.  R, mu, g and u never go to HBM.
 template <typename T> struct PrecipMidArgs {
   const cplx<T>* rspec;  // [F1][rows][H]: R_eta_p^2 (p < V), then R_c
   const T* c;            // [N]
   const T* eta;          // [V][N]
-  cplx<T>* dst;          // [2V+2][rows][H]
+  cplx<T>* dst;          // [V+2][rows][H]
   int lr_req;            // rows per block asked by the schedule (0: the launcher's choice)
   long long nrows;
   int n2, lr, F1;
@@ -115,7 +124,7 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   V* smb = reinterpret_cast<V*>(smraw);
   const int Vn = a.loc.V;
-  const int NL = 2 * Vn + 2;  // lines per row
+  const int NL = Vn + 2;  // lines per row
   const int n2 = a.n2;
   const long long N = a.nrows * n2;
   const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
@@ -123,9 +132,9 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
   const long long row = (long long)blockIdx.x * a.lr + rr;
   const bool rok = rr < a.lr && row < a.nrows;
   V* sl = smb + line * L::PAD;
-  // R field feeding this line: g_p lines take R_p, the mu line R_c
+  // R field feeding this line: u_p lines take R_p, the mu line R_c
   int rf = -1;
-  if (f2 >= 3 && (f2 & 1)) rf = (f2 - 3) >> 1;
+  if (f2 >= 2) rf = f2 - 2;
   if (f2 == 1 && a.loc.c_elastic && a.F1 > Vn) rf = Vn;
   {
     const bool act = rok && rf >= 0;
@@ -136,9 +145,8 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
     if (rf >= 0) {
 #pragma unroll
       for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = r[i];
-    } else if (rok && (f2 == 0 || f2 >= 2)) {  // c or eta_p: the row itself
-      const T* src = f2 == 0 ? a.c : a.eta + (long long)((f2 - 2) >> 1) * N;
-      const V* srow = reinterpret_cast<const V*>(src + row * n2);
+    } else if (rok && f2 == 0) {  // c: the row itself
+      const V* srow = reinterpret_cast<const V*>(a.c + row * n2);
 #pragma unroll
       for (int i = 0; i < L::R1; ++i) sl[L::in_pos(t, i)] = srow[L::in_pos(t, i)];
     } else {
@@ -165,10 +173,7 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
     for (int j = 0; j < CW; ++j) cc[j] = ln(0)[j];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
-      if (p < Vn) {
-#pragma unroll
-        for (int j = 0; j < CW; ++j) e[p][j] = ln(2 + 2 * p)[j];
-      }
+      if (p < Vn) ldv<CW>(a.eta + (long long)p * N + cell, e[p]);
     const bool hi_pair = CW == 2 && (cell & 2);
     {
       T zc[4] = {0, 0, 0, 0};
@@ -200,7 +205,8 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
             t4 += x * x * x * x;
           }
         const T zj = CW == 2 ? (hi_pair ? zp[j + 2 < 4 ? j + 2 : 3] : zp[j]) : zp[j];
-        ln(3 + 2 * p)[j] = precip_g(lc, cc[j], e[p][j], t2, t4, ln(3 + 2 * p)[j], zj);
+        const T gv = precip_g(lc, cc[j], e[p][j], t2, t4, ln(2 + p)[j], zj);
+        ln(2 + p)[j] = e[p][j] - lc.dtL * gv;
       }
     }
   }
@@ -210,6 +216,62 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
   for (int r = 0; r < L::R1; ++r) x[r] = sl[L::in_pos(t, r)];
   __syncthreads();
   zfwd_line<T, H>(x, t, sl, rok ? a.dst + ((long long)f2 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
+}
+
+// The end of the precipitate step fused with the start of the next one: the
+// z inverse of the updated spectra [c', eta'_0 .. eta'_V-1] into the fields
+// (the concentration with its FP64 mass offset added before rounding, as
+// k_zinv does), then the z forward of the next step's chain-1 inputs
+// [eta'_p^2 (p < V), c'] from the rounded values just stored, written over
+// the spectrum rows the block read.  Every field of a row lives in one block,
+// so no other block reads those rows; the next step starts at its y forward.
+template <typename T> struct PrecipZArgs {
+  cplx<T>* spec;  // in: [V+1][rows][H] spectra of c', eta'; out: [F1][rows][H] chain-1 z spectra
+  T* c;           // [N]
+  T* eta;         // [V][N]
+  long long nrows, N;
+  int lr, V, F1;  // F1 = V + 1 when c couples elastically (its row is transformed too)
+  int mass;       // add `offset` to c' in FP64
+  double offset;
+  const cplx<T>* tw_h;
+  const cplx<T>* tw_n2;
+};
+
+template <typename T, int H>
+__global__ void __launch_bounds__(256) k_precip_zinv_fwd(PrecipZArgs<T> a) {
+  using L = Line<T, H>;
+  using V = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* smb = reinterpret_cast<V*>(smraw);
+  const int NL = a.V + 1;  // lines per row: c', then eta'_p
+  const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
+  const int rr = line / NL, f = line - rr * NL;
+  const long long row = (long long)blockIdx.x * a.lr + rr;
+  const bool act = rr < a.lr && row < a.nrows;
+  V* sl = smb + line * L::PAD;
+  V r[L::R1];
+  // its reads of the block's spectrum rows finish before its first barrier
+  zinv_row<T, H>(a.spec + ((long long)f * a.nrows + (act ? row : 0)) * H, act, t, sl, a.tw_h, a.tw_n2, r);
+  T* const dst = f == 0 ? a.c : a.eta + (long long)(f - 1) * a.N;
+  const bool off = f == 0 && a.mass;
+#pragma unroll
+  for (int i = 0; i < L::R1; ++i) {
+    V v = r[i];
+    if (off) v = mk2((T)((double)v.x + a.offset), (T)((double)v.y + a.offset));
+    if (act) reinterpret_cast<V*>(dst + row * (2 * H))[L::out_pos(t, i)] = v;
+    r[i] = f == 0 ? v : mk2(v.x * v.x, v.y * v.y);  // the chain-1 input: c' itself, eta'_p^2
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = r[i];
+  __syncthreads();
+  V x[L::R1];
+#pragma unroll
+  for (int q = 0; q < L::R1; ++q) x[q] = sl[L::in_pos(t, q)];
+  __syncthreads();
+  const int f1 = f == 0 ? a.V : f - 1;  // chain-1 order: eta_p^2, then c
+  const bool out = act && f1 < a.F1;
+  zfwd_line<T, H>(x, t, sl, out ? a.spec + ((long long)f1 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
 }
 
 template <typename T>

@@ -54,9 +54,8 @@ def test_precip_baseline_noise_fp64(gb, orc):
 
 @pytest.mark.parametrize("shape,V", [((8, 12, 2), 4), ((8, 8, 16), 6), ((2, 4, 512), 8)])
 def test_precip_fused_and_separate_passes_fp64(gb, orc, shape, V):
-    """Odd runs of two cells (n2 = 2), the wide-variant instances, and rows
-    too wide for one block (512 cells x 18 update fields), which take the
-    separate z-inverse / local / z-forward passes."""
+    """Odd runs of two cells (n2 = 2), the wide-variant instances, and the
+    longest rows (512 cells, 8 variants: 10 update fields of 16 threads)."""
     p = precip_base(gb, shape, F64, V=V)
     c0 = gb.initial_c(p, 12)
     e0 = gb.initial_eta(p, 13, 0.4)
@@ -64,6 +63,42 @@ def test_precip_fused_and_separate_passes_fp64(gb, orc, shape, V):
     cr, er = orc.precip_run(p, c0, e0, 2)
     cg, eg = run_precip(gb, p, c0, e0, 2)
     assert rel_l2(cg, cr) < 1e-11 and rel_l2(eg, er) < 1e-11
+
+
+@pytest.mark.parametrize("dtype,shape,ce", [(F64, (8, 8, 16), 1), (F32, (16, 12, 32), 1), (F64, (8, 12, 2), 0)])
+def test_precip_fused_next_z_forward_same_bits(gb, dtype, shape, ce):
+    """The last sweep of a step also writes the next step's chain-1 z spectra;
+    uploading eta again before every step (its own values; the concentration
+    and its mass stay on the device) forces the separate z forward.  Both give
+    the same bits (with and without the concentration's misfit)."""
+    p = precip_base(gb, shape, dtype)
+    p.c_elastic = ce
+    p.noise_amp = 1e-3
+    c0 = gb.initial_c(p, 21)
+    e0 = gb.initial_eta(p, 22, 0.4)
+    if dtype == F32:
+        c0 = c0.astype(np.float32).astype(np.float64)
+        e0 = e0.astype(np.float32).astype(np.float64)
+    s = gb.Sim(p)
+    try:
+        s.set_field("concentration", c0)
+        s.set_field("eta", e0)
+        s.step(4)
+        fc, fe = s.concentration(np.float64), s.eta(np.float64)
+    finally:
+        s.close()
+    s = gb.Sim(p)
+    try:
+        s.set_field("concentration", c0)
+        e = e0
+        for k in range(4):
+            s.set_field("eta", e)
+            s.step(1)
+            e = s.eta(np.float64)
+        c = s.concentration(np.float64)
+    finally:
+        s.close()
+    assert np.array_equal(fc, c) and np.array_equal(fe, e)
 
 
 @pytest.mark.parametrize("V", [1, 2, 3])
