@@ -40,31 +40,6 @@ template <typename V> __host__ __device__ __forceinline__ V conjg(V a) { return 
 // i * a
 template <typename V> __host__ __device__ __forceinline__ V muli(V a) { return mk2(-a.y, a.x); }
 
-// L2 eviction priorities of individual loads (createpolicy + ld with an L2
-// cache hint, sm_80 and later): a small table read many times per pass is
-// loaded with evict_last, the streaming spectra with evict_first, so the
-// streams do not push the table out of the 126 MB L2.
-__device__ __forceinline__ uint64_t l2_evict_last() {
-  uint64_t p;
-  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ uint64_t l2_evict_first() {
-  uint64_t p;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ float2 ld_hint(const float2* q, uint64_t pol) {
-  float2 v;
-  asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(q), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ double2 ld_hint(const double2* q, uint64_t pol) {
-  double2 v;
-  asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(q), "l"(pol));
-  return v;
-}
-
 // Derived constants of one simulation, passed by value to every pass.
 template <typename T> struct ElasticConst {
   int na, nb;           // rows (outputs) and columns (inputs) of B

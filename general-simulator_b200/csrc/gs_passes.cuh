@@ -409,10 +409,9 @@ struct TableOp {
       }
     } else {
       const cplx<T>* b2 = reinterpret_cast<const cplx<T>*>(pt);
-      const uint64_t keep = l2_evict_last();  // the table is read again for the other ky, kz signs
 #pragma unroll
       for (int i = 0; i < S / 2; ++i) {
-        const cplx<T> w = ld_hint(b2 + i, keep);
+        const cplx<T> w = __ldg(b2 + i);
         bv[2 * i] = w.x;
         bv[2 * i + 1] = w.y;
       }
@@ -763,9 +762,8 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const bool fw = grp < a.F;
   {
     const V* src = in_base + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
-    const uint64_t stream = l2_evict_first();  // read once: leave L2 to the B table
 #pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = fw ? ld_hint(src + (long long)r * (L::P * rstride), stream) : mk2((T)0, (T)0);
+    for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
   }
   xpass_tile<T, N0, FM, GM, Op, true, EX>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v, tws);
 }
