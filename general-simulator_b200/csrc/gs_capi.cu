@@ -15,6 +15,8 @@
 #include <condition_variable>
 #include <cstring>
 #include <string>
+#include <algorithm>
+#include <utility>
 #include <mutex>
 #include <vector>
 
@@ -997,6 +999,11 @@ static void free_snaps(gs_sim* s);
 static void free_sim(gs_sim* s) {
   if (!s) return;
   free_snaps(s);
+  if (s->up_stream) cudaStreamSynchronize(s->up_stream);
+  if (s->stage) cudaFree(s->stage);
+  if (s->up_stream) cudaStreamDestroy(s->up_stream);
+  if (s->up_done) cudaEventDestroy(s->up_done);
+  if (s->stage_free) cudaEventDestroy(s->stage_free);
   void* ptrs[] = {s->eta[0], s->eta[1], s->spec, s->spec2, s->defect, s->K, s->conc, s->rbuf, s->mubuf,
                   s->stressbuf, s->ktab, s->tw, s->partials, s->red, s->btab, s->d_mcs, s->d_simscale};
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
@@ -1222,6 +1229,7 @@ extern "C" int gs_sim_set_field(gs_sim* s, const char* name, const void* host, s
   if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_set_field: null argument");
   sim_graph_reset(s);
   s->spec_ready = false;
+  if (std::string(name) == "eta") s->staged = false;  // a field set given now replaces a staged one
   gs_cufft_invalidate(s);
   if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
   const int V = s->p.nvariants;
@@ -1448,11 +1456,50 @@ static int timed_steps(gs_sim* s, int nsteps, cudaStream_t st, const char* targe
   return GS_OK;
 }
 
+// a field set staged by gs_sim_stage_field_async becomes the current one:
+// the stepping stream waits for its copy, the buffers swap, and the buffer
+// handed to the stage is free once the stepping stream passes this point
+static int take_staged(gs_sim* s, cudaStream_t st) {
+  if (!s->staged) return GS_OK;
+  GS_CU(cudaStreamWaitEvent(st, s->up_done, 0), "wait for the staged upload");
+  std::swap(s->eta[s->cur], s->stage);
+  sim_graph_reset(s);
+  s->spec_ready = false;
+  gs_cufft_invalidate(s);
+  GS_CU(cudaEventRecord(s->stage_free, st), "stage free");
+  s->staged = false;
+  return GS_OK;
+}
+
+extern "C" int gs_sim_stage_field_async(gs_sim* s, const char* name, const void* host, size_t count, int dtype) {
+  if (!s || !name || !host) return gs_set_error(GS_EINVAL, "gs_sim_stage_field_async: null argument");
+  if (std::string(name) != "eta") return gs_set_error(GS_EINVAL, "gs_sim_stage_field_async: only \"eta\"");
+  if (s->p.model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "gs_sim_stage_field_async: martensite only");
+  if (dtype != s->p.dtype) return gs_set_error(GS_EINVAL, "gs_sim_stage_field_async: dtype must be the simulation's");
+  const size_t n = (size_t)s->N * s->p.nvariants;
+  if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
+  if (s->staged) return gs_set_error(GS_EINVAL, "gs_sim_stage_field_async: a staged field set waits for a step");
+  if (!s->stage) {
+    GS_CU(cudaMalloc(&s->stage, n * elt(s)), "cudaMalloc staging field set");
+    GS_CU(cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking), "upload stream");
+    GS_CU(cudaEventCreateWithFlags(&s->up_done, cudaEventDisableTiming), "event");
+    GS_CU(cudaEventCreateWithFlags(&s->stage_free, cudaEventDisableTiming), "event");
+    GS_CU(cudaEventRecord(s->stage_free, s->own_stream), "event");
+  }
+  // the stage may still be the buffer an earlier step read or a snapshot copied
+  GS_CU(cudaStreamWaitEvent(s->up_stream, s->stage_free, 0), "wait for a free stage");
+  GS_CU(cudaMemcpyAsync(s->stage, host, n * elt(s), cudaMemcpyHostToDevice, s->up_stream), "staged upload");
+  GS_CU(cudaEventRecord(s->up_done, s->up_stream), "event");
+  s->staged = true;
+  return GS_OK;
+}
+
 extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
   if (!s) return gs_set_error(GS_EINVAL, "gs_sim_step: null sim");
   if (nsteps < 0) return gs_set_error(GS_EINVAL, "nsteps %d", nsteps);
   cudaStream_t st = pick_stream(s, stream);
   s->launches = 0;
+  GS_TRY(take_staged(s, st));
   const bool f64 = s->p.dtype == GS_DTYPE_F64;
   if (const char* tt = timing_target())
     if (!s->profiling && !s->trial) return timed_steps(s, nsteps, st, tt);
@@ -3258,6 +3305,7 @@ extern "C" int gs_sim_set_field_async(gs_sim* s, const char* name, const void* h
   if (count != n) return gs_set_error(GS_EINVAL, "eta: %zu values, expected %zu", count, n);
   sim_graph_reset(s);
   s->spec_ready = false;
+  s->staged = false;  // a field set given now replaces a staged one
   gs_cufft_invalidate(s);
   cudaStream_t st = pick_stream(s, stream);
   GS_CU(cudaMemcpyAsync(s->eta[s->cur], host, n * elt(s), cudaMemcpyHostToDevice, st), "upload");

@@ -76,6 +76,13 @@ struct gs_sim {
   int nmarks = 0;
   bool profiling = false;
   gs_snaps* snaps = nullptr;  // created by the first gs_sim_copy_field_async
+  // gs_sim_stage_field_async: the next field set, copied into `stage` on the
+  // upload stream while the GPU steps; the next gs_sim_step swaps it in
+  void* stage = nullptr;
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t up_done = nullptr;     // the staged copy has landed
+  cudaEvent_t stage_free = nullptr;  // the buffer now in `stage` is no longer read
+  bool staged = false;               // a staged field set waits for the next step
 };
 
 // record a pass boundary when gs_sim_profile_step (or GS_TIMING) is active;

@@ -164,6 +164,7 @@ def lib() -> C.CDLL:
         "gs_plain_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_plain_step": (C.c_int, [vp, C.c_int, vp]),
         "gs_sim_pass_name": (C.c_char_p, [vp, C.c_int]),
+        "gs_sim_stage_field_async": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.c_int]),
         "gs_cufft_create": (C.c_int, [P, C.POINTER(vp)]),
         "gs_cufft_step": (C.c_int, [vp, C.c_int, vp]),
         "gs_adjoint_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),

@@ -193,6 +193,15 @@ int gs_sim_device_field(gs_sim* s, const char* name, void** dptr, size_t* bytes)
 int gs_sim_copy_field_async(gs_sim* s, const char* name, void* stream, void* pinned_dst, int* ticket);
 int gs_sim_copy_field_wait(gs_sim* s, int ticket, void* host, size_t count, int dtype);
 int gs_sim_set_field_async(gs_sim* s, const char* name, const void* host, size_t count, int dtype, void* stream);
+/* The next step's field set ("eta", the simulation's dtype), copied from
+ * `host` (page-locked for the copy to overlap) into a staging buffer on the
+ * simulation's upload stream, so the copy runs while the GPU steps and
+ * while an earlier download runs the other way; the next gs_sim_step waits
+ * for it and swaps it in as the current field set.  gs_sim_set_field(_async)
+ * of "eta" in between drops the staged set.  One staged set at a time
+ * (GS_EINVAL otherwise); martensite simulations.  The caller keeps `host`
+ * unchanged until that step has started on the GPU. */
+int gs_sim_stage_field_async(gs_sim* s, const char* name, const void* host, size_t count, int dtype);
 /* Run one step with a CUDA event between consecutive passes on the step's
  * stream; pass_ms[i] receives the device time of pass i (in launch order:
  * z forward, y forward, x contraction, y inverse, update for the

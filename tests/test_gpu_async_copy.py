@@ -100,3 +100,56 @@ def test_fp64_copy_converted_and_third_copy_waits_for_a_slot(gb):
             gb.check(L.gs_sim_copy_field_wait(sim.h, t.value, got.ctypes.data, got.size, 0), "wait")
     finally:
         sim.close()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_staged_uploads_equal_synchronous_uploads(gb, graph):
+    """gs_sim_stage_field_async: each step's input staged from page-locked
+    memory while the previous step runs and its output downloads; the steps
+    give the same bits as uploading with gs_sim_set_field before each step.
+    A set_field after staging drops the staged set; a second stage before a
+    step is refused."""
+    import torch
+
+    p = gb.mart3d_params(32, dtype=0, noise=1e-3)
+    n = p.nvariants * p.ncells
+    L = gb.lib()
+    inputs = [torch.from_numpy(gb.initial_eta(p, 30 + k, 0.3).astype(np.float32).ravel()).pin_memory()
+              for k in range(4)]
+    outs = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
+    ref = []
+    s = gb.Sim(p)
+    try:
+        for k in range(4):
+            s.set_field("eta", inputs[k].numpy())
+            s.step(1)
+            ref.append(s.eta(np.float32).ravel())
+    finally:
+        s.close()
+    s = gb.Sim(p)
+    try:
+        s.use_graph(graph)
+        tk = C.c_int(0)
+        gb.check(L.gs_sim_stage_field_async(s.h, b"eta", C.c_void_p(inputs[0].data_ptr()), n, 0), "stage")
+        assert L.gs_sim_stage_field_async(s.h, b"eta", C.c_void_p(inputs[0].data_ptr()), n, 0) == gb.GS_EINVAL
+        tickets = []
+        for k in range(4):
+            s.step(1)
+            gb.check(L.gs_sim_copy_field_async(s.h, b"eta", None, C.c_void_p(outs[k].data_ptr()), C.byref(tk)), "dl")
+            tickets.append(tk.value)
+            if k + 1 < 4:
+                gb.check(L.gs_sim_stage_field_async(s.h, b"eta", C.c_void_p(inputs[k + 1].data_ptr()), n, 0), "stage")
+            if len(tickets) == 2:
+                gb.check(L.gs_sim_copy_field_wait(s.h, tickets.pop(0), None, 0, 0), "wait")
+        for t in tickets:
+            gb.check(L.gs_sim_copy_field_wait(s.h, t, None, 0, 0), "wait")
+        for k in range(4):
+            assert np.array_equal(outs[k].numpy(), ref[k]), k
+        # a staged set dropped by a direct upload
+        gb.check(L.gs_sim_stage_field_async(s.h, b"eta", C.c_void_p(inputs[3].data_ptr()), n, 0), "stage")
+        s.set_field("eta", inputs[0].numpy())
+        s.set_scalar("step", 0)
+        s.step(1)
+        assert np.array_equal(s.eta(np.float32).ravel(), ref[0])
+    finally:
+        s.close()
