@@ -638,6 +638,20 @@ def run_ours(args, ws, rank, local):
     value = N * args.steps * ws / (ms_max / 1e3)
     launches = int(round(launches_per_step * args.steps))
 
+    # the same steps replayed from a captured CUDA graph (gs_sim_use_graph)
+    with torch.cuda.stream(stream):
+        sim.use_graph(True)
+        sim.step(4, sh)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        sim.step(args.steps, sh)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        graph_ms = g0.elapsed_time(g1) / args.steps
+        sim.use_graph(False)
+
     # per-pass device times of one step (live, on the launching stream)
     with torch.cuda.stream(stream):
         passes = [sim.profile_step(sh) for _ in range(5)]
@@ -781,6 +795,10 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
+        "graph_replay": {"ms_per_step": graph_ms,
+                         "note": "the timed steps again, replayed from a captured CUDA graph (gs_sim_use_graph): "
+                                 "the captured kernels read the step constants from device memory (the noise "
+                                 "counter advances between replays), which costs more than the launches it saves"},
         **extras,
     }
     print(json.dumps(line), flush=True)
