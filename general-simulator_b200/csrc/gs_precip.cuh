@@ -238,7 +238,7 @@ template <typename T> struct PrecipZArgs {
 };
 
 template <typename T, int H>
-__global__ void __launch_bounds__(256) k_precip_zinv_fwd(PrecipZArgs<T> a) {
+__global__ void __launch_bounds__(256, 3) k_precip_zinv_fwd(PrecipZArgs<T> a) {
   using L = Line<T, H>;
   using V = cplx<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
