@@ -2,6 +2,7 @@
 
 Outputs (in-tree, git-ignored, shipped with the working copy):
   general-simulator_b200/libgsb200.so   CUDA kernels + C ABI (include/gs_capi.h)
+  general-simulator_b200/libgsb200_bc.so  the same with the kernels' index asserts (-DGS_BOUNDS_CHECK)
   general-simulator_b200/gsi            script interpreter (the reference's front end)
 """
 from __future__ import annotations
@@ -23,8 +24,9 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 CU_SOURCES = ["gs_capi.cu", "gs_k_zy.cu", "gs_k_zy_f32.cu", "gs_k_zy_f64.cu", "gs_k_x.cu", "gs_k_x33.cu",
               "gs_k_x55.cu", "gs_k_x86.cu", "gs_k_x99.cu", "gs_k_xt.cu", "gs_k_xp10.cu", "gs_k_xp2.cu", "gs_k_xp18.cu",
               "gs_k_precip.cu", "gs_k_mart.cu", "gs_k_mart_f32.cu", "gs_k_mart_f64.cu",
-              "gs_k_adj_f32.cu", "gs_k_adj_f64.cu", "gs_plain.cu", "gs_cores.cu", "gs_k_padj.cu", "gs_k_xtma.cu", "gs_noise.cu", "gs_cufft.cu"]
+              "gs_k_adj_f32.cu", "gs_k_adj_f64.cu", "gs_plain.cu", "gs_cores.cu", "gs_k_padj.cu", "gs_k_xtma.cu", "gs_noise.cu", "gs_cufft.cu", "gs_bounds.cu"]
 LIB = os.path.join(HERE, "libgsb200.so")
+LIB_BC = os.path.join(HERE, "libgsb200_bc.so")
 
 
 def _run(cmd: list[str]) -> None:
@@ -48,24 +50,29 @@ def _headers() -> list[str]:
     return hs + [os.path.join(ROOT, "include", "gs_capi.h")]
 
 
-def build_lib(jobs: int = 8, verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build_lib(jobs: int = 8, verbose: bool = False, bounds_check: bool = False) -> str:
+    """libgsb200.so, or with bounds_check the bounds-check build libgsb200_bc.so
+    (index asserts in every pass kernel, GS_EBOUNDS from the step entries)."""
+    bdir = BUILD + ("_bc" if bounds_check else "")
+    lib = LIB_BC if bounds_check else LIB
+    extra = ["-DGS_BOUNDS_CHECK"] if bounds_check else []
+    os.makedirs(bdir, exist_ok=True)
     hdrs = _headers()
     objs = []
     todo = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(bdir, src.replace(".cu", ".o"))
         objs.append(o)
         if _stale(o, [s] + hdrs):
-            todo.append([NVCC, *ARCH, *NVFLAGS, "-c", s, "-o", o])
+            todo.append([NVCC, *ARCH, *NVFLAGS, *extra, "-c", s, "-o", o])
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         for f in [ex.submit(_run, c) for c in todo]:
             f.result()
-    if todo or _stale(LIB, objs):
-        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcufft", "-Xlinker",
+    if todo or _stale(lib, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", lib, *objs, "-lcufft", "-Xlinker",
               "-rpath=/usr/local/cuda/lib64"])
-    return LIB
+    return lib
 
 
 HOST_SOURCES = ["gs_script.cpp", "gs_driver.cpp", "gs_plugins.cpp", "gs_main.cpp"]
@@ -108,6 +115,7 @@ def build_reference() -> str | None:
 
 def build_all(jobs: int = 8) -> None:
     build_lib(jobs)
+    build_lib(jobs, bounds_check=True)
     build_frontend()
     build_oracle()
     build_reference()

@@ -51,6 +51,8 @@ __global__ void __launch_bounds__(256, VM <= 4 ? 2 : 1) k_adj_update(AdjArgs<T> 
   V* smb = reinterpret_cast<V*>(smraw);
   const MartConst<T>& mc = a.mc;
   const int Vn = mc.V;
+  GS_BC_SMEM_GUARD((long long)(blockDim.x / L::P) * L::PAD, V, BC_UPD_SMEM)
+  GS_BC_DECL(const long long fext = (long long)Vn * a.nrows * a.n2)
   {
     const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
     const int v = line % Vn, rr = line / Vn;
@@ -59,7 +61,8 @@ __global__ void __launch_bounds__(256, VM <= 4 ? 2 : 1) k_adj_update(AdjArgs<T> 
     V* sl = smb + line * L::PAD;
     const V* srow = a.spec + ((long long)v * a.nrows + (act ? row : 0)) * H;
     V r[L::R1];
-    zinv_row<T, H>(srow, act, t, sl, a.tw_h, a.tw_n2, r);
+    zinv_row<T, H>(srow, act, t, sl, a.tw_h, a.tw_n2, r, GS_BCX(((long long)v * a.nrows + (act ? row : 0)) * H),
+                   GS_BCX(fext / 2));
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = r[i];
@@ -91,8 +94,8 @@ __global__ void __launch_bounds__(256, VM <= 4 ? 2 : 1) k_adj_update(AdjArgs<T> 
 #pragma unroll
     for (int p = 0; p < VM; ++p)
       if (p < Vn) {
-        ldv<CW>(a.eta + (long long)p * N + cell, e[p]);
-        ldv<CW>(a.lam_in + (long long)p * N + cell, l[p]);
+        ldv<CW>(a.eta + GS_BCR(0, (long long)p * N + cell, CW, fext, BC_UPD_ETA), e[p]);
+        ldv<CW>(a.lam_in + GS_BCR(0, (long long)p * N + cell, CW, fext, BC_UPD_ETA), l[p]);
       }
     T S[CW], ed[CW];
 #pragma unroll
@@ -111,13 +114,14 @@ __global__ void __launch_bounds__(256, VM <= 4 ? 2 : 1) k_adj_update(AdjArgs<T> 
     for (int q = 0; q < VM; ++q) {
       if (q >= Vn) break;
       const T* lq_ = a.lam_in + (long long)q * N + cell;
+      GS_BC_DECL(const long long qoff = (long long)q * N + cell)
       T vxp[CW], vxm[CW], vyp[CW], vym[CW], Rq[CW];
-      ldv<CW>(lq_ + oxp, vxp);
-      ldv<CW>(lq_ + oxm, vxm);
-      ldv<CW>(lq_ + oyp, vyp);
-      ldv<CW>(lq_ + oym, vym);
-      ldv<CW>(a.R + (long long)q * N + cell, Rq);
-      const T zl_ = lq_[ozl], zr_ = lq_[ozr];
+      ldv<CW>(lq_ + GS_BCR(qoff, oxp, CW, fext, BC_UPD_ETA), vxp);
+      ldv<CW>(lq_ + GS_BCR(qoff, oxm, CW, fext, BC_UPD_ETA), vxm);
+      ldv<CW>(lq_ + GS_BCR(qoff, oyp, CW, fext, BC_UPD_ETA), vyp);
+      ldv<CW>(lq_ + GS_BCR(qoff, oym, CW, fext, BC_UPD_ETA), vym);
+      ldv<CW>(a.R + GS_BCR(0, (long long)q * N + cell, CW, fext, BC_UPD_AUX), Rq);
+      const T zl_ = lq_[GS_BCO(qoff, ozl, fext, BC_UPD_ETA)], zr_ = lq_[GS_BCO(qoff, ozr, fext, BC_UPD_ETA)];
       const T* Qq = reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0;
       const T linq = mc.lin[q];
       T out[CW];
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(256, VM <= 4 ? 2 : 1) k_adj_update(AdjArgs<T> 
         acc[ADJ_AC_LAM] += 2.0 * ((double)S[j] - (double)e2) * el_;
         acc[ADJ_S_LAM] += (2.0 * (double)mc.el * (double)Rv + (double)linq) * el_;
       }
-      stv<CW>(a.lam_out + (long long)q * N + cell, out);
+      stv<CW>(a.lam_out + GS_BCR(0, (long long)q * N + cell, CW, fext, BC_UPD_ETA_OUT), out);
     }
   }
   Neu nacc[ADJ_N];

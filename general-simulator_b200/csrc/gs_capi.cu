@@ -45,6 +45,11 @@ int gs_set_error(int code, const char* fmt, ...) {
 
 int gs_cuda_check(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return GS_OK;
+  if (e == cudaErrorInvalidValue && gs::bounds_message()[0]) {  // a launch refused by the range check
+    const int r = gs_set_error(GS_EINVAL, "%s: %s", what, gs::bounds_message());
+    gs::clear_bounds_message();
+    return r;
+  }
   if (e == cudaErrorMemoryAllocation) return gs_set_error(GS_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
     return gs_set_error(GS_ENODEV, "%s: %s", what, cudaGetErrorString(e));
@@ -1494,7 +1499,13 @@ extern "C" int gs_sim_stage_field_async(gs_sim* s, const char* name, const void*
   return GS_OK;
 }
 
+static int gs_sim_step_body(gs_sim* s, int nsteps, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_sim_step(gs_sim* s, int nsteps, void* stream) {
+  return bc_after(gs_sim_step_body(s, nsteps, stream), static_cast<cudaStream_t>(stream));
+}
+
+static int gs_sim_step_body(gs_sim* s, int nsteps, void* stream) {
   if (!s) return gs_set_error(GS_EINVAL, "gs_sim_step: null sim");
   if (nsteps < 0) return gs_set_error(GS_EINVAL, "nsteps %d", nsteps);
   cudaStream_t st = pick_stream(s, stream);
@@ -1883,7 +1894,13 @@ extern "C" int gs_batch_get_field(gs_batch* b, int sim, const char* name, void* 
   return download(g, src, host, count, dtype);
 }
 
+static int gs_batch_step_body(gs_batch* b, int nsteps, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_batch_step(gs_batch* b, int nsteps, void* stream) {
+  return bc_after(gs_batch_step_body(b, nsteps, stream), static_cast<cudaStream_t>(stream));
+}
+
+static int gs_batch_step_body(gs_batch* b, int nsteps, void* stream) {
   if (!b || nsteps < 0) return gs_set_error(GS_EINVAL, "gs_batch_step: bad arguments");
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
   for (gs_sim* g : b->groups) g->launches = 0;
@@ -2044,7 +2061,13 @@ template <typename T> static int noalloc_step(gs_sim& s, const void* in, void* o
 
 extern "C" size_t gs_mart_step_noalloc_max_bytes(void) { return kNoallocScratchBytes; }
 
-extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void* eta_out, int64_t step,
+static int gs_mart_step_noalloc_body(const gs_params* p, const void* eta_in, void* eta_out, int64_t step, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
+extern "C" int gs_mart_step_noalloc(const gs_params* p, const void* eta_in, void* eta_out, int64_t step, void* stream) {
+  return bc_after(gs_mart_step_noalloc_body(p, eta_in, eta_out, step, stream), static_cast<cudaStream_t>(stream));
+}
+
+static int gs_mart_step_noalloc_body(const gs_params* p, const void* eta_in, void* eta_out, int64_t step,
                                     void* stream) {
   if (!p || !eta_in || !eta_out) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: null argument");
   if (p->model != GS_MODEL_MART) return gs_set_error(GS_EINVAL, "gs_mart_step_noalloc: model must be martensite");
@@ -2394,7 +2417,16 @@ template <typename T> static int adj_forward(gs_adjoint* a, cudaStream_t st) {
   return GS_OK;
 }
 
+static int gs_adjoint_forward_body(gs_adjoint* a, const void* eta0, int dtype, void* eta_final, double* e_el_final,
+                                   void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_adjoint_forward(gs_adjoint* a, const void* eta0, int dtype, void* eta_final, double* e_el_final,
+                                  void* stream) {
+  return bc_after(gs_adjoint_forward_body(a, eta0, dtype, eta_final, e_el_final, stream),
+                  static_cast<cudaStream_t>(stream));
+}
+
+static int gs_adjoint_forward_body(gs_adjoint* a, const void* eta0, int dtype, void* eta_final, double* e_el_final,
                                   void* stream) {
   if (!a || !eta0) return gs_set_error(GS_EINVAL, "gs_adjoint_forward: null argument");
   if (dtype != GS_DTYPE_F32 && dtype != GS_DTYPE_F64) return gs_set_error(GS_EINVAL, "dtype %d", dtype);
@@ -2466,7 +2498,16 @@ static int adj_backward(gs_adjoint* a, const void* seed_dev, double seed_e, doub
   return c;  // index of the buffer holding dJ/deta_0
 }
 
+static int gs_adjoint_backward_body(gs_adjoint* a, const void* seed, int seed_dtype, double seed_e, double* loss,
+                                    double* grads, void* grad_eta0, int grad_dtype, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_adjoint_backward(gs_adjoint* a, const void* seed, int seed_dtype, double seed_e, double* loss,
+                                   double* grads, void* grad_eta0, int grad_dtype, void* stream) {
+  return bc_after(gs_adjoint_backward_body(a, seed, seed_dtype, seed_e, loss, grads, grad_eta0, grad_dtype, stream),
+                  static_cast<cudaStream_t>(stream));
+}
+
+static int gs_adjoint_backward_body(gs_adjoint* a, const void* seed, int seed_dtype, double seed_e, double* loss,
                                    double* grads, void* grad_eta0, int grad_dtype, void* stream) {
   if (!a || !grads) return gs_set_error(GS_EINVAL, "gs_adjoint_backward: null argument");
   if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_adjoint_backward: run gs_adjoint_forward first");
@@ -2849,7 +2890,16 @@ static int padj_recompute(gs_padjoint* a, int j, cudaStream_t st) {
   return GS_OK;
 }
 
+static int gs_precip_adjoint_forward_body(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
+                                          void* eta_final, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_precip_adjoint_forward(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
+                                         void* eta_final, void* stream) {
+  return bc_after(gs_precip_adjoint_forward_body(a, c0, eta0, dtype, c_final, eta_final, stream),
+                  static_cast<cudaStream_t>(stream));
+}
+
+static int gs_precip_adjoint_forward_body(gs_padjoint* a, const void* c0, const void* eta0, int dtype, void* c_final,
                                          void* eta_final, void* stream) {
   if (!a) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: null handle");
   if (!c0 != !eta0) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_forward: give both c0 and eta0, or neither");
@@ -3054,7 +3104,16 @@ extern "C" int gs_precip_adjoint_set_seed(gs_padjoint* a, const void* seed_c, co
   return GS_OK;
 }
 
+static int gs_precip_adjoint_backward_body(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype,
+                                           double* grads, void* grad_c0, void* grad_eta0, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_precip_adjoint_backward(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype,
+                                          double* grads, void* grad_c0, void* grad_eta0, void* stream) {
+  return bc_after(gs_precip_adjoint_backward_body(a, seed_c, seed_eta, dtype, grads, grad_c0, grad_eta0, stream),
+                  static_cast<cudaStream_t>(stream));
+}
+
+static int gs_precip_adjoint_backward_body(gs_padjoint* a, const void* seed_c, const void* seed_eta, int dtype,
                                           double* grads, void* grad_c0, void* grad_eta0, void* stream) {
   if (!a || !grads) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: null argument");
   if (!a->forward_done) return gs_set_error(GS_EINVAL, "gs_precip_adjoint_backward: run the forward first");
@@ -3606,21 +3665,39 @@ static int slab_check(gs_slab* sl, const void* a, const void* b, const char* wha
   return GS_OK;
 }
 
+static int gs_slab_begin_body(gs_slab* sl, void* send, void* halo_send, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_slab_begin(gs_slab* sl, void* send, void* halo_send, void* stream) {
+  return bc_after(gs_slab_begin_body(sl, send, halo_send, stream), static_cast<cudaStream_t>(stream));
+}
+
+static int gs_slab_begin_body(gs_slab* sl, void* send, void* halo_send, void* stream) {
   GS_TRY(slab_check(sl, send, halo_send, "gs_slab_begin"));
   cudaStream_t st = pick_stream(sl->loc, stream);
   return sl->loc->p.dtype == GS_DTYPE_F64 ? slab_begin<double>(sl, send, halo_send, st)
                                           : slab_begin<float>(sl, send, halo_send, st);
 }
 
+static int gs_slab_xpass_body(gs_slab* sl, const void* recv, void* send, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_slab_xpass(gs_slab* sl, const void* recv, void* send, void* stream) {
+  return bc_after(gs_slab_xpass_body(sl, recv, send, stream), static_cast<cudaStream_t>(stream));
+}
+
+static int gs_slab_xpass_body(gs_slab* sl, const void* recv, void* send, void* stream) {
   GS_TRY(slab_check(sl, recv, send, "gs_slab_xpass"));
   cudaStream_t st = pick_stream(sl->loc, stream);
   return sl->loc->p.dtype == GS_DTYPE_F64 ? slab_xpass<double>(sl, recv, send, st)
                                           : slab_xpass<float>(sl, recv, send, st);
 }
 
+static int gs_slab_end_body(gs_slab* sl, const void* recv, const void* halo_recv, void* stream);
+// the bounds-check build waits here and reports index violations (GS_EBOUNDS)
 extern "C" int gs_slab_end(gs_slab* sl, const void* recv, const void* halo_recv, void* stream) {
+  return bc_after(gs_slab_end_body(sl, recv, halo_recv, stream), static_cast<cudaStream_t>(stream));
+}
+
+static int gs_slab_end_body(gs_slab* sl, const void* recv, const void* halo_recv, void* stream) {
   GS_TRY(slab_check(sl, recv, halo_recv, "gs_slab_end"));
   cudaStream_t st = pick_stream(sl->loc, stream);
   return sl->loc->p.dtype == GS_DTYPE_F64 ? slab_end<double>(sl, recv, halo_recv, st)

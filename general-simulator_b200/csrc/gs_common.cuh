@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "gs_bc.cuh"
+
 #define GS_MAXF 9    // elastic fields: up to 8 variants + concentration
 #define GS_MAXG 9    // contraction outputs (6 stress components or F)
 

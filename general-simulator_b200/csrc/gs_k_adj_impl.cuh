@@ -16,6 +16,17 @@ template <typename T, int H, int VM> cudaError_t adj_n(AdjArgs<T>& a, cudaStream
   const size_t smem = (size_t)lr * a.mc.V * L::PAD * sizeof(cplx<T>);
   allow_max_smem<k_adj_update<T, H, VM>>();
   const long long grid = (a.nrows + lr - 1) / lr;
+  if (bounds_check_on()) {
+    const char* k = "adjoint update";
+    const long long VN = (long long)a.mc.V * a.nrows * a.n2;
+    constexpr size_t va = ((2 * H) % 4 == 0 ? 4 : 2) * sizeof(T) < 16 ? ((2 * H) % 4 == 0 ? 4 : 2) * sizeof(T) : 16;
+    GS_RANGE(a.spec, VN / 2, cplx<T>, sizeof(cplx<T>), k, "Q spectra");
+    GS_RANGE(a.eta, VN, T, va, k, "eta");
+    GS_RANGE(a.lam_in, VN, T, va, k, "lambda in");
+    GS_RANGE(a.lam_out, VN, T, va, k, "lambda out");
+    GS_RANGE(a.R, VN, T, va, k, "R");
+    GS_RANGE(a.partials, grid * ADJ_N, double, sizeof(double), k, "partials");
+  }
   if (nblocks) *nblocks = (int)grid;
   k_adj_update<T, H, VM><<<(unsigned)grid, (unsigned)(per * lr), smem, s>>>(a);
   return cudaGetLastError();

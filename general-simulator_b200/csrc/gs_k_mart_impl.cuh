@@ -21,6 +21,20 @@ cudaError_t mu_n(MartArgs<T>& a, cudaStream_t s, int* nblocks, int nsim) {
   const size_t smem = (size_t)lr * a.mc.V * L::PAD * sizeof(cplx<T>);
   allow_max_smem<k_mart_update<T, H, VM, ST, BA, FU, true, HA>>();
   const long long grid = (a.nrows + lr - 1) / lr;
+  if (bounds_check_on()) {
+    const char* k = "martensite update";
+    const long long ns = BA ? nsim : 1, N = a.nrows * a.n2, VN = (long long)a.mc.V * N;
+    constexpr size_t va = ((2 * H) % 4 == 0 ? 4 : 2) * sizeof(T) < 16 ? ((2 * H) % 4 == 0 ? 4 : 2) * sizeof(T) : 16;
+    GS_RANGE(a.spec, ns * VN / 2, cplx<T>, sizeof(cplx<T>), k, "R spectra");
+    GS_RANGE(a.eta_in, ns * VN, T, va, k, "eta");
+    if (!ST) GS_RANGE(a.eta_out, ns * VN, T, va, k, "eta out");
+    if (a.mc.has_defect) GS_RANGE(a.defect, N, T, va, k, "defect mask");
+    if (a.mc.has_K) GS_RANGE(a.K, VN, T, va, k, "dislocation field");
+    if (!BA && a.r_out) GS_RANGE(a.r_out, VN, T, va, k, "R out");
+    if (FU) GS_RANGE(a.spec_next, ns * VN / 2, cplx<T>, sizeof(cplx<T>), k, "next spectra");
+    if (HA) GS_RANGE(a.halo, 2 * (long long)a.mc.V * a.n1 * a.n2, T, va, k, "halo planes");
+    if (ST) GS_RANGE(a.partials, grid * ACC_N, double, sizeof(double), k, "statistics partials");
+  }
   if (nblocks) *nblocks = (int)grid;
   k_mart_update<T, H, VM, ST, BA, FU, true, HA>
       <<<dim3((unsigned)grid, (unsigned)nsim), (unsigned)(per * lr), smem, s>>>(a);

@@ -7,6 +7,9 @@ namespace gs {
 
 template <typename T, int H> static cudaError_t zinv_n(ZinvArgs<T>& a, cudaStream_t s) {
   using L = Line<T, H>;
+  GS_RANGE(a.spec, a.nrows * H, cplx<T>, sizeof(cplx<T>), "z inverse", "spectrum");
+  for (long long f = 0; bounds_check_on() && f < a.nrows / a.rows_per_field; ++f)
+    GS_RANGE(a.dst[f], a.rows_per_field * 2 * H, T, sizeof(cplx<T>), "z inverse", "field");
   long long lpc = 256 / L::P;
   if (lpc < 1) lpc = 1;
   if (lpc > a.nrows) lpc = a.nrows;
@@ -41,6 +44,13 @@ template <typename T, int H, int VM> static cudaError_t pmid_n(PrecipMidArgs<T>&
   using L = Line<T, H>;
   const int per = L::P * (a.loc.V + 2);  // threads of one row
   if (per > 256) return cudaErrorInvalidConfiguration;
+  const long long N = a.nrows * 2 * H;
+  GS_RANGE(a.rspec, (long long)a.F1 * a.nrows * H, cplx<T>, sizeof(cplx<T>), "precipitate middle sweep", "R spectra");
+  constexpr size_t va = (2 * H) % 4 == 0 ? 4 * sizeof(T) : 2 * sizeof(T);  // the sweep's vector loads
+  GS_RANGE(a.c, N, T, sizeof(cplx<T>), "precipitate middle sweep", "concentration");
+  GS_RANGE(a.eta, (long long)a.loc.V * N, T, va < 16 ? va : 16, "precipitate middle sweep", "order parameters");
+  GS_RANGE(a.dst, (long long)(a.loc.V + 2) * a.nrows * H, cplx<T>, sizeof(cplx<T>), "precipitate middle sweep",
+           "update spectra");
   long long lr = 256 / per;
   if (a.lr_req > 0 && (long long)a.lr_req * per <= 256) lr = a.lr_req;
   if (lr > a.nrows) lr = a.nrows;
@@ -70,6 +80,10 @@ template <typename T, int H> static cudaError_t pzf_n(PrecipZArgs<T>& a, cudaStr
   using L = Line<T, H>;
   const int per = L::P * (a.V + 1);  // threads of one row
   if (per > 256) return cudaErrorInvalidConfiguration;
+  GS_RANGE(a.spec, (long long)(a.F1 > a.V + 1 ? a.F1 : a.V + 1) * a.nrows * H, cplx<T>, sizeof(cplx<T>),
+           "precipitate last sweep", "spectra");
+  GS_RANGE(a.c, a.N, T, sizeof(cplx<T>), "precipitate last sweep", "concentration");
+  GS_RANGE(a.eta, (long long)a.V * a.N, T, sizeof(cplx<T>), "precipitate last sweep", "order parameters");
   long long lr = 256 / per;
   if (lr > a.nrows) lr = a.nrows;
   a.lr = (int)lr;

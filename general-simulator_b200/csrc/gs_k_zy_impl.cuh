@@ -7,8 +7,27 @@
 namespace gs {
 
 
+// the launch-range check of a z-forward pass (F fields of rows_per_field rows of 2H values)
+template <typename T, int H> static cudaError_t zfwd_ranges(const ZfwdArgs<T>& a) {
+  const long long F = a.nrows / a.rows_per_field, per = a.rows_per_field * 2 * H;
+  if (a.src0) {
+    GS_RANGE(a.src0, (F - 1) * a.fstride + per, T, sizeof(cplx<T>), "z forward", "source fields");
+  } else {
+    for (long long f = 0; f < F; ++f) {
+      GS_RANGE(a.src[f], per, T, sizeof(cplx<T>), "z forward", "source field");
+      if (a.mul[f]) GS_RANGE(a.mul[f], per, T, sizeof(cplx<T>), "z forward", "multiplier field");
+    }
+  }
+  GS_RANGE(a.dst, a.nrows * H, cplx<T>, sizeof(cplx<T>), "z forward", "spectrum");
+  return cudaSuccess;
+}
+
 template <typename T, int H> static cudaError_t zfwd_n(ZfwdArgs<T>& a, cudaStream_t s, int lines_req) {
   using L = Line<T, H>;
+  if (bounds_check_on()) {
+    const cudaError_t e = zfwd_ranges<T, H>(a);
+    if (e != cudaSuccess) return e;
+  }
   long long lpc = 256 / L::P;
   // a requested line count (autotuner) when the block stays within 1024
   // threads and the shared-memory opt-in
@@ -47,6 +66,7 @@ static cudaError_t ypass_n(YArgs<T>& a, int F, cudaStream_t s, int cols_req) {
       (size_t)cols_req * L::PAD * sizeof(cplx<T>) <= 200 * 1024)
     a.tz = cols_req;
   const size_t smem = (size_t)a.tz * L::PAD * sizeof(cplx<T>);
+  GS_RANGE(a.spec, (long long)F * a.n0 * N1 * a.h, cplx<T>, sizeof(cplx<T>), "y pass", "spectrum");
   allow_max_smem<k_ypass<T, N1, DIR, R1>>();
   dim3 grid(a.h / a.tz, a.n0, F);
   k_ypass<T, N1, DIR, R1><<<grid, a.tz * L::P, smem, s>>>(a);

@@ -115,6 +115,27 @@ template <auto Kernel> inline int max_block_threads() {
   return r;
 }
 
+// Bounds checks (gs_bounds.cu).  check_range: does [p, p + elems * elem_bytes)
+// lie in one device allocation, with p aligned to `align` (cudaErrorInvalidValue
+// and a message for bounds_message() otherwise; cudaSuccess while the check is
+// off).  bc_after: the bounds-check build's end of a step entry (wait, then
+// GS_EBOUNDS after an index violation); rc itself in a normal build.
+bool bounds_check_on();
+void set_bounds_check(bool on);
+const char* bounds_message();
+void clear_bounds_message();
+cudaError_t check_range(const void* p, long long elems, size_t elem_bytes, size_t align, const char* kernel,
+                        const char* what);
+int bc_after(int rc, cudaStream_t st);
+// in a launcher: refuse the launch when a buffer range does not fit
+#define GS_RANGE(p, n, E, align, kernel, what)                                                            \
+  do {                                                                                                    \
+    if (::gs::bounds_check_on()) {                                                                        \
+      const cudaError_t e__ = ::gs::check_range((p), (long long)(n), sizeof(E), (align), (kernel), (what)); \
+      if (e__ != cudaSuccess) return e__;                                                                 \
+    }                                                                                                     \
+  } while (0)
+
 #define GS_SIZE_CASES(M) \
   M(1) M(2) M(4) M(6) M(8) M(12) M(16) M(24) M(32) M(48) M(64) M(96) M(128) M(256)
 

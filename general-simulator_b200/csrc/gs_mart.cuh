@@ -169,7 +169,13 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     if (FUSE) a.spec_next += off / 2;
   }
   const int Vn = mc.V;
+  // logical extents (values): every field set of the launch (gridDim.y sims
+  // when batched) and this block's simulation's offset in them
+  GS_BC_DECL(const long long fext = (long long)(BATCH ? gridDim.y : 1) * Vn * a.nrows * a.n2,
+             foff = BATCH ? (long long)blockIdx.y * Vn * a.nrows * a.n2 : 0,
+             next = (long long)a.nrows * a.n2)
   if constexpr (ZF) {
+    GS_BC_SMEM_GUARD((long long)(blockDim.x / L::P) * L::PAD, V, BC_UPD_SMEM)
     const int line = threadIdx.x / L::P, t = threadIdx.x % L::P;
     const int v = line % Vn, rr = line / Vn;
     const long long row = (long long)blockIdx.x * a.lr + rr;
@@ -177,7 +183,8 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     V* sl = smb + line * L::PAD;
     const V* srow = a.spec + ((long long)v * a.nrows + (act ? row : 0)) * H;
     V r[L::R1];
-    zinv_row<T, H>(srow, act, t, sl, a.tw_h, a.tw_n2, r);
+    zinv_row<T, H>(srow, act, t, sl, a.tw_h, a.tw_n2, r,
+                   GS_BCX(foff / 2 + ((long long)v * a.nrows + (act ? row : 0)) * H), GS_BCX(fext / 2));
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = r[i];
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     T e[VM][CW];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
-      if (p < Vn) ldv<CW>(a.eta_in + p * N + cell, e[p]);
+      if (p < Vn) ldv<CW>(a.eta_in + GS_BCR(foff, p * N + cell, CW, fext, BC_UPD_ETA), e[p]);
     T s2[CW], s4[CW], pr[CW], P0[CW];
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
@@ -242,7 +249,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
 #pragma unroll
     for (int j = 0; j < CW; ++j) dfc[j] = 1;
     if (mc.has_defect) {
-      ldv<CW>(a.defect + cell, dfc);
+      ldv<CW>(a.defect + GS_BCR(0, cell, CW, next, BC_UPD_AUX), dfc);
 #pragma unroll
       for (int j = 0; j < CW; ++j) dfc[j] = (T)1 - dfc[j];
     }
@@ -252,24 +259,27 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
     for (int q = 0; q < VM; ++q) {
       if (q >= Vn) break;
       const T* eq = a.eta_in + q * N + cell;
+      GS_BC_DECL(const long long qoff = foff + (long long)q * N + cell, hext = 2 * Vn * hplane)
       T vxp[CW], vxm[CW], vyp[CW], vym[CW];
-      ldv<CW>(hhi ? a.halo + ((long long)(Vn + q) * hplane + yz) : eq + oxp, vxp);
-      ldv<CW>(hlo ? a.halo + ((long long)q * hplane + yz) : eq + oxm, vxm);
-      ldv<CW>(eq + oyp, vyp);
-      ldv<CW>(eq + oym, vym);
-      const T el_ = eq[ozl], er_ = eq[ozr];
+      ldv<CW>(hhi ? a.halo + GS_BCR(0, (long long)(Vn + q) * hplane + yz, CW, hext, BC_UPD_HALO)
+                  : eq + GS_BCR(qoff, oxp, CW, fext, BC_UPD_ETA), vxp);
+      ldv<CW>(hlo ? a.halo + GS_BCR(0, (long long)q * hplane + yz, CW, hext, BC_UPD_HALO)
+                  : eq + GS_BCR(qoff, oxm, CW, fext, BC_UPD_ETA), vxm);
+      ldv<CW>(eq + GS_BCR(qoff, oyp, CW, fext, BC_UPD_ETA), vyp);
+      ldv<CW>(eq + GS_BCR(qoff, oym, CW, fext, BC_UPD_ETA), vym);
+      const T el_ = eq[GS_BCO(qoff, ozl, fext, BC_UPD_ETA)], er_ = eq[GS_BCO(qoff, ozr, fext, BC_UPD_ETA)];
       const T* Rq = ZF ? reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0 : nullptr;
       T Rl[CW];
       if constexpr (ZF) {
 #pragma unroll
         for (int j = 0; j < CW; ++j) Rl[j] = Rq[j];
       } else {
-        ldv<CW>(a.r_in + q * N + cell, Rl);
+        ldv<CW>(a.r_in + GS_BCR(0, q * N + cell, CW, (long long)Vn * next, BC_UPD_AUX), Rl);
       }
       T Kq[CW];
 #pragma unroll
       for (int j = 0; j < CW; ++j) Kq[j] = 0;
-      if (mc.has_K) ldv<CW>(a.K + q * N + cell, Kq);
+      if (mc.has_K) ldv<CW>(a.K + GS_BCR(0, q * N + cell, CW, (long long)Vn * next, BC_UPD_AUX), Kq);
       T xi[4] = {0, 0, 0, 0};
       if (!STATS && mc.noise != (T)0)
         normal_quad<T>((uint32_t)(gcell >> 2), mc.step, mc.sim, (uint32_t)q, mc.k0, mc.k1, xi);
@@ -332,8 +342,8 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
           acc[ACC_FDISL].add((double)lin);
         }
       }
-      if (!STATS) stv<CW>(a.eta_out + q * N + cell, out);
-      if (!BATCH && a.r_out) stv<CW>(a.r_out + q * N + cell, rv);
+      if (!STATS) stv<CW>(a.eta_out + GS_BCR(foff, q * N + cell, CW, fext, BC_UPD_ETA_OUT), out);
+      if (!BATCH && a.r_out) stv<CW>(a.r_out + GS_BCR(0, q * N + cell, CW, (long long)Vn * next, BC_UPD_AUX), rv);
       if (FUSE) {
         if constexpr (ZF) {
           T* sq = const_cast<T*>(Rq);
@@ -343,7 +353,7 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
           T o2[CW];
 #pragma unroll
           for (int j = 0; j < CW; ++j) o2[j] = out[j] * out[j];
-          stv<CW>(a.sq_out + q * N + cell, o2);
+          stv<CW>(a.sq_out + GS_BCR(0, q * N + cell, CW, (long long)Vn * next, BC_UPD_AUX), o2);
         }
       }
     }
@@ -360,7 +370,8 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) x[r] = sl[L::in_pos(t, r)];
     __syncthreads();
-    zfwd_line<T, H>(x, t, sl, act ? a.spec_next + ((long long)v * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
+    zfwd_line<T, H>(x, t, sl, act ? a.spec_next + ((long long)v * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2,
+                    GS_BCX(foff / 2 + ((long long)v * a.nrows + row) * H), GS_BCX(fext / 2));
   }
 }
 

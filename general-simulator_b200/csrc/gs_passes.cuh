@@ -155,7 +155,8 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
 // sl is the line's shared buffer (PAD values).  All threads of the block call it.
 template <typename T, int H>
 __device__ __forceinline__ void zfwd_line(cplx<T> (&v)[Line<T, H>::R1], int t, cplx<T>* sl, cplx<T>* dst,
-                                          const cplx<T>* __restrict__ tw_h, const cplx<T>* __restrict__ tw_n2) {
+                                          const cplx<T>* __restrict__ tw_h, const cplx<T>* __restrict__ tw_n2,
+                                          long long bc_doff, long long bc_dext) {
   using L = Line<T, H>;
   using V = cplx<T>;
   auto sm = [sl](int pos) -> V& { return sl[pos]; };
@@ -179,7 +180,7 @@ __device__ __forceinline__ void zfwd_line(cplx<T> (&v)[Line<T, H>::R1], int t, c
         const V o = mk2((T)0.5 * d.y, (T)-0.5 * d.x);  // -i d / 2
         s = e + cmul(o, __ldg(&tw_n2[k]));
       }
-      dst[k] = s;
+      dst[GS_BCO(bc_doff, k, bc_dext, BC_ZFWD_DST)] = s;
     }
   }
 }
@@ -208,6 +209,7 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
   const int t = threadIdx.x % L::P, line = threadIdx.x / L::P;
   const long long row = (long long)blockIdx.x * a.lpc + line;
   const bool act = row < a.nrows;
+  GS_BC_SMEM_GUARD((long long)(blockDim.x / L::P) * L::PAD, V, BC_ZFWD_SMEM)
   V* sl = smb + line * L::PAD;
   V v[L::R1];
   if (act) {
@@ -216,12 +218,17 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
     const V* src = reinterpret_cast<const V*>(a.src0 ? a.src0 + f * a.fstride : a.src[f]) + rin * H;
     const int sq = a.src0 ? a.square0 : a.square[f];
     const T* mp = a.src0 ? nullptr : a.mul[f];
+    // source extent in complex pairs: one field's rows, or all fields of src0
+    GS_BC_DECL(const long long soff = (a.src0 ? f * (a.fstride / 2) : 0) + rin * H,
+               sext = a.rows_per_field * H +
+                      (a.src0 ? (a.nrows / a.rows_per_field - 1) * (a.fstride / 2) : 0))
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) {
-      V x = src[L::in_pos(t, r)];
+      V x = src[GS_BCO(soff, L::in_pos(t, r), sext, BC_ZFWD_SRC)];
       if (sq) x = mk2(x.x * x.x, x.y * x.y);
       if (mp) {
-        const V m = reinterpret_cast<const V*>(mp)[rin * H + L::in_pos(t, r)];
+        const V m =
+            reinterpret_cast<const V*>(mp)[GS_BCI(rin * H + L::in_pos(t, r), a.rows_per_field * H, BC_ZFWD_SRC)];
         x = mk2(x.x * m.x, x.y * m.y);
       }
       v[r] = x;
@@ -230,7 +237,7 @@ __global__ void k_zfwd(ZfwdArgs<T> a) {
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) v[r] = mk2((T)0, (T)0);
   }
-  zfwd_line<T, H>(v, t, sl, act ? a.dst + row * H : nullptr, a.tw_h, a.tw_n2);
+  zfwd_line<T, H>(v, t, sl, act ? a.dst + row * H : nullptr, a.tw_h, a.tw_n2, GS_BCX(row * H), GS_BCX(a.nrows * H));
 }
 
 // ---------------------------------------------------------------------------
@@ -254,20 +261,24 @@ __global__ void k_ypass(YArgs<T> a) {
   const int c = threadIdx.x % TZ, t = threadIdx.x / TZ;
   const int kz0 = blockIdx.x * TZ, x = blockIdx.y, f = blockIdx.z;
   const int h = a.h;
+  GS_BC_SMEM_GUARD((long long)TZ * L::PAD, V, BC_Y_SMEM)
   V* base = a.spec + ((long long)(f * a.n0 + x) * N1) * h + kz0 + c;
+  // the spectrum's logical extent: gridDim.z fields of n0 x N1 x h
+  GS_BC_DECL(const long long boff = ((long long)(f * a.n0 + x) * N1) * h + kz0 + c,
+             bext = (long long)gridDim.z * a.n0 * N1 * h)
   auto sm = [smb, TZ, c](int pos) -> V& { return smb[pos * TZ + c]; };
   const bool special = (kz0 == 0);
   constexpr int HH = N1 / 2;
   V v[L::R1];
   if (DIR < 0 || !special) {
 #pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = base[(long long)L::in_pos(t, r) * h];
+    for (int r = 0; r < L::R1; ++r) v[r] = base[GS_BCO(boff, (long long)L::in_pos(t, r) * h, bext, BC_Y_SPEC)];
   } else {
     // inverse, tile holding kz slot 0: rebuild U(ky) = A(ky) + i B(ky)
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) {
       const int p = L::in_pos(t, r);
-      sm(p) = base[(long long)p * h];
+      sm(p) = base[GS_BCO(boff, (long long)p * h, bext, BC_Y_SPEC)];
     }
     __syncthreads();
 #pragma unroll
@@ -298,7 +309,7 @@ __global__ void k_ypass(YArgs<T> a) {
   L::template run<DIR>(v, t, sm, a.tw);
   if (DIR > 0 || !special) {
 #pragma unroll
-    for (int i = 0; i < L::R1; ++i) base[(long long)L::out_pos(t, i) * h] = v[i];
+    for (int i = 0; i < L::R1; ++i) base[GS_BCO(boff, (long long)L::out_pos(t, i) * h, bext, BC_Y_SPEC)] = v[i];
   } else {
     __syncthreads();
 #pragma unroll
@@ -323,7 +334,7 @@ __global__ void k_ypass(YArgs<T> a) {
         const V d = mk2(u.x - w.x, u.y + w.y);  // u - conj(w)
         o = mk2((T)0.5 * d.y, (T)-0.5 * d.x);
       }
-      base[(long long)s * h] = o;
+      base[GS_BCO(boff, (long long)s * h, bext, BC_Y_SPEC)] = o;
     }
   }
 }
@@ -396,7 +407,8 @@ struct TableOp {
     mx = mx < 0 ? -mx : mx;
     my = my < 0 ? -my : my;
     mz = mz < 0 ? -mz : mz;
-    const T* pt = a.btab + (((long long)mx * a.bt_d1 + my) * a.bt_d2 + mz) * S;
+    const T* pt = a.btab + GS_BCI((((long long)mx * a.bt_d1 + my) * a.bt_d2 + mz) * S,
+                                  (long long)(a.n0 / 2 + 1) * a.bt_d1 * a.bt_d2 * S, BC_X_TAB);
     if constexpr (sizeof(T) == 4 && S % 4 == 0) {
       const float4* b4 = reinterpret_cast<const float4*>(pt);
 #pragma unroll
@@ -484,7 +496,9 @@ struct PrecipOp {
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
                                                const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
     const PrecipUpd<T>& u = a.pu;
-    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+    // the per-axis tables hold n0, n1 and n2 entries
+    const T K = u.ktab[0][GS_BCI(ix, a.n0, BC_X_KTAB)] + u.ktab[1][GS_BCI(iy, a.n1, BC_X_KTAB)] +
+                u.ktab[2][GS_BCI(iz, a.n2, BC_X_KTAB)];
     const T ic = u.scale / ((T)1 + u.dtM * u.kc * K * K);
     const T ie = u.scale / ((T)1 + u.dtL * u.ke * K);
 #pragma unroll
@@ -508,7 +522,9 @@ struct PrecipPairOp {
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
                                                const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
     const PrecipUpd<T>& u = a.pu;
-    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+    // the per-axis tables hold n0, n1 and n2 entries
+    const T K = u.ktab[0][GS_BCI(ix, a.n0, BC_X_KTAB)] + u.ktab[1][GS_BCI(iy, a.n1, BC_X_KTAB)] +
+                u.ktab[2][GS_BCI(iz, a.n2, BC_X_KTAB)];
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
     if (blockIdx.z == 0) {
@@ -530,7 +546,9 @@ struct PrecipEtaOp {
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
                                                const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
     const PrecipUpd<T>& u = a.pu;
-    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+    // the per-axis tables hold n0, n1 and n2 entries
+    const T K = u.ktab[0][GS_BCI(ix, a.n0, BC_X_KTAB)] + u.ktab[1][GS_BCI(iy, a.n1, BC_X_KTAB)] +
+                u.ktab[2][GS_BCI(iz, a.n2, BC_X_KTAB)];
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
     out[0] = in[0] * (u.scale / ((T)1 + u.dtL * u.ke * K));
@@ -547,7 +565,9 @@ struct PrecipAdjOp {
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
                                                const cplx<T> (&in)[FM], cplx<T> (&out)[GM]) {
     const PrecipUpd<T>& u = a.pu;
-    const T K = u.ktab[0][ix] + u.ktab[1][iy] + u.ktab[2][iz];
+    // the per-axis tables hold n0, n1 and n2 entries
+    const T K = u.ktab[0][GS_BCI(ix, a.n0, BC_X_KTAB)] + u.ktab[1][GS_BCI(iy, a.n1, BC_X_KTAB)] +
+                u.ktab[2][GS_BCI(iz, a.n2, BC_X_KTAB)];
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
     if (blockIdx.z == 0) {
@@ -729,8 +749,10 @@ __device__ __forceinline__ void xpass_tile(const XArgs<T>& a, cplx<T>* smb, cplx
   L::template run<1, TWS>(v, t, sm, tw);
   if (iv) {
     V* dst = out_base + grp * fstride + (long long)ky * h + kz0 + c;
+    GS_BC_DECL(const long long ooff = (out_base - a.out) + grp * fstride + (long long)ky * h + kz0 + c,
+               oext = (long long)(a.nsim > 1 ? a.nsim : 1) * a.G * fstride)
 #pragma unroll
-    for (int i = 0; i < L::R1; ++i) dst[(long long)L::out_pos(t, i) * rstride] = v[i];
+    for (int i = 0; i < L::R1; ++i) dst[GS_BCO(ooff, (long long)L::out_pos(t, i) * rstride, oext, BC_X_OUT)] = v[i];
   }
 }
 
@@ -749,6 +771,8 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const int h = a.h, n1 = a.n1;
   const long long fstride = (long long)a.n0 * n1 * h;
   const int rstride = n1 * h;
+  // line regions of the groups, the packed-column results, the twiddles
+  GS_BC_SMEM_GUARD((long long)a.groups * L::PAD * TZ + (long long)(GM + 1) * N0, V, BC_X_SMEM)
   // batched simulations: one sim per blockIdx.z, fields stored sim after sim
   const V* in_base = a.in + (long long)blockIdx.z * a.F * fstride;
   V* out_base = a.out + (long long)blockIdx.z * a.G * fstride;
@@ -762,8 +786,12 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
   const bool fw = grp < a.F;
   {
     const V* src = in_base + (fw ? grp : 0) * fstride + (long long)ky * h + kz0 + c + (long long)t * rstride;
+    GS_BC_DECL(const long long ioff = (long long)blockIdx.z * a.F * fstride + (fw ? grp : 0) * fstride +
+                                      (long long)ky * h + kz0 + c + (long long)t * rstride,
+               iext = (long long)(a.nsim > 1 ? a.nsim : 1) * a.F * fstride)
 #pragma unroll
-    for (int r = 0; r < L::R1; ++r) v[r] = fw ? src[(long long)r * (L::P * rstride)] : mk2((T)0, (T)0);
+    for (int r = 0; r < L::R1; ++r)
+      v[r] = fw ? src[GS_BCO(ioff, (long long)r * (L::P * rstride), iext, BC_X_IN)] : mk2((T)0, (T)0);
   }
   xpass_tile<T, N0, FM, GM, Op, true, EX>(a, smb, part, TZ, grp, c, t, kz0, ky, out_base, v, tws);
 }
@@ -777,14 +805,15 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
 template <typename T, int H>
 __device__ __forceinline__ void zinv_row(const cplx<T>* __restrict__ srow, bool act, int t, cplx<T>* sl,
                                          const cplx<T>* __restrict__ tw_h, const cplx<T>* __restrict__ tw_n2,
-                                         cplx<T> (&v)[Line<T, H>::R1]) {
+                                         cplx<T> (&v)[Line<T, H>::R1], long long bc_soff,
+                                         long long bc_sext) {
   using L = Line<T, H>;
   using V = cplx<T>;
   if (act) {
 #pragma unroll
     for (int r = 0; r < L::R1; ++r) {
       const int k = L::in_pos(t, r);
-      sl[k] = srow[k];
+      sl[k] = srow[GS_BCO(bc_soff, k, bc_sext, BC_ZINV_SPEC)];
     }
   }
   __syncthreads();
@@ -837,9 +866,11 @@ __global__ void k_zinv(ZinvArgs<T> a) {
   const int t = threadIdx.x % L::P, line = threadIdx.x / L::P;
   const long long row = (long long)blockIdx.x * a.lpc + line;
   const bool act = row < a.nrows;
+  GS_BC_SMEM_GUARD((long long)(blockDim.x / L::P) * L::PAD, V, BC_ZFWD_SMEM)
   V* sl = smb + line * L::PAD;
   V r[L::R1];
-  zinv_row<T, H>(a.spec + (act ? row : 0) * H, act, t, sl, a.tw_h, a.tw_n2, r);
+  zinv_row<T, H>(a.spec + (act ? row : 0) * H, act, t, sl, a.tw_h, a.tw_n2, r, GS_BCX((act ? row : 0) * H),
+                 GS_BCX(a.nrows * H));
   if (!act) return;
   const int f = (int)(row / a.rows_per_field);
   const long long rin = row - (long long)f * a.rows_per_field;
@@ -849,7 +880,7 @@ __global__ void k_zinv(ZinvArgs<T> a) {
   for (int i = 0; i < L::R1; ++i) {
     V x = r[i];
     if (off) x = mk2((T)((double)x.x + a.offset), (T)((double)x.y + a.offset));
-    dst[L::out_pos(t, i)] = x;
+    dst[GS_BCO(rin * H, L::out_pos(t, i), a.rows_per_field * H, BC_ZINV_DST)] = x;
   }
 }
 

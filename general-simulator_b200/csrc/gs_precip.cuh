@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
   const int rr = line / NL, f2 = line - rr * NL;
   const long long row = (long long)blockIdx.x * a.lr + rr;
   const bool rok = rr < a.lr && row < a.nrows;
+  GS_BC_SMEM_GUARD((long long)(blockDim.x / L::P) * L::PAD, V, BC_PMID_SMEM)
   V* sl = smb + line * L::PAD;
   // R field feeding this line: u_p lines take R_p, the mu line R_c
   int rf = -1;
@@ -140,7 +141,8 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
     const bool act = rok && rf >= 0;
     V r[L::R1];
     zinv_row<T, H>(a.rspec + ((long long)(rf >= 0 ? rf : 0) * a.nrows + (rok ? row : 0)) * H, act, t, sl, a.tw_h,
-                   a.tw_n2, r);
+                   a.tw_n2, r, GS_BCX(((long long)(rf >= 0 ? rf : 0) * a.nrows + (rok ? row : 0)) * H),
+                   GS_BCX((long long)a.F1 * a.nrows * H));
     __syncthreads();
     if (rf >= 0) {
 #pragma unroll
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
     } else if (rok && f2 == 0) {  // c: the row itself
       const V* srow = reinterpret_cast<const V*>(a.c + row * n2);
 #pragma unroll
-      for (int i = 0; i < L::R1; ++i) sl[L::in_pos(t, i)] = srow[L::in_pos(t, i)];
+      for (int i = 0; i < L::R1; ++i) sl[L::in_pos(t, i)] = srow[GS_BCO(row * H, L::in_pos(t, i), N / 2, BC_PMID_SRC)];
     } else {
 #pragma unroll
       for (int i = 0; i < L::R1; ++i) sl[L::in_pos(t, i)] = mk2((T)0, (T)0);
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
     for (int j = 0; j < CW; ++j) cc[j] = ln(0)[j];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
-      if (p < Vn) ldv<CW>(a.eta + (long long)p * N + cell, e[p]);
+      if (p < Vn) ldv<CW>(a.eta + GS_BCR(0, (long long)p * N + cell, CW, Vn * N, BC_PMID_SRC), e[p]);
     const bool hi_pair = CW == 2 && (cell & 2);
     {
       T zc[4] = {0, 0, 0, 0};
@@ -215,7 +217,8 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
 #pragma unroll
   for (int r = 0; r < L::R1; ++r) x[r] = sl[L::in_pos(t, r)];
   __syncthreads();
-  zfwd_line<T, H>(x, t, sl, rok ? a.dst + ((long long)f2 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
+  zfwd_line<T, H>(x, t, sl, rok ? a.dst + ((long long)f2 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2,
+                  GS_BCX(((long long)f2 * a.nrows + row) * H), GS_BCX((long long)NL * a.nrows * H));
 }
 
 // The end of the precipitate step fused with the start of the next one: the
@@ -248,17 +251,24 @@ __global__ void __launch_bounds__(256, 3) k_precip_zinv_fwd(PrecipZArgs<T> a) {
   const int rr = line / NL, f = line - rr * NL;
   const long long row = (long long)blockIdx.x * a.lr + rr;
   const bool act = rr < a.lr && row < a.nrows;
+  GS_BC_SMEM_GUARD((long long)(blockDim.x / L::P) * L::PAD, V, BC_PZF_SMEM)
+  // the spectrum holds max(V + 1, F1) fields
+  GS_BC_DECL(const long long sext = (long long)(a.F1 > NL ? a.F1 : NL) * a.nrows * H)
   V* sl = smb + line * L::PAD;
   V r[L::R1];
   // its reads of the block's spectrum rows finish before its first barrier
-  zinv_row<T, H>(a.spec + ((long long)f * a.nrows + (act ? row : 0)) * H, act, t, sl, a.tw_h, a.tw_n2, r);
+  zinv_row<T, H>(a.spec + ((long long)f * a.nrows + (act ? row : 0)) * H, act, t, sl, a.tw_h, a.tw_n2, r,
+                 GS_BCX(((long long)f * a.nrows + (act ? row : 0)) * H), GS_BCX(sext));
   T* const dst = f == 0 ? a.c : a.eta + (long long)(f - 1) * a.N;
   const bool off = f == 0 && a.mass;
 #pragma unroll
   for (int i = 0; i < L::R1; ++i) {
     V v = r[i];
     if (off) v = mk2((T)((double)v.x + a.offset), (T)((double)v.y + a.offset));
-    if (act) reinterpret_cast<V*>(dst + row * (2 * H))[L::out_pos(t, i)] = v;
+    if (act)
+      reinterpret_cast<V*>(dst + row * (2 * H))[GS_BCO(((f == 0 ? 0 : (long long)(f - 1) * a.N) / 2) + row * H,
+                                                       L::out_pos(t, i), (f == 0 ? a.N : (long long)a.V * a.N) / 2,
+                                                       BC_PZF_FIELD)] = v;
     r[i] = f == 0 ? v : mk2(v.x * v.x, v.y * v.y);  // the chain-1 input: c' itself, eta'_p^2
   }
   __syncthreads();
@@ -271,7 +281,8 @@ __global__ void __launch_bounds__(256, 3) k_precip_zinv_fwd(PrecipZArgs<T> a) {
   __syncthreads();
   const int f1 = f == 0 ? a.V : f - 1;  // chain-1 order: eta_p^2, then c
   const bool out = act && f1 < a.F1;
-  zfwd_line<T, H>(x, t, sl, out ? a.spec + ((long long)f1 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2);
+  zfwd_line<T, H>(x, t, sl, out ? a.spec + ((long long)f1 * a.nrows + row) * H : nullptr, a.tw_h, a.tw_n2,
+                  GS_BCX(((long long)f1 * a.nrows + row) * H), GS_BCX(sext));
 }
 
 template <typename T>

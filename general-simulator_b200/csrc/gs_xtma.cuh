@@ -60,6 +60,8 @@ __global__ void __launch_bounds__(XTmaShape<N0, FM, TZ>::threads, XTmaShape<N0, 
   using V = cplx<T>;
   using S = XTmaShape<N0, FM, TZ>;
   extern __shared__ __align__(1024) unsigned char smtma[];
+  // two stages of F fields, the packed-column results, the twiddles, two mbarriers (one value each)
+  GS_BC_SMEM_GUARD(2LL * a.F * S::region + (FM + 1) * N0 + 2, V, BC_X_SMEM)
   const int F = a.F;
   V* const stage0 = reinterpret_cast<V*>(smtma);  // stage s at stage0 + s * F * region
   V* part = stage0 + 2 * F * S::region;           // GM x N0 values of the packed columns

@@ -18,10 +18,15 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgsb200.so")
+# GS_BOUNDS_CHECK=1 loads the bounds-check build (index asserts in the kernels,
+# GS_EBOUNDS from the step entries, the launch-range check on)
+BOUNDS_CHECK_BUILD = os.environ.get("GS_BOUNDS_CHECK", "0") not in ("", "0")
+LIB_PATH = os.path.join(HERE, "libgsb200_bc.so" if BOUNDS_CHECK_BUILD else "libgsb200.so")
 
 GS_OK = 0
 GS_EINVAL = -10
+GS_ENOTSUP = -14
+GS_EBOUNDS = -16
 GS_MODEL_MART, GS_MODEL_PRECIPITATE, GS_MODEL_STRESS = 1, 2, 3
 GS_MODE_BASELINE, GS_MODE_REFCOMPAT = 0, 1
 GS_DTYPE_F32, GS_DTYPE_F64 = 0, 1
@@ -124,12 +129,13 @@ _lib: Optional[C.CDLL] = None
 
 
 def lib() -> C.CDLL:
-    """Load libgsb200.so (built in-tree by build.py); raise if it is missing."""
+    """Load libgsb200.so (libgsb200_bc.so under GS_BOUNDS_CHECK=1; built
+    in-tree by build.py); raise if it is missing."""
     global _lib
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise RuntimeError(f"libgsb200.so not built at {LIB_PATH}; run __graft_entry__.build()")
+        raise RuntimeError(f"{os.path.basename(LIB_PATH)} not built at {LIB_PATH}; run __graft_entry__.build()")
     L = C.CDLL(LIB_PATH)
     P, S = C.POINTER(GsParams), C.POINTER(GsStats)
     vp = C.c_void_p
@@ -210,6 +216,12 @@ def lib() -> C.CDLL:
                                      vp, vp]),
         "gs_mart_step_noalloc": (C.c_int, [P, vp, vp, C.c_int64, vp]),
         "gs_mart_step_noalloc_max_bytes": (C.c_size_t, []),
+        "gs_set_bounds_check": (None, [C.c_int]),
+        "gs_bounds_check_enabled": (C.c_int, []),
+        "gs_bounds_check_build": (C.c_int, []),
+        "gs_bounds_check_read": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
+        "gs_bounds_site_name": (C.c_char_p, [C.c_int]),
+        "gs_bounds_selftest": (C.c_int, [vp, C.c_int, C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -232,6 +244,23 @@ class GsError(RuntimeError):
 def check(rc: int, what: str) -> None:
     if rc != GS_OK:
         raise GsError(f"{what} failed with status {rc}: {last_error()}")
+
+
+def set_bounds_check(on: bool) -> None:
+    """The launch-range check (every build): each pass launcher checks that
+    its buffers' ranges lie inside their allocations before it launches."""
+    lib().gs_set_bounds_check(1 if on else 0)
+
+
+def bounds_record(clear: bool = False) -> dict:
+    """The bounds-check build's index-assert record of the current device
+    (synchronises it): violations, the first one's site, index, extent,
+    block and thread.  GsError in a normal build."""
+    out = (C.c_longlong * 6)()
+    check(lib().gs_bounds_check_read(out, 1 if clear else 0), "gs_bounds_check_read")
+    site = int(out[1])
+    return {"violations": int(out[0]), "site": site, "site_name": lib().gs_bounds_site_name(site).decode(),
+            "index": int(out[2]), "extent": int(out[3]), "block": int(out[4]), "thread": int(out[5])}
 
 
 def default_params(model: int, mode: int = GS_MODE_BASELINE) -> GsParams:

@@ -40,6 +40,7 @@ extern "C" {
 #define GS_ETIMEOUT (-13)   /* a bounded device wait gave up */
 #define GS_ENOTSUP (-14)    /* configuration not supported by the kernels */
 #define GS_ENODEV (-15)     /* no CUDA device visible */
+#define GS_EBOUNDS (-16)    /* the bounds-check build saw an index outside its buffer */
 
 /* ---- enums ------------------------------------------------------------- */
 #define GS_MODEL_MART 1        /* Dynamics_mart: TDGL of V variants + FFT elasticity */
@@ -463,6 +464,36 @@ int gs_plain_step(gs_sim* s, int nsteps, void* stream);
  * handle otherwise behaves as gs_sim_create's (fields, stats, destroy). */
 int gs_cufft_create(const gs_params* p, gs_sim** out);
 int gs_cufft_step(gs_sim* s, int nsteps, void* stream);
+
+/* ---- bounds checks (debugging; no counterpart in the reference, whose
+ * kernels check nothing, src/dynamics_mart.cu:113-117) ------------------- */
+/* The launch-range check, in every build: on != 0 makes each pass launcher
+ * check, before it launches, that every buffer range its kernel reaches lies
+ * inside one device allocation and is aligned for its vector accesses; a
+ * range that does not fit refuses the launch (the step returns GS_ECUDA with
+ * a message naming the kernel and the buffer).  Off by default; on when the
+ * environment has GS_BOUNDS_CHECK=1 or in the bounds-check build. */
+void gs_set_bounds_check(int on);
+int gs_bounds_check_enabled(void);
+/* 1 when this library is the bounds-check build (libgsb200_bc.so): its
+ * kernels check every index against the launch's extents, record the first
+ * violation and keep the access inside the buffer (no trap); gs_sim_step,
+ * gs_batch_step, gs_mart_step_noalloc, gs_cufft_step, the adjoint and slab
+ * entries then wait for their kernels and return GS_EBOUNDS after a
+ * violation (not while their stream is being captured). */
+int gs_bounds_check_build(void);
+/* The bounds-check build's record on the current device, summed over the
+ * library's modules: out[0] violations, out[1] site of the first one
+ * (gs_bounds_site_name), out[2] its index, out[3] the extent it broke,
+ * out[4] its block (x | y << 32), out[5] its thread.  clear != 0 zeroes the
+ * records.  Synchronises the device.  GS_ENOTSUP in a normal build. */
+int gs_bounds_check_read(long long out[6], int clear);
+const char* gs_bounds_site_name(int site);
+/* Self-test of the index asserts: a kernel stores i into buf[i] for i < n
+ * through a checked index against cap elements.  The bounds-check build
+ * records n - cap violations (n > cap) and writes nothing beyond buf[cap-1];
+ * a normal build refuses it (GS_ENOTSUP), since its kernel would. */
+int gs_bounds_selftest(int* buf, int cap, int n, void* stream);
 
 #ifdef __cplusplus
 }

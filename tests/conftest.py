@@ -21,6 +21,8 @@ def _ensure_built():
 
     if not os.path.exists(build.LIB):
         build.build_lib()
+    if not os.path.exists(build.LIB_BC):
+        build.build_lib(bounds_check=True)
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         build.build_oracle()
 

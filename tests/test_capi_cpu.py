@@ -87,3 +87,43 @@ def test_unsupported_grid_rejected_before_device(gb):
     h = C.c_void_p()
     rc = gb.lib().gs_sim_create(C.byref(p), C.byref(h))
     assert rc in (-14, -15)
+
+
+def test_bounds_check_build_exports_every_declared_symbol(gb):
+    """libgsb200_bc.so (kernels with index asserts) is a drop-in for the
+    normal library: the same entry points, and it says which build it is."""
+    import build
+
+    L = C.CDLL(build.LIB_BC)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    L.gs_bounds_check_build.restype = C.c_int
+    assert L.gs_bounds_check_build() == 1
+
+
+def test_normal_build_has_no_index_asserts(gb):
+    L = gb.lib()
+    if gb.BOUNDS_CHECK_BUILD:
+        pytest.skip("this process loaded the bounds-check build")
+    assert L.gs_bounds_check_build() == 0
+    rec = (C.c_longlong * 6)()
+    assert L.gs_bounds_check_read(rec, 0) == gb.GS_ENOTSUP
+    assert list(rec) == [0] * 6
+    # the unchecked self-test kernel would write beyond cap: refused before any launch
+    dummy = (C.c_int * 4)()
+    assert L.gs_bounds_selftest(C.cast(dummy, C.c_void_p), 2, 4, None) == gb.GS_ENOTSUP
+    assert "not the bounds-check build" in gb.last_error()
+    assert L.gs_bounds_site_name(1) == b"selftest"
+    assert L.gs_bounds_site_name(999) == b"unknown"
+
+
+def test_launch_range_check_switch(gb):
+    L = gb.lib()
+    was = L.gs_bounds_check_enabled()
+    try:
+        gb.set_bounds_check(True)
+        assert L.gs_bounds_check_enabled() == 1
+        gb.set_bounds_check(False)
+        assert L.gs_bounds_check_enabled() == 0
+    finally:
+        gb.set_bounds_check(bool(was))
