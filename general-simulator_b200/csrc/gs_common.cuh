@@ -31,6 +31,20 @@ __host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { re
 __host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __host__ __device__ __forceinline__ double2 operator*(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
+// Lane-wise add / subtract of two complex values: one packed FP32x2
+// instruction for float2 (the same IEEE round-to-nearest result per lane as
+// the scalar operations), two scalar ones for double2.
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+__device__ __forceinline__ double2 padd(double2 a, double2 b) { return a + b; }
+__device__ __forceinline__ double2 psub(double2 a, double2 b) { return a - b; }
+
 template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
   return mk2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

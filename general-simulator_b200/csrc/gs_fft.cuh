@@ -115,8 +115,8 @@ template <int DIR> struct Dft<1, DIR> {
 template <int DIR> struct Dft<2, DIR> {
   template <typename V> __device__ __forceinline__ static void run(V* v) {
     V a = v[0], b = v[1];
-    v[0] = a + b;
-    v[1] = a - b;
+    v[0] = padd(a, b);
+    v[1] = psub(a, b);
   }
 };
 template <int DIR> struct Dft<3, DIR> {
@@ -134,11 +134,11 @@ template <int DIR> struct Dft<3, DIR> {
 };
 template <int DIR> struct Dft<4, DIR> {
   template <typename V> __device__ __forceinline__ static void run(V* v) {
-    V t0 = v[0] + v[2], t1 = v[0] - v[2], t2 = v[1] + v[3], t3 = v[1] - v[3];
-    // w = DIR * i
+    V t0 = padd(v[0], v[2]), t1 = psub(v[0], v[2]), t2 = padd(v[1], v[3]), t3 = psub(v[1], v[3]);
+    // w = DIR * i (the swapped lanes stay scalar)
     V w3 = DIR > 0 ? mk2(-t3.y, t3.x) : mk2(t3.y, -t3.x);
-    v[0] = t0 + t2;
-    v[2] = t0 - t2;
+    v[0] = padd(t0, t2);
+    v[2] = psub(t0, t2);
     v[1] = t1 + w3;
     v[3] = t1 - w3;
   }

@@ -131,6 +131,32 @@ template <int CW> __device__ __forceinline__ void stv(double* p, const double (&
   for (int j = 0; j < CW; j += 2) *reinterpret_cast<double2*>(p + j) = make_double2(o[j], o[j + 1]);
 }
 
+// The baseline right-hand side and Euler step of two cells of one variant
+// as packed FP32x2 operations: lane by lane the operations and the order of
+// the scalar path in k_mart_update (the same bits), in half the instructions.
+//   g   = lapc0 (x+ + x-) + (lapc1 (y+ + y-) + lapc2 (z+ + z-))
+//   rhs = eta (lin' + kc K - L (P0 - cA eta^2) + el R) + g
+//   eta' = (eta + dt rhs + noise xi) (1 - defect)
+__device__ __forceinline__ float2 mart_upd2(const MartConst<float>& mc, float2 et, float2 xp, float2 xm, float2 yp,
+                                            float2 ym, float2 zs, float2 P0, float2 R, float2 K, float2 xi,
+                                            float2 dfc, float lqc, float cA) {
+  auto b = [](float s) { return make_float2(s, s); };
+  const float2 vx = __fadd2_rn(xp, xm), vy = __fadd2_rn(yp, ym);
+  float2 g = __fmul2_rn(b(mc.lapc[2]), zs);
+  g = __ffma2_rn(b(mc.lapc[1]), vy, g);
+  g = __ffma2_rn(b(mc.lapc[0]), vx, g);
+  const float2 e2 = __fmul2_rn(et, et);
+  const float2 m = __ffma2_rn(b(mc.kc), K, b(lqc));
+  const float2 t1 = __ffma2_rn(b(-cA), e2, P0);
+  const float2 s1 = __ffma2_rn(b(mc.el), R, m);
+  const float2 coef = __ffma2_rn(b(-mc.L), t1, s1);
+  const float2 rhs = __ffma2_rn(et, coef, g);
+  float2 en = __ffma2_rn(b(mc.dt), rhs, et);
+  en = __ffma2_rn(b(mc.noise), xi, en);
+  if (mc.has_defect) en = __fmul2_rn(en, dfc);
+  return en;
+}
+
 // One row group per block: the inverse z FFT of R_p for every (variant,
 // row) line leaves R in shared memory; then each thread updates a run of CW
 // cells (a quad, or a pair when n2 = 2) for all variants at once, so the
@@ -271,8 +297,15 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       const T* Rq = ZF ? reinterpret_cast<const T*>(smb + (rr * Vn + q) * L::PAD) + z0 : nullptr;
       T Rl[CW];
       if constexpr (ZF) {
+        if constexpr (sizeof(T) == 4 && CW == 4 && L::PAD % 2 == 0) {
+          // 16-byte shared-memory load: the line starts on a 16-byte boundary
+          // when its padded length is even, and z0 is a multiple of 4
+          const float4 R4 = *reinterpret_cast<const float4*>(Rq);
+          Rl[0] = R4.x; Rl[1] = R4.y; Rl[2] = R4.z; Rl[3] = R4.w;
+        } else {
 #pragma unroll
-        for (int j = 0; j < CW; ++j) Rl[j] = Rq[j];
+          for (int j = 0; j < CW; ++j) Rl[j] = Rq[j];
+        }
       } else {
         ldv<CW>(a.r_in + GS_BCR(0, q * N + cell, CW, (long long)Vn * next, BC_UPD_AUX), Rl);
       }
@@ -286,8 +319,30 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       const T lq = mc.lin[q];
       const T lqc = lq - lapsum2;
       T out[CW], rv[CW];
+      bool done = false;  // the packed FP32 path below advanced the run
+      if constexpr (sizeof(T) == 4 && CW == 4 && !STATS) {
+        if (!mc.refcompat) {
+          // z neighbour sums, then cells (0, 1) and (2, 3) as packed pairs
+          const float zs[4] = {el_ + e[q][1], e[q][0] + e[q][2], e[q][1] + e[q][3], e[q][2] + er_};
+#pragma unroll
+          for (int j = 0; j < 4; j += 2) {
+            const float2 en = mart_upd2(mc, make_float2(e[q][j], e[q][j + 1]), make_float2(vxp[j], vxp[j + 1]),
+                                        make_float2(vxm[j], vxm[j + 1]), make_float2(vyp[j], vyp[j + 1]),
+                                        make_float2(vym[j], vym[j + 1]), make_float2(zs[j], zs[j + 1]),
+                                        make_float2(P0[j], P0[j + 1]), make_float2(Rl[j], Rl[j + 1]),
+                                        make_float2(Kq[j], Kq[j + 1]), make_float2(xi[j], xi[j + 1]),
+                                        make_float2(dfc[j], dfc[j + 1]), lqc, cA);
+            out[j] = en.x;
+            out[j + 1] = en.y;
+            rv[j] = Rl[j];
+            rv[j + 1] = Rl[j + 1];
+          }
+          done = true;
+        }
+      }
 #pragma unroll
       for (int j = 0; j < CW; ++j) {
+        if (done) break;
         const T et = e[q][j];
         const T zlv = j == 0 ? el_ : e[q][j - 1];
         const T zrv = j == CW - 1 ? er_ : e[q][j + 1];
@@ -347,8 +402,19 @@ __global__ void __launch_bounds__(256, UpdBlocks<VM, STATS>::v) k_mart_update(Ma
       if (FUSE) {
         if constexpr (ZF) {
           T* sq = const_cast<T*>(Rq);
+          if constexpr (sizeof(T) == 4 && CW == 4) {
+            const float2 a = __fmul2_rn(make_float2(out[0], out[1]), make_float2(out[0], out[1]));
+            const float2 b = __fmul2_rn(make_float2(out[2], out[3]), make_float2(out[2], out[3]));
+            if constexpr (L::PAD % 2 == 0) {  // 16-byte aligned (as the load above)
+              *reinterpret_cast<float4*>(sq) = make_float4(a.x, a.y, b.x, b.y);
+            } else {  // 8-byte aligned: a line holds whole complex values
+              reinterpret_cast<float2*>(sq)[0] = a;
+              reinterpret_cast<float2*>(sq)[1] = b;
+            }
+          } else {
 #pragma unroll
-          for (int j = 0; j < CW; ++j) sq[j] = out[j] * out[j];
+            for (int j = 0; j < CW; ++j) sq[j] = out[j] * out[j];
+          }
         } else {
           T o2[CW];
 #pragma unroll

@@ -175,8 +175,9 @@ __device__ __forceinline__ void zfwd_line(cplx<T> (&v)[Line<T, H>::R1], int t, c
         s = mk2(zk.x + zk.y, zk.x - zk.y);
       } else {
         const V zm = sl[H - k];
-        const V e = mk2((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
-        const V d = mk2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+        const V Pz = padd(zk, zm), Mz = psub(zk, zm);
+        const V e = mk2((T)0.5 * Pz.x, (T)0.5 * Mz.y);
+        const V d = mk2(Mz.x, Pz.y);  // zk - conj(zm)
         const V o = mk2((T)0.5 * d.y, (T)-0.5 * d.x);  // -i d / 2
         s = e + cmul(o, __ldg(&tw_n2[k]));
       }
@@ -828,8 +829,9 @@ __device__ __forceinline__ void zinv_row(const cplx<T>* __restrict__ srow, bool 
       z = mk2(s0.x + s0.y, s0.x - s0.y);
     } else {
       const V sk = sl[k], sm_ = sl[H - k];
-      const V A = mk2(sk.x + sm_.x, sk.y - sm_.y);   // sk + conj(sm)
-      const V D = mk2(sk.x - sm_.x, sk.y + sm_.y);   // sk - conj(sm)
+      const V Ps = padd(sk, sm_), Ms = psub(sk, sm_);
+      const V A = mk2(Ps.x, Ms.y);   // sk + conj(sm)
+      const V D = mk2(Ms.x, Ps.y);   // sk - conj(sm)
       const V w = __ldg(&tw_n2[k]);
       const V Bv = cmulc(D, w);                      // D * w^-k
       z = mk2(A.x - Bv.y, A.y + Bv.x);               // A + i Bv

@@ -7,6 +7,8 @@
 // of the semi-implicit update in k space.  Stress (src/dynamics_stress.cu:
 // 184-191): the defect mask |eta_v| > 0.9, on the device.
 #pragma once
+#include <type_traits>
+
 #include "gs_mart.cuh"
 
 namespace gs {
@@ -27,25 +29,55 @@ template <typename T> struct PrecipLocalArgs {
   T dtL;
 };
 
+// Lane-wise arithmetic with one rounding per operation, on a scalar or on a
+// packed FP32 pair (two cells per instruction): the local terms below are
+// written once in these operations, so the packed and the scalar sweeps give
+// the same bits lane by lane.
+__device__ __forceinline__ float lfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double lfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float lmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double lmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float2 lmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float ladd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double ladd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float2 ladd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float lsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double lsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float2 lsub(float2 a, float2 b) { return psub(a, b); }
+template <typename X, typename T> __device__ __forceinline__ X lbc(T s) {
+  if constexpr (sizeof(X) == 2 * sizeof(T))
+    return X{s, s};
+  else
+    return s;
+}
+
 // mu_c at one cell (s1 = sum_p eta_p^2; rc = R of c when c couples)
-template <typename T>
-__device__ __forceinline__ T precip_mu(const PrecipLocalArgs<T>& a, T c, T s1, T rc, T z) {
-  T mu = a.A[1] * (c - a.c1) + a.A[2] / (T)2 * s1;
-  if (a.c_elastic) mu += a.Es * rc;
-  mu += a.an * z;
-  return mu;
+//   mu = A1 (c - c1) + A2/2 s1 [+ Xi w_el R_c] + noise z
+template <typename X, typename T>
+__device__ __forceinline__ X precip_mu(const PrecipLocalArgs<T>& a, X c, X s1, X rc, X z) {
+  X mu = lfma(lbc<X>(a.A[1]), lsub(c, lbc<X>(a.c1)), lmul(lbc<X>(a.A[2] / (T)2), s1));
+  if (a.c_elastic) mu = lfma(lbc<X>(a.Es), rc, mu);
+  return lfma(lbc<X>(a.an), z, mu);
 }
 
 // g_p at one cell (t2, t4: sums of eta_r^2, eta_r^4 over r != p)
-template <typename T>
-__device__ __forceinline__ T precip_g(const PrecipLocalArgs<T>& a, T c, T x, T t2, T t4, T rp, T z) {
-  const T t22 = t2 * t2 - t4;  // sum over ordered pairs i != j, both != p
-  const T x2 = x * x;
-  T gv = (2 * a.A[5] * x + 4 * a.A[6] * x2 * x) * t2 + (2 * a.A[6] * x) * t4 + (2 * a.A[7] * x) * t22 +
-         a.A[2] * x * (c - a.c2) - a.A[3] * x2 * x + a.A[4] * x2 * x2 * x;
-  gv += a.Es * (T)2 * x * rp;
-  gv += a.an * z;
-  return gv;
+//   g = (2 A5 x + 4 A6 x^3) t2 + 2 A6 x t4 + 2 A7 x (t2^2 - t4) + A2 x (c - c2)
+//       - A3 x^3 + A4 x^5 + 2 Xi w_el x R_p + noise z
+template <typename X, typename T>
+__device__ __forceinline__ X precip_g(const PrecipLocalArgs<T>& a, X c, X x, X t2, X t4, X rp, X z) {
+  const X t22 = lsub(lmul(t2, t2), t4);  // sum over ordered pairs i != j, both != p
+  const X x2 = lmul(x, x);
+  const X x3 = lmul(x2, x);
+  X gv = lfma(lbc<X>((T)4 * a.A[6]), x3, lmul(lbc<X>((T)2 * a.A[5]), x));
+  gv = lmul(gv, t2);
+  gv = lfma(lmul(lbc<X>((T)2 * a.A[6]), x), t4, gv);
+  gv = lfma(lmul(lbc<X>((T)2 * a.A[7]), x), t22, gv);
+  gv = lfma(lmul(lbc<X>(a.A[2]), x), lsub(c, lbc<X>(a.c2)), gv);
+  gv = lfma(lbc<X>(-a.A[3]), x3, gv);
+  gv = lfma(lmul(lbc<X>(a.A[4]), lmul(x2, x2)), x, gv);
+  gv = lfma(lmul(lbc<X>((T)2 * a.Es), x), rp, gv);
+  return lfma(lbc<X>(a.an), z, gv);
 }
 
 template <typename T>
@@ -170,25 +202,50 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
     const long long cell = urow * n2 + z0;
     T* const lbase = reinterpret_cast<T*>(smb + ur * NL * L::PAD) + z0;
     auto ln = [lbase](int q) { return lbase + q * (2 * L::PAD); };  // line q of this row (reals)
-    T e[VM][CW], cc[CW];
-#pragma unroll
-    for (int j = 0; j < CW; ++j) cc[j] = ln(0)[j];
+    T e[VM][CW];
 #pragma unroll
     for (int p = 0; p < VM; ++p)
       if (p < Vn) ldv<CW>(a.eta + GS_BCR(0, (long long)p * N + cell, CW, Vn * N, BC_PMID_SRC), e[p]);
     const bool hi_pair = CW == 2 && (cell & 2);
+    // the run's cells in lanes of X: FP32 runs of four as two packed pairs
+    constexpr bool PK = sizeof(T) == 4 && CW == 4;
+    using X = typename std::conditional<PK, float2, T>::type;
+    constexpr int NX = PK ? CW / 2 : CW;
+    auto lx = [](const T* q, int k) -> X {  // lane group k of a shared-memory line
+      if constexpr (PK)
+        return *reinterpret_cast<const float2*>(q + 2 * k);
+      else
+        return q[k];
+    };
+    auto sx = [](T* q, int k, X v) {
+      if constexpr (PK)
+        *reinterpret_cast<float2*>(q + 2 * k) = v;
+      else
+        q[k] = v;
+    };
+    auto rx = [](const T (&r)[CW], int k) -> X {
+      if constexpr (PK)
+        return X{r[2 * k], r[2 * k + 1]};
+      else
+        return r[k];
+    };
+    auto zx = [hi_pair](const T (&z)[4], int k) -> X {  // the noise of lane group k
+      if constexpr (PK)
+        return X{z[2 * k], z[2 * k + 1]};
+      else
+        return CW == 2 ? (hi_pair ? z[k + 2 < 4 ? k + 2 : 3] : z[k]) : z[k];
+    };
     {
       T zc[4] = {0, 0, 0, 0};
       if (lc.an != (T)0) normal_quad<T>((uint32_t)(cell >> 2), lc.step, lc.sim, (uint32_t)Vn, lc.k0, lc.k1, zc);
 #pragma unroll
-      for (int j = 0; j < CW; ++j) {
-        T s1 = 0;
+      for (int k = 0; k < NX; ++k) {
+        X s1 = lbc<X>((T)0);
 #pragma unroll
         for (int p = 0; p < VM; ++p)
-          if (p < Vn) s1 += e[p][j] * e[p][j];
-        const T rc = (lc.c_elastic && a.F1 > Vn) ? ln(1)[j] : (T)0;
-        const T zj = CW == 2 ? (hi_pair ? zc[j + 2 < 4 ? j + 2 : 3] : zc[j]) : zc[j];
-        ln(1)[j] = precip_mu(lc, cc[j], s1, rc, zj);
+          if (p < Vn) s1 = lfma(rx(e[p], k), rx(e[p], k), s1);
+        const X rc = (lc.c_elastic && a.F1 > Vn) ? lx(ln(1), k) : lbc<X>((T)0);
+        sx(ln(1), k, precip_mu(lc, lx(ln(0), k), s1, rc, zx(zc, k)));
       }
     }
 #pragma unroll
@@ -197,18 +254,18 @@ __global__ void __launch_bounds__(256, 3) k_precip_mid(PrecipMidArgs<T> a) {
       T zp[4] = {0, 0, 0, 0};
       if (lc.an != (T)0) normal_quad<T>((uint32_t)(cell >> 2), lc.step, lc.sim, (uint32_t)p, lc.k0, lc.k1, zp);
 #pragma unroll
-      for (int j = 0; j < CW; ++j) {
-        T t2 = 0, t4 = 0;
+      for (int k = 0; k < NX; ++k) {
+        X t2 = lbc<X>((T)0), t4 = lbc<X>((T)0);
 #pragma unroll
         for (int r = 0; r < VM; ++r)
           if (r < Vn && r != p) {
-            const T x = e[r][j];
-            t2 += x * x;
-            t4 += x * x * x * x;
+            const X x2 = lmul(rx(e[r], k), rx(e[r], k));
+            t2 = ladd(t2, x2);
+            t4 = lfma(x2, x2, t4);
           }
-        const T zj = CW == 2 ? (hi_pair ? zp[j + 2 < 4 ? j + 2 : 3] : zp[j]) : zp[j];
-        const T gv = precip_g(lc, cc[j], e[p][j], t2, t4, ln(2 + p)[j], zj);
-        ln(2 + p)[j] = e[p][j] - lc.dtL * gv;
+        const X x = rx(e[p], k);
+        const X gv = precip_g(lc, lx(ln(0), k), x, t2, t4, lx(ln(2 + p), k), zx(zp, k));
+        sx(ln(2 + p), k, lfma(lbc<X>(-lc.dtL), gv, x));  // u_p = eta_p - dt L g_p
       }
     }
   }
