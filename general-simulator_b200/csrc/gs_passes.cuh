@@ -492,6 +492,12 @@ __global__ void k_btab_fill(ElasticConst<T> ec, int n0, int n1, int n2, int d0, 
   }
 }
 
+// A semi-implicit symbol scale / den (den >= 1, far below 2^126): FP32
+// through the hardware reciprocal (__fdividef, within 2 ulp), FP64 by the
+// IEEE division.
+__device__ __forceinline__ float sym_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double sym_div(double a, double b) { return a / b; }
+
 struct PrecipOp {
   template <typename T, int FM, int GM>
   __device__ __forceinline__ static void apply(const XArgs<T>& a, const int (&nn)[3], int ix, int iy, int iz,
@@ -500,8 +506,8 @@ struct PrecipOp {
     // the per-axis tables hold n0, n1 and n2 entries
     const T K = u.ktab[0][GS_BCI(ix, a.n0, BC_X_KTAB)] + u.ktab[1][GS_BCI(iy, a.n1, BC_X_KTAB)] +
                 u.ktab[2][GS_BCI(iz, a.n2, BC_X_KTAB)];
-    const T ic = u.scale / ((T)1 + u.dtM * u.kc * K * K);
-    const T ie = u.scale / ((T)1 + u.dtL * u.ke * K);
+    const T ic = sym_div(u.scale, (T)1 + u.dtM * u.kc * K * K);
+    const T ie = sym_div(u.scale, (T)1 + u.dtL * u.ke * K);
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
     out[0] = (in[0] - in[1] * (u.dtM * K)) * ic;
@@ -529,11 +535,11 @@ struct PrecipPairOp {
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
     if (blockIdx.z == 0) {
-      const T ic = u.scale / ((T)1 + u.dtM * u.kc * K * K);
+      const T ic = sym_div(u.scale, (T)1 + u.dtM * u.kc * K * K);
       out[0] = (in[0] - in[1] * (u.dtM * K)) * ic;
       if (u.mass_proj && ix == 0 && iy == 0 && iz == 0) out[0] = mk2((T)0, (T)0);
     } else {
-      const T ie = u.scale / ((T)1 + u.dtL * u.ke * K);
+      const T ie = sym_div(u.scale, (T)1 + u.dtL * u.ke * K);
       out[0] = (in[0] - in[1] * u.dtL) * ie;
     }
   }
@@ -552,7 +558,7 @@ struct PrecipEtaOp {
                 u.ktab[2][GS_BCI(iz, a.n2, BC_X_KTAB)];
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
-    out[0] = in[0] * (u.scale / ((T)1 + u.dtL * u.ke * K));
+    out[0] = in[0] * sym_div(u.scale, (T)1 + u.dtL * u.ke * K);
   }
 };
 
@@ -572,12 +578,12 @@ struct PrecipAdjOp {
 #pragma unroll
     for (int g = 0; g < GM; ++g) out[g] = mk2((T)0, (T)0);
     if (blockIdx.z == 0) {
-      const T d = u.scale / ((T)1 + u.dtM * u.kc * K * K);
+      const T d = sym_div(u.scale, (T)1 + u.dtM * u.kc * K * K);
       out[0] = in[0] * d;
       out[1] = in[0] * (K * d);
       out[2] = in[1] * (K * K * d);
     } else {
-      const T d = u.scale / ((T)1 + u.dtL * u.ke * K);
+      const T d = sym_div(u.scale, (T)1 + u.dtL * u.ke * K);
       out[0] = in[0] * d;
       out[1] = in[0] * (K * d);
       out[2] = in[1] * (K * d);

@@ -4,15 +4,17 @@ profiler captures (ncu) and quick timings of a single workload.
 
   python general-simulator_b200/gs_profile.py --workload martensite|precipitate|cufft|plain|batch
       [--n 256] [--steps 3] [--warmup 2] [--dtype f32|f64] [--graph] [--tune]
-      [--shape NX,NY,NZ]
+      [--shape NX,NY,NZ] [--noise AMP]
 
 martensite: the 3D three-variant workload (noise 1e-3, sigma_zz 0.005);
 precipitate: concentration + 4 variants, semi-implicit; cufft / plain: the
 two comparator steps on the martensite workload; batch: the 64-simulation
 ensemble (--shape keeps only its simulations of one grid shape, to time a
-shape group alone).  --graph replays the steps as captured graphs, --tune
-runs the autotuner first.  Prints the device time per step (CUDA events on
-the stepping stream, after the warm-up steps)."""
+shape group alone).  --noise sets the martensite workloads' noise amplitude
+(0: the same kernels with the noise term skipped).  --graph replays the
+steps as captured graphs, --tune runs the autotuner first.  Prints the
+device time per step (CUDA events on the stepping stream, after the warm-up
+steps)."""
 from __future__ import annotations
 
 import argparse
@@ -36,6 +38,7 @@ def main() -> None:
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--tune", action="store_true")
     ap.add_argument("--shape", default="")
+    ap.add_argument("--noise", type=float, default=1e-3)
     args = ap.parse_args()
 
     import torch
@@ -63,7 +66,7 @@ def main() -> None:
         obj.set_field("eta", gb.initial_eta(p, 3))
         cells = p.ncells
     else:
-        p = gb.mart3d_params(args.n, dtype=dt, noise=1e-3)
+        p = gb.mart3d_params(args.n, dtype=dt, noise=args.noise)
         obj = gb.Sim(p, plain=args.workload == "plain", cufft=args.workload == "cufft")
         obj.set_field("eta", gb.initial_eta(p, 1))
         cells = p.ncells
