@@ -804,9 +804,11 @@ __global__ void __launch_bounds__(XBounds<FM, GM>::v) k_xpass(XArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// z inverse of a packed row into registers.  Loads the row into the line's
-// shared buffer, rebuilds Z'_k = (S_k + conj S_{h-k}) + i (S_k - conj
-// S_{h-k}) w^-k and runs the inverse length-h FFT.  On return v[i] holds
+// z inverse of a packed row into registers.  Loads each value S_k of the
+// row with its partner S_{h-k} (no shared-memory round trip, no barrier),
+// rebuilds Z'_k = (S_k + conj S_{h-k}) + i (S_k - conj S_{h-k}) w^-k and runs
+// the inverse length-h FFT; every read of the row is done before the FFT's
+// first barrier.  On return v[i] holds
 // (r[2m], r[2m+1]) for m = out_pos(t, i).  All threads of the block call it.
 // ---------------------------------------------------------------------------
 template <typename T, int H>
@@ -816,14 +818,8 @@ __device__ __forceinline__ void zinv_row(const cplx<T>* __restrict__ srow, bool 
                                          long long bc_sext) {
   using L = Line<T, H>;
   using V = cplx<T>;
-  if (act) {
-#pragma unroll
-    for (int r = 0; r < L::R1; ++r) {
-      const int k = L::in_pos(t, r);
-      sl[k] = srow[GS_BCO(bc_soff, k, bc_sext, BC_ZINV_SPEC)];
-    }
-  }
-  __syncthreads();
+  // each value and its partner H - k straight from the row (the partner is
+  // another thread's own value of the same warp: an L1 hit)
 #pragma unroll
   for (int r = 0; r < L::R1; ++r) {
     const int k = L::in_pos(t, r);
@@ -831,10 +827,11 @@ __device__ __forceinline__ void zinv_row(const cplx<T>* __restrict__ srow, bool 
     if (!act) {
       z = mk2((T)0, (T)0);
     } else if (k == 0) {
-      const V s0 = sl[0];
+      const V s0 = srow[GS_BCO(bc_soff, 0, bc_sext, BC_ZINV_SPEC)];
       z = mk2(s0.x + s0.y, s0.x - s0.y);
     } else {
-      const V sk = sl[k], sm_ = sl[H - k];
+      const V sk = srow[GS_BCO(bc_soff, k, bc_sext, BC_ZINV_SPEC)];
+      const V sm_ = srow[GS_BCO(bc_soff, H - k, bc_sext, BC_ZINV_SPEC)];
       const V Ps = padd(sk, sm_), Ms = psub(sk, sm_);
       const V A = mk2(Ps.x, Ms.y);   // sk + conj(sm)
       const V D = mk2(Ms.x, Ps.y);   // sk - conj(sm)
@@ -844,7 +841,6 @@ __device__ __forceinline__ void zinv_row(const cplx<T>* __restrict__ srow, bool 
     }
     v[r] = z;
   }
-  __syncthreads();
   auto sm = [sl](int pos) -> V& { return sl[pos]; };
   L::template run<1>(v, t, sm, tw_h);
 }
