@@ -153,6 +153,12 @@ __device__ __forceinline__ void contract_at(const ElasticConst<T>& ec, const int
 // (r[2m], r[2m+1]) of the real row): the length-H FFT, then the split into
 // the packed half spectrum, written to dst (nullptr: the line is inactive).
 // sl is the line's shared buffer (PAD values).  All threads of the block call it.
+// Register of thread 0 of a line that holds the partner Z_{H-k} of its
+// register i (out_pos order; i = 0 is k = 0, its own partner).
+template <int R1, int R2> __device__ __forceinline__ constexpr int zfwd_partner0(int i) {
+  return i / R2 == 0 ? (i % R2 == 0 ? 0 : R2 - i % R2) : (R1 / R2 - i / R2) * R2 + (R2 - 1 - i % R2);
+}
+
 template <typename T, int H>
 __device__ __forceinline__ void zfwd_line(cplx<T> (&v)[Line<T, H>::R1], int t, cplx<T>* sl, cplx<T>* dst,
                                           const cplx<T>* __restrict__ tw_h, const cplx<T>* __restrict__ tw_n2,
@@ -161,20 +167,30 @@ __device__ __forceinline__ void zfwd_line(cplx<T> (&v)[Line<T, H>::R1], int t, c
   using V = cplx<T>;
   auto sm = [sl](int pos) -> V& { return sl[pos]; };
   L::template run<-1>(v, t, sm, tw_h);
-  __syncthreads();
+  // The split needs Z_k and Z_{H-k}: for t != 0 the partner is register
+  // R1-1-i of thread P-t of the same line, exchanged by a shuffle; thread 0
+  // holds its own partners (zfwd_partner0).  No shared memory, no barrier.
+  const unsigned wb = threadIdx.x & ~31u;
+  const unsigned mask = blockDim.x - wb >= 32 ? 0xffffffffu : ((1u << (blockDim.x - wb)) - 1u);
+  const int src = (L::P - t) % L::P;
 #pragma unroll
-  for (int i = 0; i < L::R1; ++i) sl[L::out_pos(t, i)] = v[i];
-  __syncthreads();
-  if (dst) {
-#pragma unroll
-    for (int i = 0; i < L::R1; ++i) {
+  for (int i = 0; i < L::R1; ++i) {
+    V zm;
+    if constexpr (L::P > 1) {
+      const V send = v[L::R1 - 1 - i];
+      zm.x = __shfl_sync(mask, send.x, src, L::P);
+      zm.y = __shfl_sync(mask, send.y, src, L::P);
+      if (t == 0) zm = v[zfwd_partner0<L::R1, L::R2>(i)];
+    } else {
+      zm = v[zfwd_partner0<L::R1, L::R2>(i)];
+    }
+    if (dst) {
       const int k = L::out_pos(t, i);
-      const V zk = sl[k];
+      const V zk = v[i];
       V s;
       if (k == 0) {
         s = mk2(zk.x + zk.y, zk.x - zk.y);
       } else {
-        const V zm = sl[H - k];
         const V Pz = padd(zk, zm), Mz = psub(zk, zm);
         const V e = mk2((T)0.5 * Pz.x, (T)0.5 * Mz.y);
         const V d = mk2(Mz.x, Pz.y);  // zk - conj(zm)
